@@ -1,0 +1,244 @@
+"""Python bindings (ctypes) of libbbkde.so, the B200 direct kernel-density library.
+
+The product is the C ABI in include/bbkde.h and the C++ drop-in headers in
+include/bbkde/; this module only binds the C ABI so that tests and bench.py can
+drive it. There is no CPU fallback: if the CUDA library is missing or no device
+is present, every call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "lib", "libbbkde.so")
+
+# Status codes (bbkde_status).
+OK, OUT_OF_RANGE, INVALID_ARGUMENT, CUDA_ERROR, TIMEOUT, UNSUPPORTED, NO_DEVICE, \
+    ALLOC_FAILED = range(8)
+
+# Kernel kinds (bbkde_kernel_kind).
+GAUSSIAN, EPANECHNIKOV, GAUSSIAN_PRODUCT_2D, EPANECHNIKOV_PRODUCT_2D, \
+    GAUSSIAN_PRODUCT_CONV_2D, EPANECHNIKOV_PRODUCT_CONV_2D, GAUSSIAN_CONV_1D, \
+    EPANECHNIKOV_CONV_1D = range(8)
+
+FP32C, FP64 = 0, 1
+REFERENCE, QUERY = 0, 1
+FLAG_EXACT_GAUSS_CONV = 1
+
+# Every symbol include/bbkde.h declares.
+EXPORTED = [
+    "bbkde_abi_version", "bbkde_status_string", "bbkde_ctx_create", "bbkde_ctx_destroy",
+    "bbkde_ctx_last_error", "bbkde_ctx_set_stream", "bbkde_upload", "bbkde_size",
+    "bbkde_download_attributes", "bbkde_eval_range", "bbkde_eval_range_device",
+    "bbkde_adapt_density", "bbkde_unadapt_density", "bbkde_likelihood_cv",
+    "bbkde_lsq_conv_cv", "bbkde_last_launch_stats", "bbkde_launch_count",
+    "bbkde_device_info",
+]
+
+
+class KernelDesc(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("dim", C.c_int32), ("h", C.c_double * 2),
+                ("flags", C.c_int32), ("reserved", C.c_int32)]
+
+
+def kernel_desc(kind: int, dim: int, h, flags: int = 0) -> KernelDesc:
+    h = list(h) if hasattr(h, "__len__") else [h]
+    if len(h) == 1:
+        h = h * 2
+    return KernelDesc(kind, dim, (C.c_double * 2)(*h[:2]), flags, 0)
+
+
+class BBKDEError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"[{status}] {msg}")
+        self.status = status
+
+
+class OutOfRange(BBKDEError, IndexError):
+    pass
+
+
+class InvalidArgument(BBKDEError, ValueError):
+    pass
+
+
+_dp = C.POINTER(C.c_double)
+_lib = None
+
+
+def _ensure_built():
+    if not os.path.exists(LIB_PATH):
+        from . import build
+        build.build()
+
+
+def load_library(path: str = LIB_PATH):
+    """Load libbbkde.so (building it first if absent) and declare its signatures."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if path == LIB_PATH:
+        _ensure_built()
+    if not os.path.exists(path):
+        raise RuntimeError(f"libbbkde.so not found at {path}; run python -m bbrcit_kde_b200.build")
+    lib = C.CDLL(path)
+    vp = C.c_void_p
+    i64 = C.c_int64
+    lib.bbkde_abi_version.restype = C.c_int
+    lib.bbkde_status_string.restype = C.c_char_p
+    lib.bbkde_status_string.argtypes = [C.c_int]
+    lib.bbkde_ctx_create.argtypes = [C.c_int, C.POINTER(vp)]
+    lib.bbkde_ctx_destroy.argtypes = [vp]
+    lib.bbkde_ctx_last_error.restype = C.c_char_p
+    lib.bbkde_ctx_last_error.argtypes = [vp]
+    lib.bbkde_ctx_set_stream.argtypes = [vp, vp]
+    lib.bbkde_upload.argtypes = [vp, C.c_int, C.c_int, i64, _dp, _dp, _dp, _dp]
+    lib.bbkde_size.restype = i64
+    lib.bbkde_size.argtypes = [vp, C.c_int]
+    lib.bbkde_download_attributes.argtypes = [vp, _dp, _dp]
+    kd = C.POINTER(KernelDesc)
+    lib.bbkde_eval_range.argtypes = [vp, kd, i64, i64, i64, i64, C.c_int, C.c_int, _dp, i64]
+    lib.bbkde_eval_range_device.argtypes = [vp, kd, i64, i64, i64, i64, C.c_int, C.c_int, vp,
+                                            i64]
+    lib.bbkde_adapt_density.argtypes = [vp, kd, C.c_double, C.c_int, _dp, _dp, _dp, _dp]
+    lib.bbkde_unadapt_density.argtypes = [vp]
+    lib.bbkde_likelihood_cv.argtypes = [vp, kd, C.c_int, _dp]
+    lib.bbkde_lsq_conv_cv.argtypes = [vp, kd, C.c_int, _dp]
+    lib.bbkde_last_launch_stats.argtypes = [vp, _dp, _dp, C.POINTER(i64)]
+    lib.bbkde_launch_count.restype = i64
+    lib.bbkde_launch_count.argtypes = [vp]
+    lib.bbkde_device_info.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    _lib = lib
+    return lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(_dp)
+
+
+def _c(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+
+
+class Context:
+    """One bbkde_ctx (device buffers + stream) on one CUDA device."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load_library()
+        h = C.c_void_p()
+        rc = self.lib.bbkde_ctx_create(device, C.byref(h))
+        if rc != OK:
+            raise BBKDEError(rc, "bbkde_ctx_create failed: " +
+                             self.lib.bbkde_status_string(rc).decode())
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.bbkde_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, rc: int):
+        if rc == OK:
+            return
+        msg = (self.lib.bbkde_ctx_last_error(self.h) or b"").decode()
+        if rc == OUT_OF_RANGE:
+            raise OutOfRange(rc, msg)
+        if rc == INVALID_ARGUMENT:
+            raise InvalidArgument(rc, msg)
+        raise BBKDEError(rc, msg)
+
+    def set_stream(self, stream_ptr: int | None):
+        self._check(self.lib.bbkde_ctx_set_stream(self.h, stream_ptr))
+
+    def upload(self, role: int, coords, mass=None, abw=None, weight=None):
+        coords = _c(coords)
+        if coords.ndim == 1:
+            coords = coords.reshape(-1, 1)
+        n, dim = coords.shape
+        mass, abw, weight = _c(mass), _c(abw), _c(weight)
+        self._check(self.lib.bbkde_upload(self.h, role, dim, n, _p(coords), _p(mass), _p(abw),
+                                          _p(weight)))
+
+    def size(self, role: int) -> int:
+        return int(self.lib.bbkde_size(self.h, role))
+
+    def download_attributes(self):
+        n = self.size(REFERENCE)
+        mass, abw = np.empty(n), np.empty(n)
+        self._check(self.lib.bbkde_download_attributes(self.h, _p(mass), _p(abw)))
+        return mass, abw
+
+    def eval_range(self, desc: KernelDesc, r_i, r_j, q_i, q_j, normalized=True,
+                   precision=FP32C, block_size=0, out=None):
+        n = q_j - q_i + 1 if q_j >= q_i else 0
+        if out is None:
+            out = np.empty(max(n, 1))
+        self._check(self.lib.bbkde_eval_range(self.h, C.byref(desc), r_i, r_j, q_i, q_j,
+                                              int(normalized), precision, _p(out), block_size))
+        return out[:n]
+
+    def eval_range_device(self, desc: KernelDesc, r_i, r_j, q_i, q_j, out_ptr: int,
+                          normalized=True, precision=FP32C, block_size=0):
+        self._check(self.lib.bbkde_eval_range_device(self.h, C.byref(desc), r_i, r_j, q_i, q_j,
+                                                     int(normalized), precision, out_ptr,
+                                                     block_size))
+
+    def eval_all(self, desc: KernelDesc, normalized=True, precision=FP32C):
+        nr, nq = self.size(REFERENCE), self.size(QUERY)
+        return self.eval_range(desc, 0, nr - 1, 0, nq - 1, normalized, precision)
+
+    def adapt_density(self, desc: KernelDesc, alpha: float, precision=FP32C, outputs=True):
+        """Returns (abw, mass, pilot, g); with outputs=False nothing is copied to the
+        host and the adapted attributes only live on the device."""
+        if not outputs:
+            self._check(self.lib.bbkde_adapt_density(self.h, C.byref(desc), alpha, precision,
+                                                     None, None, None, None))
+            return None
+        n = self.size(REFERENCE)
+        abw, mass, pilot, g = np.empty(max(n, 1)), np.empty(max(n, 1)), np.empty(max(n, 1)), \
+            np.zeros(1)
+        self._check(self.lib.bbkde_adapt_density(self.h, C.byref(desc), alpha, precision,
+                                                 _p(abw), _p(mass), _p(pilot), _p(g)))
+        return abw[:n], mass[:n], pilot[:n], float(g[0])
+
+    def unadapt_density(self):
+        self._check(self.lib.bbkde_unadapt_density(self.h))
+
+    def likelihood_cv(self, desc: KernelDesc, precision=FP32C) -> float:
+        cv = np.zeros(1)
+        self._check(self.lib.bbkde_likelihood_cv(self.h, C.byref(desc), precision, _p(cv)))
+        return float(cv[0])
+
+    def lsq_conv_cv(self, desc: KernelDesc, precision=FP32C) -> float:
+        cv = np.zeros(1)
+        self._check(self.lib.bbkde_lsq_conv_cv(self.h, C.byref(desc), precision, _p(cv)))
+        return float(cv[0])
+
+    def last_launch_stats(self):
+        ms, pairs, launches = C.c_double(), C.c_double(), C.c_int64()
+        self._check(self.lib.bbkde_last_launch_stats(self.h, C.byref(ms), C.byref(pairs),
+                                                     C.byref(launches)))
+        return ms.value, pairs.value, launches.value
+
+    def launch_count(self) -> int:
+        return int(self.lib.bbkde_launch_count(self.h))
+
+    def device_info(self):
+        sm, dev = C.c_int(), C.c_int()
+        self._check(self.lib.bbkde_device_info(self.h, C.byref(sm), C.byref(dev)))
+        return sm.value, dev.value

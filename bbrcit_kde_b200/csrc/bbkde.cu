@@ -1,0 +1,794 @@
+// libbbkde.so: the C ABI declared in include/bbkde.h.
+//
+// Host code for the B200 direct kernel-density path. A context owns one
+// device's buffers and a stream; point sets live in HBM as FP64 SoA columns
+// (x, y, mass, abw, weight) and are packed on the device into per-kernel
+// records (kde_device.cuh) only when the kernel, bandwidth or attributes change.
+// Every call validates its arguments the way the reference does
+// (CudaDirectKde.h:181-190), surfaces every CUDA error as BBKDE_CUDA_ERROR, and
+// synchronises its stream before returning.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "../../include/bbkde.h"
+#include "kde_device.cuh"
+
+using namespace bbkde;
+
+namespace {
+
+struct DevBuf {
+  void *p = nullptr;
+  size_t cap = 0;
+  template <typename T> T *as() const { return static_cast<T *>(p); }
+};
+
+struct PointSet {
+  int dim = 0;
+  int64_t n = 0;
+  DevBuf x, y, mass, abw, weight;   // double columns
+  uint64_t coord_version = 0;       // bumps on upload
+  uint64_t attr_version = 0;        // bumps when mass / abw change
+};
+
+// Resolved kernel: device operator, record scales and normalisation.
+struct Resolved {
+  int op = 0, dim = 0;
+  double h1 = 1, h2 = 1;
+  double c1_f32 = 0, c2_f32 = 0;   // log2-based scale numerators (FP32 records)
+  double c1_f64 = 0, c2_f64 = 0;   // natural-log scale numerators (FP64 records)
+  double mass_scale = 1.0;
+  double norm = 1.0;               // C(h), reference formulas, FP64
+};
+
+struct PackKey {
+  int op = -1, dim = 0;
+  double h1 = 0, h2 = 0, c1 = 0, c2 = 0, ms = 0;
+  uint64_t coord_version = ~0ull, attr_version = ~0ull;
+  bool operator==(const PackKey &o) const {
+    return op == o.op && dim == o.dim && h1 == o.h1 && h2 == o.h2 && c1 == o.c1 &&
+           c2 == o.c2 && ms == o.ms && coord_version == o.coord_version &&
+           attr_version == o.attr_version;
+  }
+};
+
+struct PackCache {
+  PackKey key;
+  DevBuf rec, ext;
+};
+
+struct QueryCache {
+  int set = -1;
+  uint64_t coord_version = ~0ull;
+  DevBuf x, y;
+};
+
+constexpr double kLog2e = 1.4426950408889634074;
+
+}  // namespace
+
+struct bbkde_ctx {
+  int device = 0;
+  int sm_count = 148;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  PointSet sets[2];
+  PackCache pack32, pack64;
+  QueryCache q32, q64;
+  DevBuf partial, out_dev, block_sums, scalars, staging, status;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
+  double last_ms = 0, last_pairs = 0;
+  int64_t last_launches = 0;
+  int64_t launch_total = 0;   // every kernel this context has launched
+  std::string err;
+};
+
+namespace {
+
+int fail(bbkde_ctx *c, int code, const std::string &msg) {
+  if (c) c->err = msg;
+  return code;
+}
+
+#define CUDA_TRY(ctx, call)                                                          \
+  do {                                                                               \
+    cudaError_t e_ = (call);                                                         \
+    if (e_ != cudaSuccess) {                                                         \
+      return fail(ctx, BBKDE_CUDA_ERROR, std::string(#call) + ": " +               \
+                                             cudaGetErrorString(e_));                \
+    }                                                                                \
+  } while (0)
+
+int ensure(bbkde_ctx *c, DevBuf &b, size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  if (b.cap >= bytes) return BBKDE_OK;
+  if (b.p) {
+    cudaFree(b.p);
+    b.p = nullptr;
+    b.cap = 0;
+  }
+  cudaError_t e = cudaMalloc(&b.p, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(c, BBKDE_ALLOC_FAILED,
+                "cudaMalloc(" + std::to_string(bytes) + "): " + cudaGetErrorString(e));
+  }
+  b.cap = bytes;
+  return BBKDE_OK;
+}
+
+void release(DevBuf &b) {
+  if (b.p) cudaFree(b.p);
+  b.p = nullptr;
+  b.cap = 0;
+}
+
+#define TRY(expr)                 \
+  do {                            \
+    int rc_ = (expr);             \
+    if (rc_ != BBKDE_OK) return rc_; \
+  } while (0)
+
+#define COUNT_LAUNCH(c) (++(c)->launch_total)
+
+inline unsigned grid1d(int64_t n, int block = 256) {
+  return (unsigned)std::max<int64_t>(1, (n + block - 1) / block);
+}
+
+// Normalisation C(h) exactly as the reference computes it
+// (include/Kernels/KernelTraits.h; line numbers in oracle/kde_oracle.c).
+double normalization(int kind, int dim, const double *h) {
+  switch (kind) {
+    case BBKDE_GAUSSIAN:
+      if (dim == 1) return 0.3989422804014326779 / (double)(float)h[0];  // float h, :143
+      return 0.1591549430918953357 / (h[0] * h[0]);
+    case BBKDE_EPANECHNIKOV:
+      if (dim == 1) return 0.75 / h[0];
+      return 0.6366197723675813431 / (h[0] * h[0]);
+    case BBKDE_GAUSSIAN_PRODUCT_2D: return 0.1591549430918953357 / (h[0] * h[1]);
+    case BBKDE_EPANECHNIKOV_PRODUCT_2D: return 0.5625 / (h[0] * h[1]);
+    case BBKDE_GAUSSIAN_PRODUCT_CONV_2D: return 0.0795774715459476678 / (h[0] * h[1]);
+    case BBKDE_EPANECHNIKOV_PRODUCT_CONV_2D: return 0.36 / (h[0] * h[1]);
+    case BBKDE_GAUSSIAN_CONV_1D: return 0.2820947917738781434 / h[0];
+    case BBKDE_EPANECHNIKOV_CONV_1D: return 0.6 / h[0];
+  }
+  return 0.0;
+}
+
+int resolve(bbkde_ctx *c, const bbkde_kernel_desc *k, Resolved &r) {
+  if (!k) return fail(c, BBKDE_INVALID_ARGUMENT, "kernel descriptor is NULL");
+  if (k->dim != 1 && k->dim != 2)
+    return fail(c, BBKDE_INVALID_ARGUMENT, "kernel dim must be 1 or 2");
+  const bool product = k->kind == BBKDE_GAUSSIAN_PRODUCT_2D ||
+                       k->kind == BBKDE_EPANECHNIKOV_PRODUCT_2D ||
+                       k->kind == BBKDE_GAUSSIAN_PRODUCT_CONV_2D ||
+                       k->kind == BBKDE_EPANECHNIKOV_PRODUCT_CONV_2D;
+  const bool one_d = k->kind == BBKDE_GAUSSIAN_CONV_1D || k->kind == BBKDE_EPANECHNIKOV_CONV_1D;
+  if (k->kind < 0 || k->kind > BBKDE_EPANECHNIKOV_CONV_1D)
+    return fail(c, BBKDE_INVALID_ARGUMENT, "unknown kernel kind");
+  if (product && k->dim != 2)
+    return fail(c, BBKDE_INVALID_ARGUMENT, "product kernels are 2-D");
+  if (one_d && k->dim != 1)
+    return fail(c, BBKDE_INVALID_ARGUMENT, "1-D convolution kernels need dim 1");
+  const double hx = k->h[0], hy = product ? k->h[1] : k->h[0];
+  if (!(hx > 0) || !(hy > 0) || !std::isfinite(hx) || !std::isfinite(hy))
+    return fail(c, BBKDE_INVALID_ARGUMENT, "bandwidths must be positive and finite");
+  r = Resolved();
+  r.dim = k->dim;
+  r.h1 = hx;
+  r.h2 = hy;
+  r.norm = normalization(k->kind, k->dim, k->h);
+  double g = -0.5;  // exponent factor of the Gaussian family
+  switch (k->kind) {
+    case BBKDE_GAUSSIAN:
+    case BBKDE_GAUSSIAN_PRODUCT_2D:
+      break;
+    case BBKDE_GAUSSIAN_CONV_1D:
+      g = -0.25;
+      break;
+    case BBKDE_GAUSSIAN_PRODUCT_CONV_2D:
+      g = (k->flags & BBKDE_FLAG_EXACT_GAUSS_CONV) ? -0.25 : -0.5;
+      break;
+    default:
+      g = 0.0;
+  }
+  switch (k->kind) {
+    case BBKDE_GAUSSIAN:
+    case BBKDE_GAUSSIAN_CONV_1D:
+    case BBKDE_GAUSSIAN_PRODUCT_2D:
+    case BBKDE_GAUSSIAN_PRODUCT_CONV_2D:
+      // (dx^2/hx^2 + dy^2/hy^2) with hx == hy is the isotropic form.
+      r.op = (hx == hy) ? OP_GAUSS_ISO : OP_GAUSS_PROD;
+      r.c1_f32 = r.c2_f32 = g * kLog2e;
+      r.c1_f64 = r.c2_f64 = g;
+      break;
+    case BBKDE_EPANECHNIKOV:
+      r.op = OP_EPAN_ISO;
+      r.c1_f32 = r.c2_f32 = r.c1_f64 = r.c2_f64 = -1.0;
+      break;
+    case BBKDE_EPANECHNIKOV_PRODUCT_2D:
+      r.op = OP_EPAN_PROD;
+      r.c1_f32 = r.c2_f32 = r.c1_f64 = r.c2_f64 = -1.0;
+      break;
+    case BBKDE_EPANECHNIKOV_PRODUCT_CONV_2D:
+      r.op = OP_EPAN_CONV;
+      r.mass_scale = 1.0 / 1024.0;  // 0.03125 per dimension
+      break;
+    case BBKDE_EPANECHNIKOV_CONV_1D:
+      r.op = OP_EPAN_CONV;
+      r.mass_scale = 1.0 / 32.0;
+      break;
+  }
+  if (k->dim == 1 && r.op == OP_GAUSS_PROD) r.op = OP_GAUSS_ISO;
+  return BBKDE_OK;
+}
+
+int check_ctx(bbkde_ctx *c) {
+  if (!c) return BBKDE_INVALID_ARGUMENT;
+  cudaError_t e = cudaSetDevice(c->device);
+  if (e != cudaSuccess) return fail(c, BBKDE_CUDA_ERROR, cudaGetErrorString(e));
+  return BBKDE_OK;
+}
+
+// Pack the REFERENCE set into records for `r` (cached).
+int ensure_pack(bbkde_ctx *c, const Resolved &r, bool f64) {
+  PointSet &s = c->sets[BBKDE_REFERENCE];
+  PackCache &pc = f64 ? c->pack64 : c->pack32;
+  PackKey key;
+  key.op = r.op;
+  key.dim = r.dim;
+  key.h1 = r.h1;
+  key.h2 = r.h2;
+  key.c1 = f64 ? r.c1_f64 : r.c1_f32;
+  key.c2 = f64 ? r.c2_f64 : r.c2_f32;
+  key.ms = r.mass_scale;
+  key.coord_version = s.coord_version;
+  key.attr_version = s.attr_version;
+  if (pc.key == key) return BBKDE_OK;
+  const int64_t n = std::max<int64_t>(s.n, 1);
+  TRY(ensure(c, pc.rec, (size_t)n * (f64 ? sizeof(double4) : sizeof(float4))));
+  TRY(ensure(c, pc.ext, (size_t)n * (f64 ? sizeof(double) : sizeof(float))));
+  if (s.n > 0) {
+    PackArgs p;
+    p.x = s.x.as<double>();
+    p.y = s.y.as<double>();
+    p.mass = s.mass.as<double>();
+    p.abw = s.abw.as<double>();
+    p.n = s.n;
+    p.op = r.op;
+    p.dim = r.dim;
+    p.c1 = key.c1;
+    p.c2 = key.c2;
+    p.h1 = r.h1;
+    p.h2 = r.h2;
+    p.mass_scale = r.mass_scale;
+    if (f64)
+      k_pack_f64<<<grid1d(s.n), 256, 0, c->stream>>>(p, pc.rec.as<double4>(), pc.ext.as<double>());
+    else
+      k_pack_f32<<<grid1d(s.n), 256, 0, c->stream>>>(p, pc.rec.as<float4>(), pc.ext.as<float>());
+    COUNT_LAUNCH(c);
+    CUDA_TRY(c, cudaGetLastError());
+  }
+  pc.key = key;
+  return BBKDE_OK;
+}
+
+// Query coordinates of `set` (QUERY, or REFERENCE for self-evaluation).
+int ensure_queries(bbkde_ctx *c, int set, bool f64, const void **qx, const void **qy) {
+  PointSet &s = c->sets[set];
+  if (f64) {
+    *qx = s.x.p;
+    *qy = s.dim == 2 ? s.y.p : s.x.p;
+    return BBKDE_OK;
+  }
+  QueryCache &qc = c->q32;
+  if (!(qc.set == set && qc.coord_version == s.coord_version)) {
+    const int64_t n = std::max<int64_t>(s.n, 1);
+    TRY(ensure(c, qc.x, (size_t)n * sizeof(float)));
+    TRY(ensure(c, qc.y, (size_t)n * sizeof(float)));
+    if (s.n > 0) {
+      k_to_f32<<<grid1d(s.n), 256, 0, c->stream>>>(s.x.as<double>(), qc.x.as<float>(), s.n);
+      COUNT_LAUNCH(c);
+      if (s.dim == 2) {
+        k_to_f32<<<grid1d(s.n), 256, 0, c->stream>>>(s.y.as<double>(), qc.y.as<float>(), s.n);
+        COUNT_LAUNCH(c);
+      }
+      CUDA_TRY(c, cudaGetLastError());
+    }
+    qc.set = set;
+    qc.coord_version = s.coord_version;
+  }
+  *qx = qc.x.p;
+  *qy = s.dim == 2 ? qc.y.p : qc.x.p;
+  return BBKDE_OK;
+}
+
+// ---- launch planning ------------------------------------------------------
+
+constexpr int kBlock = 256;
+constexpr int kQpt = 4;
+constexpr int kTile = 256;
+constexpr int kBlock64 = 128;
+
+struct Plan {
+  int64_t nseg = 1, seg_len = 0;
+  unsigned gx = 1;
+};
+
+// Split the reference range into segments so that the grid fills the device
+// with ~16 waves of blocks (load balance through the hardware block scheduler),
+// but never below 512 references per segment.
+Plan plan_launch(const bbkde_ctx *c, int64_t n_ref, int64_t q_count, int q_per_block,
+                 int tile) {
+  Plan p;
+  int64_t qtiles = (q_count + q_per_block - 1) / q_per_block;
+  p.gx = (unsigned)std::max<int64_t>(qtiles, 1);
+  int64_t target = (int64_t)c->sm_count * 4 * 16;
+  int64_t want = (target + qtiles - 1) / std::max<int64_t>(qtiles, 1);
+  int64_t max_seg = std::max<int64_t>(1, (n_ref + 511) / 512);
+  p.nseg = std::min<int64_t>(std::max<int64_t>(want, 1), std::min<int64_t>(max_seg, 65535));
+  p.seg_len = (n_ref + p.nseg - 1) / p.nseg;
+  p.seg_len = (p.seg_len + tile - 1) / tile * tile;
+  p.nseg = std::max<int64_t>(1, (n_ref + p.seg_len - 1) / p.seg_len);
+  return p;
+}
+
+template <int OP, int D>
+void launch_f32(dim3 grid, cudaStream_t st, const SumArgs &a) {
+  k_pair_sum_f32<OP, D, kQpt, kBlock, kTile><<<grid, kBlock, 0, st>>>(a);
+}
+template <int OP, int D>
+void launch_f64(dim3 grid, cudaStream_t st, const SumArgs &a) {
+  k_pair_sum_f64<OP, D, kBlock64><<<grid, kBlock64, 0, st>>>(a);
+}
+
+template <int D>
+void dispatch_op(int op, bool f64, dim3 grid, cudaStream_t st, const SumArgs &a) {
+  switch (op) {
+#define CASE_(OPV)                                         \
+  case OPV:                                                \
+    if (f64) launch_f64<OPV, D>(grid, st, a);              \
+    else launch_f32<OPV, D>(grid, st, a);                  \
+    break;
+    CASE_(OP_GAUSS_ISO)
+    CASE_(OP_GAUSS_PROD)
+    CASE_(OP_EPAN_ISO)
+    CASE_(OP_EPAN_PROD)
+    CASE_(OP_EPAN_CONV)
+#undef CASE_
+  }
+}
+
+// One pair-sum over refs [r_i, r_j] x queries [q_i, q_j] of `qset`; writes
+// scale * sum into out_dev[0 .. q_count). With epi != EPI_NONE also reduces
+// sum_q w[q] * g(out[q]) into c->scalars[0] (FP64, fixed order).
+int pair_sum(bbkde_ctx *c, const Resolved &r, int precision, int qset, int64_t r_i,
+             int64_t r_j, int64_t q_i, int64_t q_j, double scale, bool exclude_self,
+             double *out_dev, int epi, const double *w_dev) {
+  const bool f64 = precision == BBKDE_FP64;
+  TRY(ensure_pack(c, r, f64));
+  const void *qx = nullptr, *qy = nullptr;
+  TRY(ensure_queries(c, qset, f64, &qx, &qy));
+  const int64_t n_ref = r_j - r_i + 1;
+  const int64_t q_count = q_j - q_i + 1;
+  const int qpb = f64 ? kBlock64 : kBlock * kQpt;
+  Plan p = plan_launch(c, n_ref, q_count, qpb, f64 ? kBlock64 : kTile);
+
+  double *partial = out_dev;
+  const bool combine = p.nseg > 1 || epi != EPI_NONE;
+  if (combine) {
+    TRY(ensure(c, c->partial, (size_t)p.nseg * q_count * sizeof(double)));
+    partial = c->partial.as<double>();
+  }
+  SumArgs a;
+  PackCache &pc = f64 ? c->pack64 : c->pack32;
+  a.refs = pc.rec.p;
+  a.extra = pc.ext.p;
+  a.qx = qx;
+  a.qy = qy;
+  a.r_begin = r_i;
+  a.r_end = r_j + 1;
+  a.seg_len = p.seg_len;
+  a.q_begin = q_i;
+  a.q_count = q_count;
+  a.exclude_self = exclude_self ? 1 : 0;
+  a.scale = combine ? 1.0 : scale;
+  a.out = partial;
+  a.status = c->status.as<int>();
+
+  dim3 grid(p.gx, (unsigned)p.nseg);
+  CUDA_TRY(c, cudaEventRecord(c->ev0, c->stream));
+  if (r.dim == 2) dispatch_op<2>(r.op, f64, grid, c->stream, a);
+  else dispatch_op<1>(r.op, f64, grid, c->stream, a);
+  COUNT_LAUNCH(c);
+  CUDA_TRY(c, cudaGetLastError());
+  CUDA_TRY(c, cudaEventRecord(c->ev1, c->stream));
+  int64_t launches = 1;
+  if (combine) {
+    const unsigned nb = grid1d(q_count, kRedBlock);
+    if (epi != EPI_NONE) TRY(ensure(c, c->block_sums, (size_t)nb * sizeof(double)));
+    k_combine<<<nb, kRedBlock, 0, c->stream>>>(partial, (int)p.nseg, q_count, scale, out_dev,
+                                               epi, w_dev, c->block_sums.as<double>());
+    COUNT_LAUNCH(c);
+    CUDA_TRY(c, cudaGetLastError());
+    ++launches;
+    if (epi != EPI_NONE) {
+      k_sum_blocks<<<1, kRedBlock, 0, c->stream>>>(c->block_sums.as<double>(), nb,
+                                                   c->scalars.as<double>());
+      COUNT_LAUNCH(c);
+      CUDA_TRY(c, cudaGetLastError());
+      ++launches;
+    }
+  }
+  CUDA_TRY(c, cudaEventRecord(c->ev2, c->stream));
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  float ms = 0.f;
+  CUDA_TRY(c, cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+  c->last_ms = ms;
+  c->last_pairs = (double)n_ref * (double)q_count;
+  c->last_launches = launches;
+  return BBKDE_OK;
+}
+
+int check_ranges(bbkde_ctx *c, int64_t r_i, int64_t r_j, int64_t q_i, int64_t q_j) {
+  const int64_t nr = c->sets[BBKDE_REFERENCE].n, nq = c->sets[BBKDE_QUERY].n;
+  // CudaDirectKde.h:181-190 (unsigned size_t there; negative indices here are
+  // out of range as well).
+  if (r_j >= nr || q_j >= nq || r_i < 0 || q_i < 0 || r_j < 0 || q_j < 0)
+    return fail(c, BBKDE_OUT_OF_RANGE,
+                "CudaDirectKde<>: unnormalized_eval(): j_r and j_q should be at most "
+                "the number of reference and query points. ");
+  if (r_i > r_j || q_i > q_j)
+    return fail(c, BBKDE_INVALID_ARGUMENT,
+                "CudaDirectKde<>: unnormalized_eval(): must have i_r <= j_r and i_q <= j_q. ");
+  return BBKDE_OK;
+}
+
+int eval_common(bbkde_ctx *c, const bbkde_kernel_desc *k, int64_t r_i, int64_t r_j,
+                int64_t q_i, int64_t q_j, int normalized, int precision, double *out,
+                bool out_is_device) {
+  TRY(check_ctx(c));
+  if (!out) return fail(c, BBKDE_INVALID_ARGUMENT, "output pointer is NULL");
+  if (precision != BBKDE_FP32C && precision != BBKDE_FP64)
+    return fail(c, BBKDE_INVALID_ARGUMENT, "unknown precision");
+  Resolved r;
+  TRY(resolve(c, k, r));
+  TRY(check_ranges(c, r_i, r_j, q_i, q_j));
+  if (c->sets[BBKDE_REFERENCE].dim != r.dim || c->sets[BBKDE_QUERY].dim != r.dim)
+    return fail(c, BBKDE_INVALID_ARGUMENT, "point dimension does not match the kernel");
+  const int64_t q_count = q_j - q_i + 1;
+  double *dst = out;
+  if (!out_is_device) {
+    TRY(ensure(c, c->out_dev, (size_t)q_count * sizeof(double)));
+    dst = c->out_dev.as<double>();
+  }
+  TRY(pair_sum(c, r, precision, BBKDE_QUERY, r_i, r_j, q_i, q_j,
+               normalized ? r.norm : 1.0, false, dst, EPI_NONE, nullptr));
+  if (!out_is_device) {
+    CUDA_TRY(c, cudaMemcpyAsync(out, dst, (size_t)q_count * sizeof(double),
+                                cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  }
+  return BBKDE_OK;
+}
+
+int download(bbkde_ctx *c, double *host, const DevBuf &src, int64_t n) {
+  if (!host || n <= 0) return BBKDE_OK;
+  CUDA_TRY(c, cudaMemcpyAsync(host, src.p, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost,
+                              c->stream));
+  return BBKDE_OK;
+}
+
+int self_checks(bbkde_ctx *c, const bbkde_kernel_desc *k, int precision, Resolved &r) {
+  TRY(check_ctx(c));
+  if (precision != BBKDE_FP32C && precision != BBKDE_FP64)
+    return fail(c, BBKDE_INVALID_ARGUMENT, "unknown precision");
+  TRY(resolve(c, k, r));
+  const PointSet &s = c->sets[BBKDE_REFERENCE];
+  if (s.dim != r.dim && s.n > 0)
+    return fail(c, BBKDE_INVALID_ARGUMENT, "point dimension does not match the kernel");
+  return BBKDE_OK;
+}
+
+int conv_kind_of(int kind, int dim) {
+  if (dim == 1 && kind == BBKDE_GAUSSIAN) return BBKDE_GAUSSIAN_CONV_1D;
+  if (dim == 1 && kind == BBKDE_EPANECHNIKOV) return BBKDE_EPANECHNIKOV_CONV_1D;
+  if (kind == BBKDE_GAUSSIAN_PRODUCT_2D) return BBKDE_GAUSSIAN_PRODUCT_CONV_2D;
+  if (kind == BBKDE_EPANECHNIKOV_PRODUCT_2D) return BBKDE_EPANECHNIKOV_PRODUCT_CONV_2D;
+  return -1;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+int bbkde_abi_version(void) { return BBKDE_ABI_VERSION; }
+
+const char *bbkde_status_string(int s) {
+  switch (s) {
+    case BBKDE_OK: return "ok";
+    case BBKDE_OUT_OF_RANGE: return "out of range";
+    case BBKDE_INVALID_ARGUMENT: return "invalid argument";
+    case BBKDE_CUDA_ERROR: return "CUDA error";
+    case BBKDE_TIMEOUT: return "timeout";
+    case BBKDE_UNSUPPORTED: return "unsupported";
+    case BBKDE_NO_DEVICE: return "no CUDA device";
+    case BBKDE_ALLOC_FAILED: return "device allocation failed";
+  }
+  return "unknown status";
+}
+
+int bbkde_ctx_create(int device, bbkde_ctx **out) {
+  if (!out) return BBKDE_INVALID_ARGUMENT;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return BBKDE_NO_DEVICE;
+  }
+  if (device < 0 || device >= ndev) return BBKDE_INVALID_ARGUMENT;
+  bbkde_ctx *c = new (std::nothrow) bbkde_ctx();
+  if (!c) return BBKDE_ALLOC_FAILED;
+  c->device = device;
+  int rc = BBKDE_OK;
+  do {
+    if (cudaSetDevice(device) != cudaSuccess) { rc = BBKDE_CUDA_ERROR; break; }
+    cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device);
+    if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+      rc = BBKDE_CUDA_ERROR;
+      break;
+    }
+    c->stream = c->own_stream;
+    if (cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
+        cudaEventCreate(&c->ev2) != cudaSuccess) {
+      rc = BBKDE_CUDA_ERROR;
+      break;
+    }
+    if ((rc = ensure(c, c->scalars, 64 * sizeof(double))) != BBKDE_OK) break;
+    if ((rc = ensure(c, c->status, 64)) != BBKDE_OK) break;
+    if (cudaMemset(c->status.p, 0, 64) != cudaSuccess) { rc = BBKDE_CUDA_ERROR; break; }
+  } while (0);
+  if (rc != BBKDE_OK) {
+    cudaGetLastError();
+    bbkde_ctx_destroy(c);
+    return rc;
+  }
+  *out = c;
+  return BBKDE_OK;
+}
+
+int bbkde_ctx_destroy(bbkde_ctx *c) {
+  if (!c) return BBKDE_OK;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  for (auto &s : c->sets) {
+    release(s.x); release(s.y); release(s.mass); release(s.abw); release(s.weight);
+  }
+  release(c->pack32.rec); release(c->pack32.ext);
+  release(c->pack64.rec); release(c->pack64.ext);
+  release(c->q32.x); release(c->q32.y); release(c->q64.x); release(c->q64.y);
+  release(c->partial); release(c->out_dev); release(c->block_sums);
+  release(c->scalars); release(c->staging); release(c->status);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->ev2) cudaEventDestroy(c->ev2);
+  if (c->own_stream) cudaStreamDestroy(c->own_stream);
+  delete c;
+  return BBKDE_OK;
+}
+
+const char *bbkde_ctx_last_error(const bbkde_ctx *c) {
+  return c ? c->err.c_str() : "null context";
+}
+
+int bbkde_ctx_set_stream(bbkde_ctx *c, void *stream) {
+  TRY(check_ctx(c));
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  c->stream = stream ? static_cast<cudaStream_t>(stream) : c->own_stream;
+  return BBKDE_OK;
+}
+
+int bbkde_upload(bbkde_ctx *c, int role, int dim, int64_t n, const double *coords,
+                 const double *mass, const double *abw, const double *weight) {
+  TRY(check_ctx(c));
+  if (role != BBKDE_REFERENCE && role != BBKDE_QUERY)
+    return fail(c, BBKDE_INVALID_ARGUMENT, "role must be REFERENCE or QUERY");
+  if (dim != 1 && dim != 2) return fail(c, BBKDE_INVALID_ARGUMENT, "dim must be 1 or 2");
+  if (n < 0) return fail(c, BBKDE_INVALID_ARGUMENT, "negative point count");
+  if (n > 0 && !coords) return fail(c, BBKDE_INVALID_ARGUMENT, "coords is NULL");
+  PointSet &s = c->sets[role];
+  const size_t nb = (size_t)std::max<int64_t>(n, 1) * sizeof(double);
+  TRY(ensure(c, s.x, nb));
+  TRY(ensure(c, s.y, nb));
+  TRY(ensure(c, s.mass, nb));
+  TRY(ensure(c, s.abw, nb));
+  TRY(ensure(c, s.weight, nb));
+  TRY(ensure(c, c->staging, nb * dim));
+  if (n > 0) {
+    CUDA_TRY(c, cudaMemcpyAsync(c->staging.p, coords, (size_t)n * dim * sizeof(double),
+                                cudaMemcpyHostToDevice, c->stream));
+    k_deinterleave<<<grid1d(n), 256, 0, c->stream>>>(c->staging.as<double>(), dim, n,
+                                                     s.x.as<double>(), s.y.as<double>());
+    COUNT_LAUNCH(c);
+    CUDA_TRY(c, cudaGetLastError());
+    if (mass)
+      CUDA_TRY(c, cudaMemcpyAsync(s.mass.p, mass, nb, cudaMemcpyHostToDevice, c->stream));
+    else
+      k_fill<<<grid1d(n), 256, 0, c->stream>>>(s.mass.as<double>(), 1.0, n), COUNT_LAUNCH(c);
+    if (abw)
+      CUDA_TRY(c, cudaMemcpyAsync(s.abw.p, abw, nb, cudaMemcpyHostToDevice, c->stream));
+    else
+      k_fill<<<grid1d(n), 256, 0, c->stream>>>(s.abw.as<double>(), 1.0, n), COUNT_LAUNCH(c);
+    if (weight)
+      CUDA_TRY(c, cudaMemcpyAsync(s.weight.p, weight, nb, cudaMemcpyHostToDevice, c->stream));
+    else
+      CUDA_TRY(c, cudaMemcpyAsync(s.weight.p, s.mass.p, nb, cudaMemcpyDeviceToDevice,
+                                  c->stream));
+    CUDA_TRY(c, cudaGetLastError());
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  }
+  s.dim = dim;
+  s.n = n;
+  ++s.coord_version;
+  ++s.attr_version;
+  return BBKDE_OK;
+}
+
+int64_t bbkde_size(const bbkde_ctx *c, int role) {
+  if (!c || (role != BBKDE_REFERENCE && role != BBKDE_QUERY)) return -1;
+  return c->sets[role].n;
+}
+
+int bbkde_download_attributes(bbkde_ctx *c, double *mass, double *abw) {
+  TRY(check_ctx(c));
+  const PointSet &s = c->sets[BBKDE_REFERENCE];
+  TRY(download(c, mass, s.mass, s.n));
+  TRY(download(c, abw, s.abw, s.n));
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  return BBKDE_OK;
+}
+
+int bbkde_eval_range(bbkde_ctx *c, const bbkde_kernel_desc *k, int64_t r_i, int64_t r_j,
+                     int64_t q_i, int64_t q_j, int normalized, int precision, double *out,
+                     int64_t block_size) {
+  (void)block_size;
+  return eval_common(c, k, r_i, r_j, q_i, q_j, normalized, precision, out, false);
+}
+
+int bbkde_eval_range_device(bbkde_ctx *c, const bbkde_kernel_desc *k, int64_t r_i,
+                            int64_t r_j, int64_t q_i, int64_t q_j, int normalized,
+                            int precision, double *out_device, int64_t block_size) {
+  (void)block_size;
+  return eval_common(c, k, r_i, r_j, q_i, q_j, normalized, precision, out_device, true);
+}
+
+int bbkde_unadapt_density(bbkde_ctx *c) {
+  TRY(check_ctx(c));
+  PointSet &s = c->sets[BBKDE_REFERENCE];
+  if (s.n > 0) {
+    k_unadapt<<<grid1d(s.n), 256, 0, c->stream>>>(s.weight.as<double>(), s.n,
+                                                  s.abw.as<double>(), s.mass.as<double>());
+    COUNT_LAUNCH(c);
+    CUDA_TRY(c, cudaGetLastError());
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  }
+  ++s.attr_version;
+  return BBKDE_OK;
+}
+
+int bbkde_adapt_density(bbkde_ctx *c, const bbkde_kernel_desc *k, double alpha, int precision,
+                        double *abw_out, double *mass_out, double *pilot_out, double *g_out) {
+  Resolved r;
+  TRY(self_checks(c, k, precision, r));
+  // KernelDensityImpl.h:301-303
+  if (!(alpha >= 0 && alpha <= 1))
+    return fail(c, BBKDE_INVALID_ARGUMENT, "adapt_density: alpha must be between [0, 1]. ");
+  TRY(bbkde_unadapt_density(c));  // :307
+  PointSet &s = c->sets[BBKDE_REFERENCE];
+  if (alpha == 0 || s.n == 0) {    // :311
+    if (g_out) *g_out = NAN;
+    TRY(download(c, abw_out, s.abw, s.n));
+    TRY(download(c, mass_out, s.mass, s.n));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return BBKDE_OK;
+  }
+  // Pilot: all-pairs self-evaluation with the self term (:319-325).
+  TRY(ensure(c, c->out_dev, (size_t)s.n * sizeof(double)));
+  double *pilot = c->out_dev.as<double>();
+  TRY(pair_sum(c, r, precision, BBKDE_REFERENCE, 0, s.n - 1, 0, s.n - 1, r.norm, false, pilot,
+               EPI_W_LOG, s.weight.as<double>()));
+  const double ms = c->last_ms, pairs = c->last_pairs;
+  const int64_t launches = c->last_launches;
+  // g, local bandwidths, masses (:330-353).
+  k_pilot_finalize<<<grid1d(s.n), 256, 0, c->stream>>>(
+      pilot, s.weight.as<double>(), c->scalars.as<double>(), alpha, r.dim, s.n,
+      s.abw.as<double>(), s.mass.as<double>(), c->scalars.as<double>() + 1);
+  COUNT_LAUNCH(c);
+  CUDA_TRY(c, cudaGetLastError());
+  ++s.attr_version;
+  TRY(download(c, pilot_out, c->out_dev, s.n));
+  TRY(download(c, abw_out, s.abw, s.n));
+  TRY(download(c, mass_out, s.mass, s.n));
+  double g = 0;
+  CUDA_TRY(c, cudaMemcpyAsync(&g, c->scalars.as<double>() + 1, sizeof(double),
+                              cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  if (g_out) *g_out = g;
+  c->last_ms = ms;
+  c->last_pairs = pairs;
+  c->last_launches = launches + 1;
+  return BBKDE_OK;
+}
+
+int bbkde_likelihood_cv(bbkde_ctx *c, const bbkde_kernel_desc *k, int precision,
+                        double *cv_out) {
+  Resolved r;
+  TRY(self_checks(c, k, precision, r));
+  if (!cv_out) return fail(c, BBKDE_INVALID_ARGUMENT, "cv_out is NULL");
+  PointSet &s = c->sets[BBKDE_REFERENCE];
+  if (s.n == 0) { *cv_out = 0.0; return BBKDE_OK; }
+  TRY(ensure(c, c->out_dev, (size_t)s.n * sizeof(double)));
+  TRY(pair_sum(c, r, precision, BBKDE_REFERENCE, 0, s.n - 1, 0, s.n - 1, r.norm, true,
+               c->out_dev.as<double>(), EPI_W_LOG, s.weight.as<double>()));
+  CUDA_TRY(c, cudaMemcpy(cv_out, c->scalars.p, sizeof(double), cudaMemcpyDeviceToHost));
+  return BBKDE_OK;
+}
+
+int bbkde_lsq_conv_cv(bbkde_ctx *c, const bbkde_kernel_desc *k, int precision, double *cv_out) {
+  Resolved r;
+  TRY(self_checks(c, k, precision, r));
+  if (!cv_out) return fail(c, BBKDE_INVALID_ARGUMENT, "cv_out is NULL");
+  const int ck = conv_kind_of(k->kind, k->dim);
+  if (ck < 0)
+    return fail(c, BBKDE_UNSUPPORTED, "no convolution kernel is associated with this kernel");
+  bbkde_kernel_desc kc = *k;
+  kc.kind = ck;
+  Resolved rc;
+  TRY(resolve(c, &kc, rc));
+  PointSet &s = c->sets[BBKDE_REFERENCE];
+  if (s.n == 0) { *cv_out = 0.0; return BBKDE_OK; }
+  TRY(ensure(c, c->out_dev, (size_t)s.n * sizeof(double)));
+  double llo = 0, sq = 0;
+  // Leave-one-out term (:162-181).
+  TRY(pair_sum(c, r, precision, BBKDE_REFERENCE, 0, s.n - 1, 0, s.n - 1, r.norm, true,
+               c->out_dev.as<double>(), EPI_W_VALUE, s.weight.as<double>()));
+  CUDA_TRY(c, cudaMemcpy(&llo, c->scalars.p, sizeof(double), cudaMemcpyDeviceToHost));
+  const double ms = c->last_ms;
+  // Square-integral term with the convolution kernel, all pairs (:187-205).
+  TRY(pair_sum(c, rc, precision, BBKDE_REFERENCE, 0, s.n - 1, 0, s.n - 1, rc.norm, false,
+               c->out_dev.as<double>(), EPI_W_VALUE, s.weight.as<double>()));
+  CUDA_TRY(c, cudaMemcpy(&sq, c->scalars.p, sizeof(double), cudaMemcpyDeviceToHost));
+  c->last_ms += ms;
+  c->last_pairs *= 2;
+  *cv_out = sq - 2 * llo;  // :207
+  return BBKDE_OK;
+}
+
+int bbkde_last_launch_stats(const bbkde_ctx *c, double *kernel_ms, double *pairs,
+                            int64_t *launches) {
+  if (!c) return BBKDE_INVALID_ARGUMENT;
+  if (kernel_ms) *kernel_ms = c->last_ms;
+  if (pairs) *pairs = c->last_pairs;
+  if (launches) *launches = c->last_launches;
+  return BBKDE_OK;
+}
+
+int64_t bbkde_launch_count(const bbkde_ctx *c) { return c ? c->launch_total : -1; }
+
+int bbkde_device_info(const bbkde_ctx *c, int *sm_count, int *device) {
+  if (!c) return BBKDE_INVALID_ARGUMENT;
+  if (sm_count) *sm_count = c->sm_count;
+  if (device) *device = c->device;
+  return BBKDE_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,395 @@
+"""Benchmark of the direct kernel-density path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one "step"): the adaptive 2-D product-Gaussian KDE of the reference's
+headline configuration -- 1,000,000 reference points from the seeded bimodal
+mixture, weights U[0.5, 1.5], pilot bandwidth (0.05, 0.05), alpha = 0.5, then the
+adapted density at 1,000,000 uniform queries over [-3, 3]^2:
+  pilot pass  (KernelDensity::adapt_density)   N x N pair evaluations
+  evaluation  (KernelDensity::direct_eval)     M x N pair evaluations
+The unit of work is one pair evaluation ("kernel eval"). Synthetic, seeded data.
+
+Lines printed by rank 0 (one JSON object):
+  value    evals/s with inputs resident in HBM (device-timed, CUDA events on the
+           library's stream, L2 flushed between timed steps, max over ranks).
+  e2e      the same through the C ABI with pinned HOST buffers: every step uploads
+           the points, runs pilot + evaluation and reads the densities back.
+  roofline the pair-sum kernel against the MUFU (ex2) bound: SMs x 16 ex2/clk x clock.
+  cpu_baseline  the reference's own CPU code (oracle/_ref, compiled from its
+           headers) timed on this host's cores on a bounded query sample.
+
+Multi-GPU: one process per GPU (torchrun); queries are independent, so each rank
+evaluates its own query batch against the full reference set with no collective
+in the data path ("scaling": "weak"); timings are reduced with MAX over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = ("2D KDE queries/s (kernel evals/s vs FP32 roofline), direct vs surrogate at "
+          "stated rel err")
+UNIT = "kernel evals/s"
+MUFU_EX2_PER_CLK_PER_SM = 16
+# DRAM bytes per launch of the pair-sum kernel on this workload, from one ncu
+# capture (dram__bytes_read.sum + dram__bytes_write.sum), scaled to a full launch:
+# profiles/pair_sum_f32_gaussiso_1M.md. None until measured.
+TRAFFIC_BYTES_PER_LAUNCH = None
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=1_000_000, help="reference points")
+    ap.add_argument("--m", type=int, default=1_000_000, help="queries per rank")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0,
+                    help="target CPU time of the bounded CPU-baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return {}
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"bbkde_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.f.close()
+        sm, smax, power, reasons = [], [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+                power.append(float(parts[3]))
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        os.unlink(self.path)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax),
+                "power_w_max": max(power), "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def l2_flush(torch, buf):
+    buf.zero_()   # 256 MB write > 126 MB L2
+
+
+def cpu_reference_rate(wl, seconds: float, kind_pref: str = "reference"):
+    """evals/s of the reference's CPU direct_eval on a bounded query sample."""
+    from oracle.pyoracle import Oracle, Reference, nthreads_default
+    threads = nthreads_default()
+    n = len(wl.refs)
+    if kind_pref == "reference" and Reference.available():
+        ref = Reference()
+        handle = ref.create(wl.kind, 2, wl.h, wl.refs, wl.weights)
+        run = lambda q: ref.direct(handle, q, nthreads=threads)  # noqa: E731
+        kind = "reference"
+        cleanup = lambda: ref.destroy(handle)  # noqa: E731
+    else:
+        orc = Oracle()
+        wn = wl.weights / wl.weights.sum()
+        run = lambda q: orc.direct(wl.kind, 2, wl.h, wl.refs, wn, q, nthreads=threads)  # noqa
+        kind = "port"
+        cleanup = lambda: None  # noqa: E731
+    # size the sample from a short probe
+    probe = max(threads, 8)
+    t0 = time.perf_counter()
+    run(wl.queries[:probe])
+    dt = time.perf_counter() - t0
+    per_q = dt / probe
+    m = int(min(len(wl.queries), max(probe, seconds / max(per_q, 1e-9))))
+    t0 = time.perf_counter()
+    run(wl.queries[:m])
+    dt = time.perf_counter() - t0
+    cleanup()
+    return {"value": m * n / dt, "unit": UNIT, "cores": threads, "kind": kind,
+            "sample": f"direct_eval of {m} queries x {n} refs "
+                      f"(GaussianProductKernel2d<double>, same per-pair code as the pilot "
+                      f"pass), {threads} host threads, {dt:.1f} s"}
+
+
+def run_reference_arm(a, world, rank):
+    if rank != 0:
+        return 0
+    from bbrcit_kde_b200 import workloads as W
+    wl = W.config2(n=a.n, m=a.m)
+    per_step = max(1.0, a.cpu_seconds / 4)
+    rates = []
+    base = None
+    for i in range(a.warmup + a.steps):
+        r = cpu_reference_rate(wl, per_step)
+        if i >= a.warmup:
+            rates.append(r["value"])
+        base = r
+    value = float(np.median(rates))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": 2.0 * a.n * a.m / value * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded splitmix64 bimodal mixture)",
+        "config": workload_config(a),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": base["cores"],
+                         "kind": base["kind"], "sample": base["sample"]},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def workload_config(a):
+    return {
+        "workload": f"adaptive 2-D product-Gaussian KDE, pilot + evaluation: N={a.n} refs "
+                    f"(bimodal mixture, weights U[0.5,1.5]), M={a.m} uniform queries on "
+                    f"[-3,3]^2 per rank, h=(0.05,0.05), alpha=0.5",
+        "n_ref": a.n, "n_query_per_rank": a.m, "kernel": "GaussianProductKernel2d",
+        "h": [0.05, 0.05], "alpha": 0.5, "precision": "FP32C (FP32 Kahan, FP64 combine)",
+        "evals_per_step_per_rank": 2 * a.n * a.m,
+        "l2": "flushed between timed steps (256 MB write)",
+        "parallelism": "queries sharded across ranks, refs replicated" if a.gpus > 1 else "1 GPU",
+    }
+
+
+def main():
+    a = parse()
+    world, rank, local = dist_env()
+    if a.impl == "reference":
+        return run_reference_arm(a, world, rank)
+
+    import torch
+    import bbrcit_kde_b200 as bk
+    from bbrcit_kde_b200 import workloads as W
+    from bbrcit_kde_b200.parity import error_stats
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    wl = W.config2(n=a.n, m=a.m)
+    if rank > 0:   # each rank its own query batch
+        rng = W.SplitMix64(W.SEED_BASE + 200 + rank)
+        wl.queries = W.f32(rng.uniform(2 * a.m, -3.0, 3.0).reshape(a.m, 2))
+    wn = wl.weights / wl.weights.sum()
+    n, m = len(wl.refs), len(wl.queries)
+    evals_per_step = 2.0 * n * m
+
+    stream = torch.cuda.Stream()   # a real (non-null) stream shared with the library
+    torch.cuda.set_stream(stream)
+    ctx = bk.Context(local)
+    ctx.set_stream(stream.cuda_stream)
+    sm_count, _ = ctx.device_info()
+    desc = bk.kernel_desc(wl.kind, 2, wl.h)
+    out = torch.empty(m, dtype=torch.float64, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    # ---- device-resident timing ------------------------------------------
+    ctx.upload(bk.REFERENCE, wl.refs, mass=wn, weight=wn)
+    ctx.upload(bk.QUERY, wl.queries)
+
+    def step():
+        ctx.adapt_density(desc, wl.alpha, bk.FP32C, outputs=False)
+        pilot_stats = ctx.last_launch_stats()
+        ctx.eval_range_device(desc, 0, n - 1, 0, m - 1, out.data_ptr(), True, bk.FP32C)
+        return pilot_stats, ctx.last_launch_stats()
+
+    for _ in range(a.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    launches0 = ctx.launch_count()
+    step_ms, kernel_launches = [], []
+    for _ in range(a.steps):
+        l2_flush(torch, flush)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        s1, s2 = step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        step_ms.append(e0.elapsed_time(e1))
+        kernel_launches += [s1, s2]
+    launches = ctx.launch_count() - launches0
+    clocks = sampler.stop()
+    total_ms = sum(step_ms)
+    if dist:
+        t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        dist.barrier()
+    value = evals_per_step * a.steps * world / (total_ms / 1e3)
+
+    # roofline of the pair-sum kernel (pilot and evaluation launches)
+    ach = [p / (ms / 1e3) for ms, p, _ in kernel_launches if ms > 0]
+    achieved = float(np.mean(ach))
+    kernel_ms = float(np.mean([ms for ms, _, _ in kernel_launches]))
+    peaks = measured_peaks()
+    sm_max = float(peaks.get("sm_max_mhz") or clocks.get("sm_max_mhz") or 1965.0)
+    peak = sm_count * MUFU_EX2_PER_CLK_PER_SM * sm_max * 1e6
+    observed = clocks.get("sm_mhz")
+    roofline = {
+        "bound": "sfu", "achieved": achieved / 1e9, "peak": peak / 1e9, "unit": "Geval/s",
+        "frac": achieved / peak,
+        "peak_basis": f"{sm_count} SMs x {MUFU_EX2_PER_CLK_PER_SM} MUFU ex2/clk x "
+                      f"{sm_max:.0f} MHz (sm_max_mhz, MEASURED_PEAKS.json); one ex2 per "
+                      f"pair evaluation",
+        "frac_at_observed_clock": (achieved / (sm_count * MUFU_EX2_PER_CLK_PER_SM * observed
+                                               * 1e6)) if observed else None,
+        "kernel_ms_per_launch": kernel_ms,
+        "pairs_per_launch": float(kernel_launches[0][1]),
+        "traffic": TRAFFIC_BYTES_PER_LAUNCH,
+        "hbm_gbs_peak": peaks.get("hbm_gbs"),
+    }
+
+    # ---- error vs FP64 (outside the timed region) -----------------------
+    sl = slice(m // 2, m // 2 + 4096)
+    ctx.adapt_density(desc, wl.alpha, bk.FP32C, outputs=False)
+    f32 = ctx.eval_range(desc, 0, n - 1, sl.start, sl.stop - 1, True, bk.FP32C)
+    abw64, mass64, _, _ = ctx.adapt_density(desc, wl.alpha, bk.FP64)
+    f64 = ctx.eval_range(desc, 0, n - 1, sl.start, sl.stop - 1, True, bk.FP64)
+    err = error_stats(f32, f64)
+    err_def = ("vs FP64 device path (pilot + eval in FP64) on 4096 queries; pass = "
+               "approximately_equal(rel 1e-6, abs 1e-8) as FloatUtils.h:49-61")
+    oracle_check = None
+    if rank == 0:
+        from oracle.pyoracle import Oracle
+        orc = Oracle()
+        want = orc.direct(wl.kind, 2, wl.h, wl.refs, mass64, wl.queries[sl][:64], abw=abw64)
+        oracle_check = error_stats(f64[:64], want, 1e-10, 0.0)["pass_rate"]
+
+    # ---- end to end through the C ABI with host buffers -----------------
+    e2e = None
+    if not a.no_e2e:
+        pin = lambda arr: torch.from_numpy(np.ascontiguousarray(arr)).pin_memory().numpy()  # noqa
+        h_refs, h_w, h_q = pin(wl.refs), pin(wn), pin(wl.queries)
+        h_out = pin(np.empty(m))
+
+        def e2e_step():
+            ctx.upload(bk.REFERENCE, h_refs, mass=h_w, weight=h_w)
+            ctx.upload(bk.QUERY, h_q)
+            ctx.adapt_density(desc, wl.alpha, bk.FP32C, outputs=False)
+            ctx.eval_range(desc, 0, n - 1, 0, m - 1, True, bk.FP32C, out=h_out)
+
+        for _ in range(a.warmup):
+            e2e_step()
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        e2e_ms = []
+        for _ in range(a.steps):
+            l2_flush(torch, flush)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            e2e_step()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            e2e_ms.append(e0.elapsed_time(e1))
+        tot = sum(e2e_ms)
+        if dist:
+            t = torch.tensor([tot], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            tot = float(t.item())
+        h2d = h_refs.nbytes + 2 * h_w.nbytes + h_q.nbytes
+        d2h = h_out.nbytes
+        e2e = {"value": evals_per_step * a.steps * world / (tot / 1e3), "unit": UNIT,
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        cpu = cpu_reference_rate(wl, a.cpu_seconds)
+
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": total_ms / a.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded splitmix64 bimodal mixture, float32-representable)",
+        "config": workload_config(a),
+        "queries_per_s": value / n / 2.0,
+        "e2e": e2e,
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "clocks": clocks,
+        "gpu_launches": int(launches),
+        "error_vs_fp64": {**err, "definition": err_def,
+                          "fp64_vs_cpu_oracle_pass_rate": oracle_check},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,198 @@
+/* bbkde.h -- C ABI of the B200 direct kernel-density library (libbbkde.so).
+ *
+ * This is the drop-in boundary for bbrcit_kde's direct N-body density path. Every
+ * entry point below replaces one piece of the reference's CudaDirectKde<> /
+ * KernelDensity<> path (file:line cited per function; paths are relative to the
+ * reference project root). Signatures use plain pointers and sizes only.
+ *
+ * Conventions
+ *   - Every call returns an int status (bbkde_status). BBKDE_OK is 0. On failure
+ *     bbkde_ctx_last_error() holds a message.
+ *   - Calls are synchronous from the caller's point of view: when a call returns,
+ *     host outputs are written and device work for the call has finished.
+ *   - Host arrays are caller-owned; the library copies what it needs.
+ *   - Coordinates are AoS with stride `dim` (x0,y0,x1,y1,... for dim 2).
+ *   - Index ranges are closed intervals [i, j], as in the reference.
+ *   - One context per host thread; distinct contexts may be used concurrently.
+ */
+#ifndef BBKDE_H_
+#define BBKDE_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BBKDE_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define BBKDE_API __attribute__((visibility("default")))
+#else
+#define BBKDE_API
+#endif
+
+typedef struct bbkde_ctx bbkde_ctx;
+
+/* Status codes. The C++ wrapper (include/bbkde/) maps OUT_OF_RANGE to
+ * std::out_of_range and INVALID_ARGUMENT to std::invalid_argument, as the
+ * reference throws them (CudaDirectKde.h:181-190, KernelDensityImpl.h:301-303). */
+typedef enum {
+  BBKDE_OK = 0,
+  BBKDE_OUT_OF_RANGE = 1,
+  BBKDE_INVALID_ARGUMENT = 2,
+  BBKDE_CUDA_ERROR = 3,
+  BBKDE_TIMEOUT = 4,
+  BBKDE_UNSUPPORTED = 5,
+  BBKDE_NO_DEVICE = 6,
+  BBKDE_ALLOC_FAILED = 7
+} bbkde_status;
+
+/* Kernel families (include/Kernels/*.h in the reference). */
+typedef enum {
+  BBKDE_GAUSSIAN = 0,                   /* GaussianKernel<D,T>, D = 1, 2 */
+  BBKDE_EPANECHNIKOV = 1,               /* EpanechnikovKernel<D,T>, D = 1, 2 */
+  BBKDE_GAUSSIAN_PRODUCT_2D = 2,        /* GaussianProductKernel2d<T> */
+  BBKDE_EPANECHNIKOV_PRODUCT_2D = 3,    /* EpanechnikovProductKernel2d<T> */
+  BBKDE_GAUSSIAN_PRODUCT_CONV_2D = 4,   /* GaussianProductConvKernel2d<T> */
+  BBKDE_EPANECHNIKOV_PRODUCT_CONV_2D = 5,/* EpanechnikovProductConvKernel2d<T> */
+  BBKDE_GAUSSIAN_CONV_1D = 6,           /* GaussianConvKernel1d<T> */
+  BBKDE_EPANECHNIKOV_CONV_1D = 7        /* EpanechnikovConvKernel1d<T> */
+} bbkde_kernel_kind;
+
+/* Arithmetic of the pair sum.
+ *   FP32C: FP32 kernel evaluation (MUFU ex2 for the Gaussians), Kahan-compensated
+ *          FP32 partial sums, FP64 cross-block combination and normalisation.
+ *   FP64 : FP64 throughout (the reference's CPU arithmetic). */
+typedef enum { BBKDE_FP32C = 0, BBKDE_FP64 = 1 } bbkde_precision;
+
+/* Which point set an upload fills: the reference points of CudaDirectKde<>
+ * (ref_pts) or its query points (query_pts), CudaDirectKde.h:57-59. */
+typedef enum { BBKDE_REFERENCE = 0, BBKDE_QUERY = 1 } bbkde_role;
+
+/* Kernel descriptor flags. */
+enum {
+  /* GaussianProductConvKernel2d: the reference's float/double specialisations
+   * evaluate exp(-0.5 arg) (KernelTraits.h:431-433, :444-446) although the
+   * convolution of two Gaussians is exp(-0.25 arg) (KernelTraits.h:418-420).
+   * By default the library reproduces the reference; this flag selects -0.25. */
+  BBKDE_FLAG_EXACT_GAUSS_CONV = 1
+};
+
+typedef struct {
+  int32_t kind;      /* bbkde_kernel_kind */
+  int32_t dim;       /* 1 or 2 */
+  double h[2];       /* bandwidth (h[0]) or (hx, hy) for the 2-D product kernels */
+  int32_t flags;     /* BBKDE_FLAG_* */
+  int32_t reserved;  /* must be 0 */
+} bbkde_kernel_desc;
+
+/* ---- library / context ------------------------------------------------- */
+
+BBKDE_API int bbkde_abi_version(void);
+BBKDE_API const char *bbkde_status_string(int status);
+
+/* Create a context on CUDA device `device`. The context owns its device buffers
+ * and a non-blocking stream. Replaces the implicit device state of
+ * CudaDirectKde<> (CudaDirectKde.h:109-116). */
+BBKDE_API int bbkde_ctx_create(int device, bbkde_ctx **out);
+BBKDE_API int bbkde_ctx_destroy(bbkde_ctx *ctx);
+BBKDE_API const char *bbkde_ctx_last_error(const bbkde_ctx *ctx);
+
+/* Run the context's work on `stream` (a cudaStream_t), or on its own stream
+ * when `stream` is NULL. */
+BBKDE_API int bbkde_ctx_set_stream(bbkde_ctx *ctx, void *stream);
+
+/* ---- point sets ---------------------------------------------------------- */
+
+/* Upload n points of dimension dim into the REFERENCE or QUERY set, replacing it.
+ * Replaces CudaDirectKde(ref_pts, query_pts) / alloc_copy_host_dev_points
+ * (CudaDirectKde.h:330-374), which copies {x, y, mass, abw} per point
+ * (Point2d.h:31-38). Any of mass / abw / weight may be NULL: mass defaults to 1,
+ * abw to 1, weight to mass. Weights are only used by bbkde_adapt_density and the
+ * cross-validation calls (the `weight` attribute, AdaKdeAttributes.h:36-37).
+ * n == 0 empties the set. */
+BBKDE_API int bbkde_upload(bbkde_ctx *ctx, int role, int dim, int64_t n, const double *coords,
+                 const double *mass, const double *abw, const double *weight);
+
+/* Number of points in a set (CudaDirectKde::reference_size / query_size,
+ * CudaDirectKde.h:290-297). Returns -1 on a bad context or role. */
+BBKDE_API int64_t bbkde_size(const bbkde_ctx *ctx, int role);
+
+/* Copy the REFERENCE set's current mass and abw back to the host (either may be
+ * NULL). After bbkde_adapt_density these are the adapted values. */
+BBKDE_API int bbkde_download_attributes(bbkde_ctx *ctx, double *mass, double *abw);
+
+/* ---- direct evaluation --------------------------------------------------- */
+
+/* For every query k in [q_i, q_j]:
+ *   out[k - q_i] = [C(h) *] sum_{r in [r_i, r_j]} mass_r * U(q_k, x_r; h * abw_r)
+ * Replaces CudaDirectKde::eval (normalized = 1) and unnormalized_eval
+ * (normalized = 0), CudaDirectKde.h:176-229, and the eval_kernel launch inside it
+ * (:126-173). Closed ranges; j >= size gives OUT_OF_RANGE and i > j gives
+ * INVALID_ARGUMENT, as the reference's checks (:181-190). `out` is host memory
+ * of length q_j - q_i + 1. `block_size` is accepted as a tuning hint, as in the
+ * reference (0 = automatic). */
+BBKDE_API int bbkde_eval_range(bbkde_ctx *ctx, const bbkde_kernel_desc *kernel, int64_t r_i,
+                     int64_t r_j, int64_t q_i, int64_t q_j, int normalized,
+                     int precision, double *out, int64_t block_size);
+
+/* As bbkde_eval_range, but `out_device` is device memory on the context's device
+ * (for callers that keep results on the GPU). */
+BBKDE_API int bbkde_eval_range_device(bbkde_ctx *ctx, const bbkde_kernel_desc *kernel,
+                            int64_t r_i, int64_t r_j, int64_t q_i, int64_t q_j,
+                            int normalized, int precision, double *out_device,
+                            int64_t block_size);
+
+/* ---- adaptive densities (Silverman 5.3) ---------------------------------- */
+
+/* KernelDensity::adapt_density(alpha) (KernelDensityImpl.h:291-359) over the
+ * REFERENCE set with exact direct sums: pilot_i = C sum_j w_j U(x_i, x_j; h)
+ * (self term included, abw = 1), g = exp(sum_i w_i log pilot_i),
+ * abw_i = (pilot_i / g)^-alpha, mass_i = w_i abw_i^-dim. The adapted abw and
+ * mass replace the set's attributes on the device. Weights are used as given
+ * (KernelDensity normalises them to sum 1 before this call). alpha outside
+ * [0, 1] returns INVALID_ARGUMENT; alpha == 0 resets abw = 1, mass = w.
+ * Any output pointer may be NULL (host memory, length n, or one double for g). */
+BBKDE_API int bbkde_adapt_density(bbkde_ctx *ctx, const bbkde_kernel_desc *kernel, double alpha,
+                        int precision, double *abw_out, double *mass_out,
+                        double *pilot_out, double *g_out);
+
+/* KernelDensity::unadapt_density (KernelDensityImpl.h:254-273): abw = 1, mass = w. */
+BBKDE_API int bbkde_unadapt_density(bbkde_ctx *ctx);
+
+/* ---- cross-validation ---------------------------------------------------- */
+
+/* KernelDensity::likelihood_cross_validate (KernelDensityImpl.h:215-252) with
+ * exact sums over the REFERENCE set: sum_i w_i log(f_i), where f_i is the
+ * leave-one-out density C sum_{j != i} m_j U(x_i, x_j; h abw_j). The diagonal is
+ * excluded rather than subtracted; see the design notes. */
+BBKDE_API int bbkde_likelihood_cv(bbkde_ctx *ctx, const bbkde_kernel_desc *kernel, int precision,
+                        double *cv_out);
+
+/* KernelDensity::lsq_convolution_cross_validate (KernelDensityImpl.h:142-209):
+ * sum_i w_i fconv_i - 2 sum_i w_i f_i, fconv the all-pairs sum with the
+ * kernel's convolution kernel (ConvKernelAssociator.h). Defined for GAUSSIAN
+ * and EPANECHNIKOV with dim 1, and for the two 2-D product kernels. */
+BBKDE_API int bbkde_lsq_conv_cv(bbkde_ctx *ctx, const bbkde_kernel_desc *kernel, int precision,
+                      double *cv_out);
+
+/* ---- introspection ------------------------------------------------------- */
+
+/* Device time (ms, CUDA events on the launching stream) and pair count of the
+ * most recent pair-sum kernel launch sequence made by this context. */
+BBKDE_API int bbkde_last_launch_stats(const bbkde_ctx *ctx, double *kernel_ms, double *pairs,
+                            int64_t *launches);
+
+/* Total number of kernels this context has launched since it was created
+ * (-1 for a NULL context). */
+BBKDE_API int64_t bbkde_launch_count(const bbkde_ctx *ctx);
+
+/* Number of SMs and the device's ordinal (for callers that size their work). */
+BBKDE_API int bbkde_device_info(const bbkde_ctx *ctx, int *sm_count, int *device);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BBKDE_H_ */
