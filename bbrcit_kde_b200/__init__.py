@@ -35,7 +35,7 @@ EXPORTED = [
     "bbkde_download_attributes", "bbkde_eval_range", "bbkde_eval_range_device",
     "bbkde_adapt_density", "bbkde_unadapt_density", "bbkde_likelihood_cv",
     "bbkde_lsq_conv_cv", "bbkde_last_launch_stats", "bbkde_launch_count",
-    "bbkde_device_info",
+    "bbkde_device_info", "bbkde_ctx_set_launch_variant", "bbkde_launch_variants",
 ]
 
 
@@ -110,6 +110,8 @@ def load_library(path: str = LIB_PATH):
     lib.bbkde_last_launch_stats.argtypes = [vp, _dp, _dp, C.POINTER(i64)]
     lib.bbkde_launch_count.restype = i64
     lib.bbkde_launch_count.argtypes = [vp]
+    lib.bbkde_ctx_set_launch_variant.argtypes = [vp, C.c_int]
+    lib.bbkde_launch_variants.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     lib.bbkde_device_info.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     _lib = lib
     return lib
@@ -237,6 +239,15 @@ class Context:
 
     def launch_count(self) -> int:
         return int(self.lib.bbkde_launch_count(self.h))
+
+    def set_launch_variant(self, variant: int):
+        """-1 = autotune (default); 0..n-1 forces a launch shape."""
+        self._check(self.lib.bbkde_ctx_set_launch_variant(self.h, variant))
+
+    def launch_variants(self):
+        n, last = C.c_int(), C.c_int()
+        self._check(self.lib.bbkde_launch_variants(self.h, C.byref(n), C.byref(last)))
+        return n.value, last.value
 
     def device_info(self):
         sm, dev = C.c_int(), C.c_int()

@@ -13,8 +13,10 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <new>
 #include <string>
+#include <tuple>
 
 #include "../../include/bbkde.h"
 #include "kde_device.cuh"
@@ -86,6 +88,10 @@ struct bbkde_ctx {
   double last_ms = 0, last_pairs = 0;
   int64_t last_launches = 0;
   int64_t launch_total = 0;   // every kernel this context has launched
+  int forced_variant = -1;    // -1: autotune
+  int last_variant = -1;
+  // autotuner cache: (op, dim, exclude_self, log2 refs, log2 queries) -> variant
+  std::map<std::tuple<int, int, int, int, int>, int> tuned;
   std::string err;
 };
 
@@ -311,10 +317,25 @@ int ensure_queries(bbkde_ctx *c, int set, bool f64, const void **qx, const void 
 
 // ---- launch planning ------------------------------------------------------
 
-constexpr int kBlock = 256;
-constexpr int kQpt = 4;
+// Launch shapes of the FP32 pair-sum kernels. The autotuner times them on a
+// slice of the actual problem and keeps the fastest per problem class.
+struct Variant {
+  int qpt;     // queries per thread
+  int block;   // threads per block
+  int minb;    // __launch_bounds__ minimum resident blocks per SM
+};
+constexpr Variant kVariants[] = {{8, 256, 2}, {4, 256, 3}, {8, 128, 4}, {4, 128, 6}};
+constexpr int kNumVariants = 4;
+constexpr int kDefaultVariant = 0;
 constexpr int kTile = 256;
 constexpr int kBlock64 = 128;
+// Problems below this many pairs skip autotuning (launch-latency bound anyway).
+constexpr double kAutotuneMinPairs = 2.0e10;
+
+inline int queries_per_block(int variant, bool f64) {
+  if (f64) return kBlock64;
+  return kVariants[variant].qpt * kVariants[variant].block;
+}
 
 struct Plan {
   int64_t nseg = 1, seg_len = 0;
@@ -339,9 +360,22 @@ Plan plan_launch(const bbkde_ctx *c, int64_t n_ref, int64_t q_count, int q_per_b
   return p;
 }
 
+template <int OP, int D, int QPT, int BLOCK, int MINB>
+void launch_shape(dim3 grid, cudaStream_t st, const SumArgs &a) {
+  if constexpr (op_packed(OP))
+    k_pair_sum_f32x2<OP, D, QPT, BLOCK, kTile, MINB><<<grid, BLOCK, 0, st>>>(a);
+  else
+    k_pair_sum_f32<OP, D, QPT, BLOCK, kTile, MINB><<<grid, BLOCK, 0, st>>>(a);
+}
+
 template <int OP, int D>
-void launch_f32(dim3 grid, cudaStream_t st, const SumArgs &a) {
-  k_pair_sum_f32<OP, D, kQpt, kBlock, kTile><<<grid, kBlock, 0, st>>>(a);
+void launch_f32(int variant, dim3 grid, cudaStream_t st, const SumArgs &a) {
+  switch (variant) {
+    case 0: launch_shape<OP, D, 8, 256, 2>(grid, st, a); break;
+    case 1: launch_shape<OP, D, 4, 256, 3>(grid, st, a); break;
+    case 2: launch_shape<OP, D, 8, 128, 4>(grid, st, a); break;
+    default: launch_shape<OP, D, 4, 128, 6>(grid, st, a); break;
+  }
 }
 template <int OP, int D>
 void launch_f64(dim3 grid, cudaStream_t st, const SumArgs &a) {
@@ -349,12 +383,12 @@ void launch_f64(dim3 grid, cudaStream_t st, const SumArgs &a) {
 }
 
 template <int D>
-void dispatch_op(int op, bool f64, dim3 grid, cudaStream_t st, const SumArgs &a) {
+void dispatch_op(int op, bool f64, int variant, dim3 grid, cudaStream_t st, const SumArgs &a) {
   switch (op) {
 #define CASE_(OPV)                                         \
   case OPV:                                                \
     if (f64) launch_f64<OPV, D>(grid, st, a);              \
-    else launch_f32<OPV, D>(grid, st, a);                  \
+    else launch_f32<OPV, D>(variant, grid, st, a);         \
     break;
     CASE_(OP_GAUSS_ISO)
     CASE_(OP_GAUSS_PROD)
@@ -363,6 +397,86 @@ void dispatch_op(int op, bool f64, dim3 grid, cudaStream_t st, const SumArgs &a)
     CASE_(OP_EPAN_CONV)
 #undef CASE_
   }
+}
+
+inline int ilog2(int64_t v) {
+  int r = 0;
+  while (v > 1) { v >>= 1; ++r; }
+  return r;
+}
+
+// Fill SumArgs and launch one pair-sum kernel over [r_i, r_j] x [q_i, q_j].
+int launch_pair_sum(bbkde_ctx *c, const Resolved &r, bool f64, int variant, const void *qx,
+                    const void *qy, int64_t r_i, int64_t r_j, int64_t q_i, int64_t q_j,
+                    bool exclude_self, double scale, double *out, int64_t *nseg_out) {
+  const int64_t n_ref = r_j - r_i + 1;
+  const int64_t q_count = q_j - q_i + 1;
+  Plan p = plan_launch(c, n_ref, q_count, queries_per_block(variant, f64),
+                       f64 ? kBlock64 : kTile);
+  PackCache &pc = f64 ? c->pack64 : c->pack32;
+  SumArgs a;
+  a.refs = pc.rec.p;
+  a.extra = pc.ext.p;
+  a.qx = qx;
+  a.qy = qy;
+  a.r_begin = r_i;
+  a.r_end = r_j + 1;
+  a.seg_len = p.seg_len;
+  a.q_begin = q_i;
+  a.q_count = q_count;
+  a.exclude_self = exclude_self ? 1 : 0;
+  a.scale = scale;
+  a.out = out;
+  a.status = c->status.as<int>();
+  if (nseg_out) *nseg_out = p.nseg;
+  if (!out) return BBKDE_OK;   // planning only
+  dim3 grid(p.gx, (unsigned)p.nseg);
+  if (r.dim == 2) dispatch_op<2>(r.op, f64, variant, grid, c->stream, a);
+  else dispatch_op<1>(r.op, f64, variant, grid, c->stream, a);
+  COUNT_LAUNCH(c);
+  CUDA_TRY(c, cudaGetLastError());
+  return BBKDE_OK;
+}
+
+// Pick the FP32 launch shape: forced, cached, or timed on a slice of the problem
+// (up to 131072 queries x 262144 references, every variant twice, fastest kept).
+int choose_variant(bbkde_ctx *c, const Resolved &r, const void *qx, const void *qy,
+                   int64_t r_i, int64_t r_j, int64_t q_i, int64_t q_j, bool exclude_self,
+                   int *variant) {
+  if (c->forced_variant >= 0) { *variant = c->forced_variant; return BBKDE_OK; }
+  const double pairs = (double)(r_j - r_i + 1) * (double)(q_j - q_i + 1);
+  if (pairs < kAutotuneMinPairs) { *variant = kDefaultVariant; return BBKDE_OK; }
+  auto key = std::make_tuple(r.op, r.dim, exclude_self ? 1 : 0, ilog2(r_j - r_i + 1),
+                             ilog2(q_j - q_i + 1));
+  auto it = c->tuned.find(key);
+  if (it != c->tuned.end()) { *variant = it->second; return BBKDE_OK; }
+  const int64_t sq_j = std::min<int64_t>(q_j, q_i + 131072 - 1);
+  const int64_t sr_j = std::min<int64_t>(r_j, r_i + 262144 - 1);
+  int64_t need = 0;
+  for (int v = 0; v < kNumVariants; ++v) {
+    int64_t nseg = 0;
+    TRY(launch_pair_sum(c, r, false, v, qx, qy, r_i, sr_j, q_i, sq_j, exclude_self, 1.0,
+                        nullptr, &nseg));
+    need = std::max<int64_t>(need, nseg * (sq_j - q_i + 1));
+  }
+  TRY(ensure(c, c->partial, (size_t)need * sizeof(double)));
+  float best_ms = 0.f;
+  int best = kDefaultVariant;
+  for (int v = 0; v < kNumVariants; ++v) {
+    float ms = 0.f;
+    for (int rep = 0; rep < 2; ++rep) {
+      CUDA_TRY(c, cudaEventRecord(c->ev0, c->stream));
+      TRY(launch_pair_sum(c, r, false, v, qx, qy, r_i, sr_j, q_i, sq_j, exclude_self, 1.0,
+                          c->partial.as<double>(), nullptr));
+      CUDA_TRY(c, cudaEventRecord(c->ev1, c->stream));
+      CUDA_TRY(c, cudaEventSynchronize(c->ev1));
+      CUDA_TRY(c, cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    }
+    if (v == 0 || ms < best_ms) { best_ms = ms; best = v; }
+  }
+  c->tuned[key] = best;
+  *variant = best;
+  return BBKDE_OK;
 }
 
 // One pair-sum over refs [r_i, r_j] x queries [q_i, q_j] of `qset`; writes
@@ -377,43 +491,26 @@ int pair_sum(bbkde_ctx *c, const Resolved &r, int precision, int qset, int64_t r
   TRY(ensure_queries(c, qset, f64, &qx, &qy));
   const int64_t n_ref = r_j - r_i + 1;
   const int64_t q_count = q_j - q_i + 1;
-  const int qpb = f64 ? kBlock64 : kBlock * kQpt;
-  Plan p = plan_launch(c, n_ref, q_count, qpb, f64 ? kBlock64 : kTile);
-
+  int variant = 0;
+  if (!f64) TRY(choose_variant(c, r, qx, qy, r_i, r_j, q_i, q_j, exclude_self, &variant));
+  int64_t nseg = 1;
+  TRY(launch_pair_sum(c, r, f64, variant, qx, qy, r_i, r_j, q_i, q_j, exclude_self, 1.0,
+                      nullptr, &nseg));
   double *partial = out_dev;
-  const bool combine = p.nseg > 1 || epi != EPI_NONE;
+  const bool combine = nseg > 1 || epi != EPI_NONE;
   if (combine) {
-    TRY(ensure(c, c->partial, (size_t)p.nseg * q_count * sizeof(double)));
+    TRY(ensure(c, c->partial, (size_t)nseg * q_count * sizeof(double)));
     partial = c->partial.as<double>();
   }
-  SumArgs a;
-  PackCache &pc = f64 ? c->pack64 : c->pack32;
-  a.refs = pc.rec.p;
-  a.extra = pc.ext.p;
-  a.qx = qx;
-  a.qy = qy;
-  a.r_begin = r_i;
-  a.r_end = r_j + 1;
-  a.seg_len = p.seg_len;
-  a.q_begin = q_i;
-  a.q_count = q_count;
-  a.exclude_self = exclude_self ? 1 : 0;
-  a.scale = combine ? 1.0 : scale;
-  a.out = partial;
-  a.status = c->status.as<int>();
-
-  dim3 grid(p.gx, (unsigned)p.nseg);
   CUDA_TRY(c, cudaEventRecord(c->ev0, c->stream));
-  if (r.dim == 2) dispatch_op<2>(r.op, f64, grid, c->stream, a);
-  else dispatch_op<1>(r.op, f64, grid, c->stream, a);
-  COUNT_LAUNCH(c);
-  CUDA_TRY(c, cudaGetLastError());
+  TRY(launch_pair_sum(c, r, f64, variant, qx, qy, r_i, r_j, q_i, q_j, exclude_self,
+                      combine ? 1.0 : scale, partial, nullptr));
   CUDA_TRY(c, cudaEventRecord(c->ev1, c->stream));
   int64_t launches = 1;
   if (combine) {
     const unsigned nb = grid1d(q_count, kRedBlock);
     if (epi != EPI_NONE) TRY(ensure(c, c->block_sums, (size_t)nb * sizeof(double)));
-    k_combine<<<nb, kRedBlock, 0, c->stream>>>(partial, (int)p.nseg, q_count, scale, out_dev,
+    k_combine<<<nb, kRedBlock, 0, c->stream>>>(partial, (int)nseg, q_count, scale, out_dev,
                                                epi, w_dev, c->block_sums.as<double>());
     COUNT_LAUNCH(c);
     CUDA_TRY(c, cudaGetLastError());
@@ -433,6 +530,7 @@ int pair_sum(bbkde_ctx *c, const Resolved &r, int precision, int qset, int64_t r
   c->last_ms = ms;
   c->last_pairs = (double)n_ref * (double)q_count;
   c->last_launches = launches;
+  c->last_variant = f64 ? -1 : variant;
   return BBKDE_OK;
 }
 
@@ -783,6 +881,21 @@ int bbkde_last_launch_stats(const bbkde_ctx *c, double *kernel_ms, double *pairs
 }
 
 int64_t bbkde_launch_count(const bbkde_ctx *c) { return c ? c->launch_total : -1; }
+
+int bbkde_ctx_set_launch_variant(bbkde_ctx *c, int variant) {
+  if (!c) return BBKDE_INVALID_ARGUMENT;
+  if (variant < -1 || variant >= kNumVariants)
+    return fail(c, BBKDE_INVALID_ARGUMENT, "launch variant out of range");
+  c->forced_variant = variant;
+  return BBKDE_OK;
+}
+
+int bbkde_launch_variants(const bbkde_ctx *c, int *n_variants, int *last_variant) {
+  if (!c) return BBKDE_INVALID_ARGUMENT;
+  if (n_variants) *n_variants = kNumVariants;
+  if (last_variant) *last_variant = c->last_variant;
+  return BBKDE_OK;
+}
 
 int bbkde_device_info(const bbkde_ctx *c, int *sm_count, int *device) {
   if (!c) return BBKDE_INVALID_ARGUMENT;

@@ -181,8 +181,8 @@ __device__ __forceinline__ void chunk_sum_diag(const float4 *__restrict__ s_rec,
   }
 }
 
-template <int OP, int D, int QPT, int BLOCK, int TILE>
-__global__ void __launch_bounds__(BLOCK, 2) k_pair_sum_f32(SumArgs a) {
+template <int OP, int D, int QPT, int BLOCK, int TILE, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) k_pair_sum_f32(SumArgs a) {
   static_assert(TILE % kChunk == 0, "tile must hold whole chunks");
   __shared__ float4 s_rec[TILE];
   __shared__ float s_ext[op_has_extra(OP) ? TILE : 1];
@@ -242,6 +242,175 @@ __global__ void __launch_bounds__(BLOCK, 2) k_pair_sum_f32(SumArgs a) {
         float t = sum[k] + y;
         comp[k] = (t - sum[k]) - y;
         sum[k] = t;
+      }
+    }
+  }
+
+  double *out = a.out + (int64_t)blockIdx.y * a.q_count;
+#pragma unroll
+  for (int k = 0; k < QPT; ++k) {
+    int64_t lq = lq0 + k * BLOCK + tid;
+    if (lq < a.q_count) out[lq] = a.scale * ((double)sum[k] - (double)comp[k]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// FP32-compensated pair sum on packed f32x2 arithmetic (sm_100 FADD2 / FMUL2 /
+// FFMA2): each instruction evaluates the same operation for two queries, so a
+// Gaussian pair costs 3 packed-FP32 issue slots + 1 MUFU.EX2 instead of 6 + 1.
+// The arithmetic per query is identical to k_pair_sum_f32 (same operations,
+// same IEEE round-to-nearest), only issued two lanes at a time.
+//
+// Shared-memory records are pre-duplicated so every operand is a ready
+// register pair: r0 = {-x, -x, -y, -y}, r1 = {m, m, s, s}, r2 = {e, e, _, _}
+// (2-D) and r0 = {-x, -x, 0, 0}, r1 = {m, m, s, s} (1-D); q - x is evaluated as
+// q + (-x), which IEEE defines identically.
+// Operators: OP_GAUSS_ISO, OP_GAUSS_PROD, OP_EPAN_ISO, OP_EPAN_PROD.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+
+template <int OP, int D>
+__device__ __forceinline__ float2 pair_u2(const float2 qx, const float2 qy, const float4 &r0,
+                                          const float4 &r1, const float4 &r2) {
+  const float2 nrx = make_float2(r0.x, r0.y);
+  const float2 s = make_float2(r1.z, r1.w);
+  float2 dx = __fadd2_rn(qx, nrx);
+  if (D == 2) {
+    const float2 nry = make_float2(r0.z, r0.w);
+    float2 dy = __fadd2_rn(qy, nry);
+    if (OP == OP_GAUSS_ISO) {
+      float2 d2 = __ffma2_rn(dy, dy, __fmul2_rn(dx, dx));
+      float2 e = __fmul2_rn(d2, s);
+      return make_float2(ex2_approx(e.x), ex2_approx(e.y));
+    } else if (OP == OP_GAUSS_PROD) {
+      const float2 sy = make_float2(r2.x, r2.y);
+      float2 e = __ffma2_rn(__fmul2_rn(dy, dy), sy, __fmul2_rn(__fmul2_rn(dx, dx), s));
+      return make_float2(ex2_approx(e.x), ex2_approx(e.y));
+    } else if (OP == OP_EPAN_ISO) {
+      float2 d2 = __ffma2_rn(dy, dy, __fmul2_rn(dx, dx));
+      float2 u = __ffma2_rn(d2, s, f2(1.0f));
+      return make_float2(fmaxf(u.x, 0.0f), fmaxf(u.y, 0.0f));
+    } else {  // OP_EPAN_PROD
+      const float2 sy = make_float2(r2.x, r2.y);
+      float2 ux = __ffma2_rn(__fmul2_rn(dx, dx), s, f2(1.0f));
+      float2 uy = __ffma2_rn(__fmul2_rn(dy, dy), sy, f2(1.0f));
+      return __fmul2_rn(make_float2(fmaxf(ux.x, 0.0f), fmaxf(ux.y, 0.0f)),
+                        make_float2(fmaxf(uy.x, 0.0f), fmaxf(uy.y, 0.0f)));
+    }
+  } else {
+    if (OP == OP_GAUSS_ISO || OP == OP_GAUSS_PROD) {
+      float2 e = __fmul2_rn(__fmul2_rn(dx, dx), s);
+      return make_float2(ex2_approx(e.x), ex2_approx(e.y));
+    } else {
+      float2 u = __ffma2_rn(__fmul2_rn(dx, dx), s, f2(1.0f));
+      return make_float2(fmaxf(u.x, 0.0f), fmaxf(u.y, 0.0f));
+    }
+  }
+}
+
+__host__ __device__ constexpr bool op_packed(int op) {
+  return op == OP_GAUSS_ISO || op == OP_GAUSS_PROD || op == OP_EPAN_ISO || op == OP_EPAN_PROD;
+}
+
+template <int OP, int D, int QPT, int BLOCK, int TILE, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) k_pair_sum_f32x2(SumArgs a) {
+  static_assert(QPT % 2 == 0, "queries are processed in pairs");
+  static_assert(TILE % kChunk == 0 && TILE % BLOCK == 0, "tile shape");
+  constexpr int NP = QPT / 2;
+  constexpr bool kExt = op_has_extra(OP) && D == 2;
+  __shared__ float4 s_r0[TILE];
+  __shared__ float4 s_r1[TILE];
+  __shared__ float4 s_r2[kExt ? TILE : 1];
+
+  const float4 *__restrict__ refs = static_cast<const float4 *>(a.refs);
+  const float *__restrict__ ext = static_cast<const float *>(a.extra);
+  const float *__restrict__ gqx = static_cast<const float *>(a.qx);
+  const float *__restrict__ gqy = static_cast<const float *>(a.qy);
+
+  const int tid = threadIdx.x;
+  const int64_t lq0 = (int64_t)blockIdx.x * (BLOCK * QPT);
+  const int64_t r_lo = a.r_begin + (int64_t)blockIdx.y * a.seg_len;
+  const int64_t r_hi = min(r_lo + a.seg_len, a.r_end);
+
+  // Query pair p of this thread = local queries (2p, 2p+1) -> slots k = 2p, 2p+1.
+  float2 qx[NP], qy[NP];
+  float sum[QPT], comp[QPT];
+#pragma unroll
+  for (int k = 0; k < QPT; ++k) {
+    int64_t lq = lq0 + k * BLOCK + tid;
+    bool ok = lq < a.q_count;
+    float x = ok ? gqx[a.q_begin + lq] : 0.0f;
+    float y = (ok && D == 2) ? gqy[a.q_begin + lq] : 0.0f;
+    if (k & 1) { qx[k >> 1].y = x; qy[k >> 1].y = y; }
+    else { qx[k >> 1].x = x; qy[k >> 1].x = y; }
+    sum[k] = 0.0f;
+    comp[k] = 0.0f;
+  }
+  const int64_t qg_lo = a.q_begin + lq0;
+  const int64_t qg_hi = qg_lo + BLOCK * QPT;
+
+  for (int64_t t0 = r_lo; t0 < r_hi; t0 += TILE) {
+    __syncthreads();
+#pragma unroll
+    for (int i = tid; i < TILE; i += BLOCK) {
+      int64_t r = t0 + i;
+      float4 v = r < r_hi ? refs[r] : make_float4(0.f, 0.f, 0.f, 0.f);  // zero-mass padding
+      if (D == 2) {
+        s_r0[i] = make_float4(-v.x, -v.x, -v.y, -v.y);
+        s_r1[i] = make_float4(v.z, v.z, v.w, v.w);
+        if (kExt) {
+          float e = r < r_hi ? ext[r] : 0.0f;
+          s_r2[i] = make_float4(e, e, 0.f, 0.f);
+        }
+      } else {
+        s_r0[i] = make_float4(-v.x, -v.x, 0.f, 0.f);
+        s_r1[i] = make_float4(v.y, v.y, v.z, v.z);
+      }
+    }
+    __syncthreads();
+    const bool diag = a.exclude_self && t0 < qg_hi && qg_lo < t0 + TILE;
+    for (int j0 = 0; j0 < TILE; j0 += kChunk) {
+      float2 acc[NP];
+#pragma unroll
+      for (int p = 0; p < NP; ++p) acc[p] = f2(0.0f);
+      if (!diag) {
+#pragma unroll 4
+        for (int j = 0; j < kChunk; ++j) {
+          const float4 r0 = s_r0[j0 + j];
+          const float4 r1 = s_r1[j0 + j];
+          const float4 r2 = kExt ? s_r2[j0 + j] : r1;
+          const float2 m = make_float2(r1.x, r1.y);
+#pragma unroll
+          for (int p = 0; p < NP; ++p)
+            acc[p] = __ffma2_rn(m, pair_u2<OP, D>(qx[p], qy[p], r0, r1, r2), acc[p]);
+        }
+      } else {
+        // Diagonal tile of a self-evaluation: zero the mass of the pair r == q.
+        for (int j = 0; j < kChunk; ++j) {
+          const float4 r0 = s_r0[j0 + j];
+          const float4 r1 = s_r1[j0 + j];
+          const float4 r2 = kExt ? s_r2[j0 + j] : r1;
+          const int64_t rg = t0 + j0 + j;
+#pragma unroll
+          for (int p = 0; p < NP; ++p) {
+            const int64_t q0 = qg_lo + (2 * p) * BLOCK + tid;
+            const int64_t q1 = q0 + BLOCK;
+            const float2 m = make_float2(rg == q0 ? 0.0f : r1.x, rg == q1 ? 0.0f : r1.y);
+            acc[p] = __ffma2_rn(m, pair_u2<OP, D>(qx[p], qy[p], r0, r1, r2), acc[p]);
+          }
+        }
+      }
+#pragma unroll
+      for (int p = 0; p < NP; ++p) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int k = 2 * p + h;
+          const float v = h ? acc[p].y : acc[p].x;
+          float y = v - comp[k];
+          float t = sum[k] + y;
+          comp[k] = (t - sum[k]) - y;
+          sum[k] = t;
+        }
       }
     }
   }

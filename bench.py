@@ -152,11 +152,15 @@ def cpu_reference_rate(wl, seconds: float, kind_pref: str = "reference"):
         run = lambda q: orc.direct(wl.kind, 2, wl.h, wl.refs, wn, q, nthreads=threads)  # noqa
         kind = "port"
         cleanup = lambda: None  # noqa: E731
-    # size the sample from a short probe
+    # size the sample from a probe of at least ~0.5 s
     probe = max(threads, 8)
-    t0 = time.perf_counter()
-    run(wl.queries[:probe])
-    dt = time.perf_counter() - t0
+    while True:
+        t0 = time.perf_counter()
+        run(wl.queries[:probe])
+        dt = time.perf_counter() - t0
+        if dt >= 0.5 or probe >= len(wl.queries):
+            break
+        probe = min(len(wl.queries), probe * 4)
     per_q = dt / probe
     m = int(min(len(wl.queries), max(probe, seconds / max(per_q, 1e-9))))
     t0 = time.perf_counter()

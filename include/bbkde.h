@@ -188,6 +188,15 @@ BBKDE_API int bbkde_last_launch_stats(const bbkde_ctx *ctx, double *kernel_ms, d
  * (-1 for a NULL context). */
 BBKDE_API int64_t bbkde_launch_count(const bbkde_ctx *ctx);
 
+/* Launch shapes of the FP32 pair-sum kernels (queries per thread x threads per
+ * block). By default (variant -1) the context autotunes: for problems of at least
+ * 2e10 pairs it times every shape on a slice of the problem once per problem
+ * class (kernel, dimension, self-evaluation, log2 sizes) and keeps the fastest.
+ * A variant in [0, n_variants) forces that shape. No reference counterpart: the
+ * reference takes a block_size hint per call (CudaDirectKde.h:83-88). */
+BBKDE_API int bbkde_ctx_set_launch_variant(bbkde_ctx *ctx, int variant);
+BBKDE_API int bbkde_launch_variants(const bbkde_ctx *ctx, int *n_variants, int *last_variant);
+
 /* Number of SMs and the device's ordinal (for callers that size their work). */
 BBKDE_API int bbkde_device_info(const bbkde_ctx *ctx, int *sm_count, int *device);
 

@@ -225,3 +225,30 @@ def test_config2_full_size_properties(ctx, oracle):
     lo = ctx.eval_range(d, 0, half - 1, qi, qj, precision=bk.FP64)
     hi = ctx.eval_range(d, half, n - 1, qi, qj, precision=bk.FP64)
     np.testing.assert_allclose(lo + hi, f64, rtol=1e-12)
+
+
+@pytest.mark.parametrize("kind,dim,h", [(W.GAUSS, 2, (0.2, 0.2)), (W.GAUSS_PROD2D, 2, (0.1, 0.3)),
+                                        (W.EPAN_PROD2D, 2, (0.4, 0.2)), (W.GAUSS, 1, (0.05,)),
+                                        (W.EPAN_PROD_CONV2D, 2, (0.4, 0.2))])
+def test_every_launch_variant(ctx, oracle, kind, dim, h):
+    """Each FP32 launch shape the autotuner may pick gives the same parity,
+    including the self-evaluation diagonal exclusion."""
+    refs, q, mass, abw = _rand_problem(31 + kind, 5003, 4099, dim, adaptive=True)
+    desc = bk.kernel_desc(kind, dim, h)
+    want = oracle.direct(kind, dim, h, refs, mass, q, abw=abw)
+    want_self = oracle.self_eval(kind, dim, h, refs, mass, abw=abw, exclude_self=True)
+    n, _ = ctx.launch_variants()
+    try:
+        for v in range(n):
+            ctx.set_launch_variant(v)
+            ctx.upload(bk.REFERENCE, refs, mass=mass, abw=abw, weight=mass)
+            ctx.upload(bk.QUERY, q)
+            assert_parity(ctx.eval_all(desc), want, REL32, ABS32, what=f"variant {v}")
+            assert ctx.launch_variants()[1] == v
+            ctx.upload(bk.QUERY, refs)
+            lik = ctx.likelihood_cv(desc)
+            np.testing.assert_allclose(lik, np.sum(mass * np.log(want_self)), rtol=1e-6)
+        with pytest.raises(bk.InvalidArgument):
+            ctx.set_launch_variant(n)
+    finally:
+        ctx.set_launch_variant(-1)
