@@ -36,6 +36,7 @@ EXPORTED = [
     "bbkde_adapt_density", "bbkde_unadapt_density", "bbkde_likelihood_cv",
     "bbkde_lsq_conv_cv", "bbkde_last_launch_stats", "bbkde_launch_count",
     "bbkde_device_info", "bbkde_ctx_set_launch_variant", "bbkde_launch_variants",
+    "bbkde_eval_noalloc",
 ]
 
 
@@ -113,6 +114,8 @@ def load_library(path: str = LIB_PATH):
     lib.bbkde_ctx_set_launch_variant.argtypes = [vp, C.c_int]
     lib.bbkde_launch_variants.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     lib.bbkde_device_info.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    lib.bbkde_eval_noalloc.argtypes = [kd, i64, vp, vp, vp, vp, i64, vp, vp, C.c_int, vp, vp,
+                                       C.c_char_p, i64]
     _lib = lib
     return lib
 
@@ -253,3 +256,18 @@ class Context:
         sm, dev = C.c_int(), C.c_int()
         self._check(self.lib.bbkde_device_info(self.h, C.byref(sm), C.byref(dev)))
         return sm.value, dev.value
+
+
+def eval_noalloc(desc: KernelDesc, n_ref: int, ref_x: int, ref_y: int | None, ref_mass: int,
+                 ref_abw: int | None, n_query: int, query_x: int, query_y: int | None,
+                 out: int, normalized: bool = True, stream: int | None = None):
+    """bbkde_eval_noalloc on device pointers (ints). Returns (status, message).
+
+    Allocates no device memory; the work is enqueued on `stream` and the call
+    returns before it finishes (synchronise before reading `out`)."""
+    lib = load_library()
+    buf = C.create_string_buffer(512)
+    rc = lib.bbkde_eval_noalloc(C.byref(desc), n_ref, ref_x, ref_y, ref_mass, ref_abw,
+                                n_query, query_x, query_y, int(normalized), out, stream,
+                                buf, len(buf))
+    return rc, buf.value.decode()

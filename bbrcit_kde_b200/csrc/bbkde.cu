@@ -11,9 +11,11 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdarg>
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <new>
 #include <string>
 #include <tuple>
@@ -905,3 +907,178 @@ int bbkde_device_info(const bbkde_ctx *c, int *sm_count, int *device) {
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Allocation-free direct evaluation (bbkde_eval_noalloc)
+//
+// For callers that must not allocate device memory: code that runs inside a
+// host framework owning every device allocation through its own pool (so a
+// cudaMalloc from a library would fragment or bypass it), work enqueued while
+// the process has memory-allocation checks that forbid new allocations, or
+// code paths that have to run when device memory is exhausted. Such callers
+// pass device pointers for every input and output; the scratch the pair sum
+// needs (packed reference records, FP32 query coordinates and the FP64 segment
+// partials) lives in one fixed array of the library's device image.
+// ===========================================================================
+
+// 64 MiB of device scratch. Every device that loads libbbkde.so holds it until
+// the process exits. Host code must not use this name as an address: on the
+// host it is only a stand-in for the device symbol, which is why the entry point
+// resolves its device address with cudaGetSymbolAddress.
+static constexpr size_t kNoAllocScratchBytes = size_t(64) << 20;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+namespace {
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void *g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+void noalloc_msg(char *buf, int64_t len, const char *fmt, ...) {
+  if (!buf || len <= 0) return;
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, (size_t)len, fmt, ap);
+  va_end(ap);
+}
+
+inline size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
+
+// Device address of g_noalloc_scratch on `device` (which must be current),
+// resolved on the first call for that device and cached afterwards.
+int noalloc_scratch(int device, void **out, char *err, int64_t errlen) {
+  if (device < 0 || device >= kNoAllocMaxDevices) {
+    noalloc_msg(err, errlen, "device ordinal %d not supported", device);
+    return BBKDE_INVALID_ARGUMENT;
+  }
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_addr[device]) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+      noalloc_msg(err, errlen, "cudaGetSymbolAddress(scratch): %s", cudaGetErrorString(e));
+      cudaGetLastError();
+      return BBKDE_CUDA_ERROR;
+    }
+    g_noalloc_addr[device] = p;
+  }
+  *out = g_noalloc_addr[device];
+  return BBKDE_OK;
+}
+
+}  // namespace
+
+extern "C" int bbkde_eval_noalloc(const bbkde_kernel_desc *kernel, int64_t n_ref,
+                                  const double *ref_x, const double *ref_y,
+                                  const double *ref_mass, const double *ref_abw,
+                                  int64_t n_query, const double *query_x,
+                                  const double *query_y, int normalized, double *out,
+                                  void *stream, char *errbuf, int64_t errbuf_len) {
+  if (errbuf && errbuf_len > 0) errbuf[0] = '\0';
+  Resolved r;
+  if (resolve(nullptr, kernel, r) != BBKDE_OK) {
+    noalloc_msg(errbuf, errbuf_len, "invalid kernel descriptor (kind, dim or bandwidths)");
+    return BBKDE_INVALID_ARGUMENT;
+  }
+  const int dim = r.dim;
+  if (n_ref < 1 || n_query < 0) {
+    noalloc_msg(errbuf, errbuf_len, "need n_ref >= 1 and n_query >= 0");
+    return BBKDE_INVALID_ARGUMENT;
+  }
+  if (n_query == 0) return BBKDE_OK;
+  if (!ref_x || !ref_mass || !query_x || !out || (dim == 2 && (!ref_y || !query_y))) {
+    noalloc_msg(errbuf, errbuf_len, "a required device pointer is NULL");
+    return BBKDE_INVALID_ARGUMENT;
+  }
+  // Scratch layout: records | extra column | query x | query y | partials.
+  const bool ext = op_has_extra(r.op);
+  const size_t off_ext = align256((size_t)n_ref * sizeof(float4));
+  const size_t off_qx = off_ext + (ext ? align256((size_t)n_ref * sizeof(float)) : 0);
+  const size_t off_qy = off_qx + align256((size_t)n_query * sizeof(float));
+  const size_t off_part = off_qy + (dim == 2 ? align256((size_t)n_query * sizeof(float)) : 0);
+  const size_t per_seg = (size_t)n_query * sizeof(double);
+  if (off_part + per_seg > kNoAllocScratchBytes) {
+    noalloc_msg(errbuf, errbuf_len,
+                "n_ref = %lld and n_query = %lld need %zu bytes of scratch, more than the "
+                "%zu bytes of the allocation-free entry point (16-20 B per reference, "
+                "4 B per query coordinate, 8 B per query and reference segment); use "
+                "bbkde_eval_range for larger problems",
+                (long long)n_ref, (long long)n_query, off_part + per_seg,
+                kNoAllocScratchBytes);
+    return BBKDE_OUT_OF_RANGE;
+  }
+  int device = 0;
+  cudaError_t e = cudaGetDevice(&device);
+  if (e != cudaSuccess) {
+    noalloc_msg(errbuf, errbuf_len, "cudaGetDevice: %s", cudaGetErrorString(e));
+    return BBKDE_CUDA_ERROR;
+  }
+  void *base = nullptr;
+  int rc = noalloc_scratch(device, &base, errbuf, errbuf_len);
+  if (rc != BBKDE_OK) return rc;
+  unsigned char *sb = static_cast<unsigned char *>(base);
+  float4 *rec = reinterpret_cast<float4 *>(sb);
+  float *extc = ext ? reinterpret_cast<float *>(sb + off_ext) : nullptr;
+  float *qx = reinterpret_cast<float *>(sb + off_qx);
+  float *qy = dim == 2 ? reinterpret_cast<float *>(sb + off_qy) : qx;
+  double *partial = reinterpret_cast<double *>(sb + off_part);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+
+  PackArgs p;
+  p.x = ref_x;
+  p.y = ref_y;
+  p.mass = ref_mass;
+  p.abw = ref_abw;
+  p.n = n_ref;
+  p.op = r.op;
+  p.dim = dim;
+  p.c1 = r.c1_f32;
+  p.c2 = r.c2_f32;
+  p.h1 = r.h1;
+  p.h2 = r.h2;
+  p.mass_scale = r.mass_scale;
+  k_pack_f32<<<grid1d(n_ref), 256, 0, st>>>(p, rec, extc);
+  k_to_f32<<<grid1d(n_query), 256, 0, st>>>(query_x, qx, n_query);
+  if (dim == 2) k_to_f32<<<grid1d(n_query), 256, 0, st>>>(query_y, qy, n_query);
+
+  // Segment the reference range as the context path does, within the scratch.
+  int sm_count = 148;
+  cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, device);
+  const int variant = kDefaultVariant;
+  const int qpb = queries_per_block(variant, false);
+  const int64_t qtiles = (n_query + qpb - 1) / qpb;
+  const int64_t target = (int64_t)sm_count * 4 * 16;
+  int64_t nseg = std::max<int64_t>(1, (target + qtiles - 1) / qtiles);
+  nseg = std::min<int64_t>(nseg, std::max<int64_t>(1, (n_ref + 511) / 512));
+  nseg = std::min<int64_t>(nseg, (int64_t)((kNoAllocScratchBytes - off_part) / per_seg));
+  nseg = std::min<int64_t>(nseg, 65535);
+  int64_t seg_len = (n_ref + nseg - 1) / nseg;
+  seg_len = (seg_len + kTile - 1) / kTile * kTile;
+  nseg = std::max<int64_t>(1, (n_ref + seg_len - 1) / seg_len);
+
+  SumArgs a;
+  a.refs = rec;
+  a.extra = extc;
+  a.qx = qx;
+  a.qy = qy;
+  a.r_begin = 0;
+  a.r_end = n_ref;
+  a.seg_len = seg_len;
+  a.q_begin = 0;
+  a.q_count = n_query;
+  a.exclude_self = 0;
+  a.scale = 1.0;
+  a.out = partial;   // every (segment, query) entry is written: nothing to clear
+  a.status = nullptr;
+  dim3 grid((unsigned)qtiles, (unsigned)nseg);
+  if (dim == 2) dispatch_op<2>(r.op, false, variant, grid, st, a);
+  else dispatch_op<1>(r.op, false, variant, grid, st, a);
+  k_combine<<<grid1d(n_query, kRedBlock), kRedBlock, 0, st>>>(
+      partial, (int)nseg, n_query, normalized ? r.norm : 1.0, out, EPI_NONE, nullptr, nullptr);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    noalloc_msg(errbuf, errbuf_len, "kernel launch: %s", cudaGetErrorString(e));
+    return BBKDE_CUDA_ERROR;
+  }
+  return BBKDE_OK;
+}

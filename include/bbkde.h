@@ -197,6 +197,40 @@ BBKDE_API int64_t bbkde_launch_count(const bbkde_ctx *ctx);
 BBKDE_API int bbkde_ctx_set_launch_variant(bbkde_ctx *ctx, int variant);
 BBKDE_API int bbkde_launch_variants(const bbkde_ctx *ctx, int *n_variants, int *last_variant);
 
+/* ---- allocation-free evaluation ----------------------------------------- */
+
+/* Direct evaluation that allocates no device memory. It has no counterpart in
+ * the reference: it exists for callers that cannot call cudaMalloc -- code
+ * running inside a host framework that owns every device allocation through its
+ * own pool, work issued where new allocations are forbidden or device memory is
+ * already exhausted. The caller passes device pointers for all inputs (FP64
+ * columns ref_x / ref_y / ref_mass / ref_abw, query_x / query_y; ref_abw may be
+ * NULL, the y columns are ignored for dim 1) and for the output out[n_query]
+ * (normalized = 1 multiplies by C(h)). The result equals bbkde_eval_range with
+ * BBKDE_FP32C over all references and queries.
+ *
+ * Scratch is one fixed 64 MiB array in the library's device image (held by every
+ * device that loads the library until the process exits). Problems that do not
+ * fit -- 16 B per reference (20 B for product and convolution kernels), 4 B per
+ * query coordinate and at least 8 B per query -- are rejected with
+ * BBKDE_OUT_OF_RANGE and a message in errbuf (may be NULL). Up to 1,000,000
+ * references with 1,000,000 2-D queries fit.
+ *
+ * The work is enqueued on `stream` (a cudaStream_t, NULL = legacy default
+ * stream) and the call returns without waiting for it. All calls share the one
+ * scratch array, so calls whose GPU work can overlap (different streams, or
+ * different host threads without ordering) race and corrupt each other's
+ * results; order them on one stream. The first call on each device resolves the
+ * array's device address (cudaGetSymbolAddress) for that device, with the device
+ * current; make that first call before any stream capture. Every scratch entry a
+ * call reads is written earlier in the same call, so nothing is cleared. */
+BBKDE_API int bbkde_eval_noalloc(const bbkde_kernel_desc *kernel, int64_t n_ref,
+                                 const double *ref_x, const double *ref_y,
+                                 const double *ref_mass, const double *ref_abw,
+                                 int64_t n_query, const double *query_x,
+                                 const double *query_y, int normalized, double *out,
+                                 void *stream, char *errbuf, int64_t errbuf_len);
+
 /* Number of SMs and the device's ordinal (for callers that size their work). */
 BBKDE_API int bbkde_device_info(const bbkde_ctx *ctx, int *sm_count, int *device);
 
