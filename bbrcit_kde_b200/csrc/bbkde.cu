@@ -84,7 +84,7 @@ struct bbkde_ctx {
   cudaStream_t stream = nullptr;
   PointSet sets[2];
   PackCache pack32, pack64;
-  QueryCache q32, q64;
+  QueryCache q32[2];          // FP32 query coordinates, one slot per point set
   DevBuf partial, out_dev, block_sums, scalars, staging, status;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
   double last_ms = 0, last_pairs = 0;
@@ -295,7 +295,7 @@ int ensure_queries(bbkde_ctx *c, int set, bool f64, const void **qx, const void 
     *qy = s.dim == 2 ? s.y.p : s.x.p;
     return BBKDE_OK;
   }
-  QueryCache &qc = c->q32;
+  QueryCache &qc = c->q32[set];
   if (!(qc.set == set && qc.coord_version == s.coord_version)) {
     const int64_t n = std::max<int64_t>(s.n, 1);
     TRY(ensure(c, qc.x, (size_t)n * sizeof(float)));
@@ -675,7 +675,7 @@ int bbkde_ctx_destroy(bbkde_ctx *c) {
   }
   release(c->pack32.rec); release(c->pack32.ext);
   release(c->pack64.rec); release(c->pack64.ext);
-  release(c->q32.x); release(c->q32.y); release(c->q64.x); release(c->q64.y);
+  for (auto &q : c->q32) { release(q.x); release(q.y); }
   release(c->partial); release(c->out_dev); release(c->block_sums);
   release(c->scalars); release(c->staging); release(c->status);
   if (c->ev0) cudaEventDestroy(c->ev0);

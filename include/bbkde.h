@@ -48,7 +48,7 @@ typedef enum {
   BBKDE_ALLOC_FAILED = 7
 } bbkde_status;
 
-/* Kernel families (include/Kernels/*.h in the reference). */
+/* Kernel families (the include/Kernels/ headers of the reference). */
 typedef enum {
   BBKDE_GAUSSIAN = 0,                   /* GaussianKernel<D,T>, D = 1, 2 */
   BBKDE_EPANECHNIKOV = 1,               /* EpanechnikovKernel<D,T>, D = 1, 2 */
