@@ -36,8 +36,13 @@ EXPORTED = [
     "bbkde_adapt_density", "bbkde_unadapt_density", "bbkde_likelihood_cv",
     "bbkde_lsq_conv_cv", "bbkde_last_launch_stats", "bbkde_launch_count",
     "bbkde_device_info", "bbkde_ctx_set_launch_variant", "bbkde_launch_variants",
-    "bbkde_eval_noalloc",
+    "bbkde_eval_noalloc", "bbkde_cv_batch",
 ]
+
+
+class Dataset(C.Structure):
+    _fields_ = [("n", C.c_int64), ("coords", C.POINTER(C.c_double)),
+                ("weights", C.POINTER(C.c_double))]
 
 
 class KernelDesc(C.Structure):
@@ -114,6 +119,8 @@ def load_library(path: str = LIB_PATH):
     lib.bbkde_ctx_set_launch_variant.argtypes = [vp, C.c_int]
     lib.bbkde_launch_variants.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     lib.bbkde_device_info.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    lib.bbkde_cv_batch.argtypes = [vp, C.c_int, C.c_int, C.POINTER(Dataset), C.c_int, _dp,
+                                   C.c_int, _dp, C.c_int, _dp, _dp]
     lib.bbkde_eval_noalloc.argtypes = [kd, i64, vp, vp, vp, vp, i64, vp, vp, C.c_int, vp, vp,
                                        C.c_char_p, i64]
     _lib = lib
@@ -242,6 +249,28 @@ class Context:
 
     def launch_count(self) -> int:
         return int(self.lib.bbkde_launch_count(self.h))
+
+    def cv_batch(self, kind: int, datasets, hx, hy, precision=FP64):
+        """Likelihood and LSQ-convolution CV of every dataset over the hx x hy grid.
+
+        datasets: list of (coords (n, 2), weights or None). Returns (lik, lsq) with
+        shape (n_sets, len(hx), len(hy))."""
+        keep = []
+        arr = (Dataset * max(len(datasets), 1))()
+        for i, (xy, w) in enumerate(datasets):
+            xy = _c(xy).reshape(-1, 2)
+            w = _c(w)
+            keep += [xy, w]
+            arr[i].n = xy.shape[0]
+            arr[i].coords = _p(xy)
+            arr[i].weights = _p(w) if w is not None else None
+        hx, hy = _c(hx), _c(hy)
+        n = len(datasets)
+        lik = np.empty((max(n, 1), len(hx), len(hy)))
+        lsq = np.empty_like(lik)
+        self._check(self.lib.bbkde_cv_batch(self.h, kind, n, arr, len(hx), _p(hx), len(hy),
+                                            _p(hy), precision, _p(lik), _p(lsq)))
+        return lik[:n], lsq[:n]
 
     def set_launch_variant(self, variant: int):
         """-1 = autotune (default); 0..n-1 forces a launch shape."""

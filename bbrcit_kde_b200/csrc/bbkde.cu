@@ -19,9 +19,11 @@
 #include <new>
 #include <string>
 #include <tuple>
+#include <vector>
 
 #include "../../include/bbkde.h"
 #include "kde_device.cuh"
+#include "kde_cv_batch.cuh"
 
 using namespace bbkde;
 
@@ -94,6 +96,11 @@ struct bbkde_ctx {
   int last_variant = -1;
   // autotuner cache: (op, dim, exclude_self, log2 refs, log2 queries) -> variant
   std::map<std::tuple<int, int, int, int, int>, int> tuned;
+  // batched cross-validation buffers and the captured launch graph
+  DevBuf cv_x, cv_y, cv_w, cv_cells, cv_sets, cv_items, cv_counter, cv_h, cv_lut,
+      cv_part, cv_hist, cv_out, cv_parts;
+  cudaGraphExec_t cv_graph = nullptr;
+  std::vector<uint64_t> cv_graph_key;
   std::string err;
 };
 
@@ -678,6 +685,11 @@ int bbkde_ctx_destroy(bbkde_ctx *c) {
   for (auto &q : c->q32) { release(q.x); release(q.y); }
   release(c->partial); release(c->out_dev); release(c->block_sums);
   release(c->scalars); release(c->staging); release(c->status);
+  for (DevBuf *b : {&c->cv_x, &c->cv_y, &c->cv_w, &c->cv_cells, &c->cv_sets, &c->cv_items,
+                    &c->cv_counter, &c->cv_h, &c->cv_lut, &c->cv_part, &c->cv_hist,
+                    &c->cv_out, &c->cv_parts})
+    release(*b);
+  if (c->cv_graph) cudaGraphExecDestroy(c->cv_graph);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->ev2) cudaEventDestroy(c->ev2);
@@ -907,6 +919,340 @@ int bbkde_device_info(const bbkde_ctx *c, int *sm_count, int *device) {
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Batched cross-validation (bbkde_cv_batch)
+// ===========================================================================
+namespace {
+
+constexpr int kCvChunk = 4096;     // queries per likelihood work item
+constexpr int kCvBlock = 1024;
+
+size_t cv_smem_bytes() {
+  return sizeof(double) * (4 * kCvHist + 6 * kCvMaxH + 3 * kCvQBlock) +
+         sizeof(int64_t) * (2 * kCvMaxRanges + 1) + 4 * sizeof(int) + 2 * kCvLut;
+}
+
+// Lower-bound table for cv_cell: bin i holds #{h[a] <= the smallest double whose
+// key (bits >> shift) is base + i}. The shift keeps as many mantissa bits as fit
+// kCvLut bins over [h_min / 4, h_max] (64 bins per octave for the usual grids).
+void cv_lut(const double *h, int n, int shift, long long &base, unsigned char *lut) {
+  auto key = [&](double v) {
+    long long b;
+    std::memcpy(&b, &v, sizeof(b));
+    return b >> shift;
+  };
+  base = key(h[0] / 4.0);
+  for (int i = 0; i < kCvLut; ++i) {
+    long long bits = (base + i) << shift;
+    double v;
+    std::memcpy(&v, &bits, sizeof(v));
+    int cnt = 0;
+    while (cnt < n && h[cnt] <= v) ++cnt;
+    lut[i] = (unsigned char)cnt;
+  }
+}
+
+int cv_lut_shift(const double *hx, int nx, const double *hy, int ny) {
+  const double lo = std::min(hx[0], hy[0]) / 4.0;
+  const double hi = std::max(hx[nx - 1], hy[ny - 1]) * 1.01;
+  const double octaves = std::log2(hi / lo) + 2.0;
+  int mbits = 8;
+  while (mbits > 0 && octaves * (1 << mbits) > kCvLut) --mbits;
+  return 52 - mbits;
+}
+
+int cv_check_grid(bbkde_ctx *c, int n, const double *h, const char *name) {
+  if (n < 1 || n > kCvMaxH || !h)
+    return fail(c, BBKDE_INVALID_ARGUMENT,
+                std::string(name) + ": between 1 and 64 bandwidths are supported");
+  for (int i = 0; i < n; ++i) {
+    if (!(h[i] > 0) || !std::isfinite(h[i]) || (i > 0 && !(h[i] > h[i - 1])))
+      return fail(c, BBKDE_INVALID_ARGUMENT,
+                  std::string(name) + ": bandwidths must be positive and strictly increasing");
+  }
+  return BBKDE_OK;
+}
+
+// Gaussian product kernel: exact per-bandwidth loop over the pair sum.
+int cv_batch_loop(bbkde_ctx *c, int kind, int n_sets, const bbkde_dataset *sets, int n_hx,
+                  const double *hx, int n_hy, const double *hy, int precision, double *lik,
+                  double *lsq) {
+  double ms = 0, pairs = 0;
+  for (int sidx = 0; sidx < n_sets; ++sidx) {
+    const bbkde_dataset &d = sets[sidx];
+    std::vector<double> w(d.n);
+    double tot = 0;
+    for (int64_t i = 0; i < d.n; ++i) tot += d.weights ? d.weights[i] : 1.0;
+    for (int64_t i = 0; i < d.n; ++i) w[i] = (d.weights ? d.weights[i] : 1.0) / tot;
+    TRY(bbkde_upload(c, BBKDE_REFERENCE, 2, d.n, d.coords, w.data(), nullptr, w.data()));
+    for (int a = 0; a < n_hx; ++a)
+      for (int b = 0; b < n_hy; ++b) {
+        bbkde_kernel_desc k = {kind, 2, {hx[a], hy[b]}, 0, 0};
+        const int64_t o = ((int64_t)sidx * n_hx + a) * n_hy + b;
+        TRY(bbkde_likelihood_cv(c, &k, precision, lik + o));
+        ms += c->last_ms;
+        TRY(bbkde_lsq_conv_cv(c, &k, precision, lsq + o));
+        ms += c->last_ms;
+        pairs += 3.0 * (double)d.n * (double)d.n;
+      }
+  }
+  c->last_ms = ms;
+  c->last_pairs = pairs;
+  return BBKDE_OK;
+}
+
+}  // namespace
+
+extern "C" int bbkde_cv_batch(bbkde_ctx *c, int kind, int n_sets, const bbkde_dataset *sets,
+                              int n_hx, const double *hx, int n_hy, const double *hy,
+                              int precision, double *lik_out, double *lsq_out) {
+  TRY(check_ctx(c));
+  if (n_sets < 0 || (n_sets > 0 && !sets) || !lik_out || !lsq_out)
+    return fail(c, BBKDE_INVALID_ARGUMENT, "cv_batch: bad dataset or output pointers");
+  if (precision != BBKDE_FP32C && precision != BBKDE_FP64)
+    return fail(c, BBKDE_INVALID_ARGUMENT, "unknown precision");
+  TRY(cv_check_grid(c, n_hx, hx, "hx"));
+  TRY(cv_check_grid(c, n_hy, hy, "hy"));
+  for (int sidx = 0; sidx < n_sets; ++sidx) {
+    if (sets[sidx].n < 2 || !sets[sidx].coords)
+      return fail(c, BBKDE_INVALID_ARGUMENT, "cv_batch: every dataset needs at least 2 points");
+  }
+  if (kind == BBKDE_GAUSSIAN_PRODUCT_2D)
+    return cv_batch_loop(c, kind, n_sets, sets, n_hx, hx, n_hy, hy, precision, lik_out,
+                         lsq_out);
+  if (kind != BBKDE_EPANECHNIKOV_PRODUCT_2D)
+    return fail(c, BBKDE_UNSUPPORTED,
+                "cv_batch: supported kernels are the 2-D Epanechnikov and Gaussian products");
+  if (n_sets == 0) return BBKDE_OK;
+
+  // ---- host: normalise weights, bin points on a grid, sort by cell --------
+  const double hmax = std::max(hx[n_hx - 1], hy[n_hy - 1]);
+  std::vector<CvSet> hs(n_sets);
+  std::vector<double> X, Y, Wt;
+  std::vector<int64_t> cells;
+  int64_t total = 0;
+  for (int sidx = 0; sidx < n_sets; ++sidx) total += sets[sidx].n;
+  X.reserve(total); Y.reserve(total); Wt.reserve(total);
+  double sum_pairs = 0;
+  for (int sidx = 0; sidx < n_sets; ++sidx) {
+    const bbkde_dataset &d = sets[sidx];
+    const int64_t n = d.n;
+    double xmin = d.coords[0], xmax = xmin, ymin = d.coords[1], ymax = ymin, wt = 0;
+    for (int64_t i = 0; i < n; ++i) {
+      const double x = d.coords[2 * i], y = d.coords[2 * i + 1];
+      if (!std::isfinite(x) || !std::isfinite(y))
+        return fail(c, BBKDE_INVALID_ARGUMENT, "cv_batch: non-finite coordinate");
+      xmin = std::min(xmin, x); xmax = std::max(xmax, x);
+      ymin = std::min(ymin, y); ymax = std::max(ymax, y);
+      wt += d.weights ? d.weights[i] : 1.0;
+    }
+    if (!(wt > 0)) return fail(c, BBKDE_INVALID_ARGUMENT, "cv_batch: weights must sum > 0");
+    // Cells of a quarter of the largest bandwidth, at most 4096 per axis.
+    const double spread = std::max(xmax - xmin, ymax - ymin);
+    const double cell = std::max(hmax / 4.0, spread / 4095.0);
+    CvSet &s = hs[sidx];
+    s.begin = (int64_t)X.size();
+    s.n = n;
+    s.cell_begin = (int64_t)cells.size();
+    s.x0 = xmin;
+    s.y0 = ymin;
+    s.inv_cell = 1.0 / cell;
+    s.gx = (int)std::floor((xmax - xmin) * s.inv_cell) + 1;
+    s.gy = (int)std::floor((ymax - ymin) * s.inv_cell) + 1;
+    const int64_t ncell = (int64_t)s.gx * s.gy;
+    std::vector<int64_t> cnt(ncell + 1, 0), key(n);
+    for (int64_t i = 0; i < n; ++i) {
+      int cx = std::min(s.gx - 1, std::max(0, (int)std::floor((d.coords[2 * i] - xmin) * s.inv_cell)));
+      int cy = std::min(s.gy - 1, std::max(0, (int)std::floor((d.coords[2 * i + 1] - ymin) * s.inv_cell)));
+      key[i] = (int64_t)cy * s.gx + cx;
+      ++cnt[key[i] + 1];
+    }
+    for (int64_t k = 0; k < ncell; ++k) cnt[k + 1] += cnt[k];
+    cells.insert(cells.end(), cnt.begin(), cnt.end());   // set-relative cell_start
+    std::vector<int64_t> pos(cnt.begin(), cnt.end() - 1);
+    X.resize(s.begin + n); Y.resize(s.begin + n); Wt.resize(s.begin + n);
+    double diag = 0;
+    for (int64_t i = 0; i < n; ++i) {                      // stable counting sort
+      const int64_t at = s.begin + pos[key[i]]++;
+      const double w = (d.weights ? d.weights[i] : 1.0) / wt;
+      X[at] = d.coords[2 * i];
+      Y[at] = d.coords[2 * i + 1];
+      Wt[at] = w;
+      diag += w * w;
+    }
+    s.diag_wm = diag;
+    sum_pairs += (double)n * (double)n;
+  }
+  // Work items: likelihood items (set, chunk of queries) and convolution items
+  // (set, grid cell, block of <= kCvQBlock queries, x-power group), ordered by
+  // estimated cost so the largest start first.
+  std::vector<CvItem> items;
+  std::vector<double> cost;
+  std::vector<int> part_begin(n_sets), part_count(n_sets);
+  int parts = 0;
+  for (int sidx = 0; sidx < n_sets; ++sidx) {
+    const CvSet &st = hs[sidx];
+    part_begin[sidx] = parts;
+    part_count[sidx] = (int)((st.n + kCvChunk - 1) / kCvChunk);
+    for (int ch = 0; ch < part_count[sidx]; ++ch) {
+      const int64_t q0 = (int64_t)ch * kCvChunk;
+      const int64_t q1 = std::min<int64_t>(st.n, q0 + kCvChunk);
+      items.push_back({sidx, 0, parts + ch, 0, 0, 0, q0, q1});
+      cost.push_back((double)(q1 - q0) * st.n);
+    }
+    parts += part_count[sidx];
+    const int64_t *cst = cells.data() + st.cell_begin;
+    for (int cy = 0; cy < st.gy; ++cy)
+      for (int cx = 0; cx < st.gx; ++cx) {
+        const int64_t cb = cst[(int64_t)cy * st.gx + cx], ce = cst[(int64_t)cy * st.gx + cx + 1];
+        for (int64_t q0 = cb; q0 < ce; q0 += kCvQBlock) {
+          const int64_t q1 = std::min<int64_t>(ce, q0 + kCvQBlock);
+          for (int g = 0; g < 4; ++g) {
+            items.push_back({sidx, 1 + g, 0, cx, cy, 0, q0, q1});
+            cost.push_back(0.5 * (double)(q1 - q0) * st.n);
+          }
+        }
+      }
+  }
+  {
+    std::vector<size_t> idx(items.size());
+    for (size_t i = 0; i < idx.size(); ++i) idx[i] = i;
+    std::stable_sort(idx.begin(), idx.end(), [&](size_t p, size_t q) { return cost[p] > cost[q]; });
+    std::vector<CvItem> sorted(items.size());
+    for (size_t i = 0; i < idx.size(); ++i) sorted[i] = items[idx[i]];
+    items.swap(sorted);
+  }
+  std::vector<double> hbuf(2 * kCvMaxH, 0.0);
+  std::copy(hx, hx + n_hx, hbuf.begin());
+  std::copy(hy, hy + n_hy, hbuf.begin() + kCvMaxH);
+  std::vector<unsigned char> luts(2 * kCvLut);
+  const int lut_shift = cv_lut_shift(hx, n_hx, hy, n_hy);
+  long long basex = 0, basey = 0;
+  cv_lut(hx, n_hx, lut_shift, basex, luts.data());
+  cv_lut(hy, n_hy, lut_shift, basey, luts.data() + kCvLut);
+
+  // ---- device buffers -----------------------------------------------------
+  const size_t nb = (size_t)total * sizeof(double);
+  TRY(ensure(c, c->cv_x, nb));
+  TRY(ensure(c, c->cv_y, nb));
+  TRY(ensure(c, c->cv_w, nb));
+  TRY(ensure(c, c->cv_cells, cells.size() * sizeof(int64_t)));
+  TRY(ensure(c, c->cv_sets, hs.size() * sizeof(CvSet)));
+  TRY(ensure(c, c->cv_items, items.size() * sizeof(CvItem)));
+  TRY(ensure(c, c->cv_counter, 64));
+  TRY(ensure(c, c->cv_h, hbuf.size() * sizeof(double)));
+  TRY(ensure(c, c->cv_lut, luts.size()));
+  TRY(ensure(c, c->cv_part, (size_t)parts * 2 * kCvCells * sizeof(double)));
+  TRY(ensure(c, c->cv_hist, (size_t)n_sets * 16 * kCvCells * sizeof(double)));
+  const size_t nout = (size_t)n_sets * n_hx * n_hy;
+  TRY(ensure(c, c->cv_out, 2 * nout * sizeof(double)));
+  TRY(ensure(c, c->cv_parts, 2 * n_sets * sizeof(int)));
+  std::vector<int> pinfo(part_begin);
+  pinfo.insert(pinfo.end(), part_count.begin(), part_count.end());
+  auto up = [&](DevBuf &b, const void *src, size_t bytes) {
+    return cudaMemcpyAsync(b.p, src, bytes, cudaMemcpyHostToDevice, c->stream);
+  };
+  CUDA_TRY(c, up(c->cv_x, X.data(), nb));
+  CUDA_TRY(c, up(c->cv_y, Y.data(), nb));
+  CUDA_TRY(c, up(c->cv_w, Wt.data(), nb));
+  CUDA_TRY(c, up(c->cv_cells, cells.data(), cells.size() * sizeof(int64_t)));
+  CUDA_TRY(c, up(c->cv_sets, hs.data(), hs.size() * sizeof(CvSet)));
+  CUDA_TRY(c, up(c->cv_items, items.data(), items.size() * sizeof(CvItem)));
+  CUDA_TRY(c, up(c->cv_h, hbuf.data(), hbuf.size() * sizeof(double)));
+  CUDA_TRY(c, up(c->cv_lut, luts.data(), luts.size()));
+  CUDA_TRY(c, up(c->cv_parts, pinfo.data(), pinfo.size() * sizeof(int)));
+
+  CvArgs a;
+  a.x = c->cv_x.as<double>();
+  a.y = c->cv_y.as<double>();
+  a.w = c->cv_w.as<double>();
+  a.m = c->cv_w.as<double>();   // non-adaptive: mass = weight
+  a.cell_start = c->cv_cells.as<int64_t>();
+  a.sets = c->cv_sets.as<CvSet>();
+  a.items = c->cv_items.as<CvItem>();
+  a.n_items = (int)items.size();
+  a.counter = c->cv_counter.as<int>();
+  a.nhx = n_hx;
+  a.nhy = n_hy;
+  a.hx = c->cv_h.as<double>();
+  a.hy = c->cv_h.as<double>() + kCvMaxH;
+  a.lutx = c->cv_lut.as<unsigned char>();
+  a.luty = c->cv_lut.as<unsigned char>() + kCvLut;
+  a.lut_basex = basex;
+  a.lut_basey = basey;
+  a.lut_shift = lut_shift;
+  a.r_epan = 4;
+  a.r_conv = 8;
+  a.epan_part = c->cv_part.as<double>();
+  a.conv_hist = c->cv_hist.as<double>();
+  double *lik_dev = c->cv_out.as<double>();
+  double *lsq_dev = lik_dev + nout;
+  const int *pbeg = c->cv_parts.as<int>();
+  const int *pcnt = pbeg + n_sets;
+
+  // ---- one persistent launch + finalisation, captured in a CUDA graph -------
+  const size_t smem = cv_smem_bytes();
+  CUDA_TRY(c, cudaFuncSetAttribute(k_cv_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)smem));
+  const std::vector<uint64_t> key = {
+      (uint64_t)(uintptr_t)a.x, (uint64_t)(uintptr_t)a.cell_start, (uint64_t)(uintptr_t)a.items,
+      (uint64_t)(uintptr_t)a.epan_part, (uint64_t)(uintptr_t)a.conv_hist,
+      (uint64_t)(uintptr_t)lik_dev, (uint64_t)a.n_items, (uint64_t)n_sets, (uint64_t)n_hx,
+      (uint64_t)n_hy, (uint64_t)(uintptr_t)c->stream,
+      (uint64_t)(uintptr_t)a.lutx, (uint64_t)basex, (uint64_t)basey, (uint64_t)lut_shift};
+  auto enqueue = [&]() -> cudaError_t {
+    cudaError_t e = cudaMemsetAsync(a.counter, 0, sizeof(int), c->stream);
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(a.conv_hist, 0, (size_t)n_sets * 16 * kCvCells * sizeof(double),
+                        c->stream);
+    if (e != cudaSuccess) return e;
+    k_cv_batch<<<c->sm_count, kCvBlock, smem, c->stream>>>(a);
+    k_cv_finalize<<<n_sets, kCvBlock, 0, c->stream>>>(a, pbeg, pcnt, lik_dev, lsq_dev);
+    return cudaGetLastError();
+  };
+  const bool capturable = c->stream != nullptr && c->stream != cudaStreamLegacy;
+  if (capturable && (c->cv_graph == nullptr || c->cv_graph_key != key)) {
+    if (c->cv_graph) { cudaGraphExecDestroy(c->cv_graph); c->cv_graph = nullptr; }
+    cudaGraph_t g = nullptr;
+    CUDA_TRY(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = enqueue();
+    cudaError_t e2 = cudaStreamEndCapture(c->stream, &g);
+    if (e != cudaSuccess || e2 != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      cudaGetLastError();
+      return fail(c, BBKDE_CUDA_ERROR, std::string("cv_batch graph capture: ") +
+                                           cudaGetErrorString(e != cudaSuccess ? e : e2));
+    }
+    e = cudaGraphInstantiate(&c->cv_graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+      c->cv_graph = nullptr;
+      return fail(c, BBKDE_CUDA_ERROR, std::string("cudaGraphInstantiate: ") +
+                                           cudaGetErrorString(e));
+    }
+    c->cv_graph_key = key;
+  }
+  CUDA_TRY(c, cudaEventRecord(c->ev0, c->stream));
+  if (capturable) {
+    CUDA_TRY(c, cudaGraphLaunch(c->cv_graph, c->stream));
+  } else {
+    CUDA_TRY(c, enqueue());
+  }
+  CUDA_TRY(c, cudaEventRecord(c->ev1, c->stream));
+  c->launch_total += 2;
+  CUDA_TRY(c, cudaMemcpyAsync(lik_out, lik_dev, nout * sizeof(double), cudaMemcpyDeviceToHost,
+                              c->stream));
+  CUDA_TRY(c, cudaMemcpyAsync(lsq_out, lsq_dev, nout * sizeof(double), cudaMemcpyDeviceToHost,
+                              c->stream));
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  float ms = 0.f;
+  CUDA_TRY(c, cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+  c->last_ms = ms;
+  c->last_pairs = sum_pairs;
+  c->last_launches = 2;
+  return BBKDE_OK;
+}
 
 // ===========================================================================
 // Allocation-free direct evaluation (bbkde_eval_noalloc)

@@ -177,6 +177,33 @@ BBKDE_API int bbkde_likelihood_cv(bbkde_ctx *ctx, const bbkde_kernel_desc *kerne
 BBKDE_API int bbkde_lsq_conv_cv(bbkde_ctx *ctx, const bbkde_kernel_desc *kernel, int precision,
                       double *cv_out);
 
+/* ---- batched cross-validation -------------------------------------------- */
+
+typedef struct {
+  int64_t n;              /* points in this dataset */
+  const double *coords;   /* host, AoS (x0, y0, x1, y1, ...) */
+  const double *weights;  /* host, n raw weights (normalised to sum 1 here); NULL = 1 */
+} bbkde_dataset;
+
+/* Likelihood and least-squares (convolution) cross-validation of many 2-D
+ * datasets over a bandwidth grid hx[0..n_hx) x hy[0..n_hy) in one call:
+ *   lik_out[(s * n_hx + a) * n_hy + b] = likelihood_cross_validate of dataset s
+ *       with the product kernel (hx[a], hy[b])   (KernelDensityImpl.h:215-252)
+ *   lsq_out[...]                       = lsq_convolution_cross_validate
+ *                                                (KernelDensityImpl.h:142-209)
+ * which the reference computes one bandwidth at a time in a host loop
+ * (grid_search/grid_search.cc:370-402). Weights are normalised per dataset and
+ * masses equal weights (non-adaptive), leave-one-out excludes the diagonal.
+ *   BBKDE_EPANECHNIKOV_PRODUCT_2D: one persistent launch for every dataset and
+ *     bandwidth (moment binning, FP64), captured in a CUDA graph and replayed
+ *     for repeated calls of the same shape.
+ *   BBKDE_GAUSSIAN_PRODUCT_2D: exact per-bandwidth loop over the pair sum.
+ * hx and hy must be strictly increasing, positive, at most 64 values each.
+ * Exact-duplicate points are not merged (the reference's Kd-tree merges them). */
+BBKDE_API int bbkde_cv_batch(bbkde_ctx *ctx, int kind, int n_sets, const bbkde_dataset *sets,
+                             int n_hx, const double *hx, int n_hy, const double *hy,
+                             int precision, double *lik_out, double *lsq_out);
+
 /* ---- introspection ------------------------------------------------------- */
 
 /* Device time (ms, CUDA events on the launching stream) and pair count of the
