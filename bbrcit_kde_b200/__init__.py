@@ -36,13 +36,23 @@ EXPORTED = [
     "bbkde_adapt_density", "bbkde_unadapt_density", "bbkde_likelihood_cv",
     "bbkde_lsq_conv_cv", "bbkde_last_launch_stats", "bbkde_launch_count",
     "bbkde_device_info", "bbkde_ctx_set_launch_variant", "bbkde_launch_variants",
-    "bbkde_eval_noalloc", "bbkde_cv_batch",
+    "bbkde_eval_noalloc", "bbkde_cv_batch", "bbkde_surrogate_create", "bbkde_surrogate_destroy",
+    "bbkde_surrogate_last_error", "bbkde_surrogate_num_params", "bbkde_surrogate_set_params",
+    "bbkde_surrogate_get_params", "bbkde_surrogate_gradient", "bbkde_surrogate_train",
+    "bbkde_surrogate_predict", "bbkde_surrogate_predict_device", "bbkde_surrogate_save",
+    "bbkde_surrogate_load",
 ]
 
 
 class Dataset(C.Structure):
     _fields_ = [("n", C.c_int64), ("coords", C.POINTER(C.c_double)),
                 ("weights", C.POINTER(C.c_double))]
+
+
+class TrainConfig(C.Structure):
+    _fields_ = [("steps", C.c_int64), ("batch", C.c_int64), ("lr", C.c_double),
+                ("lr_final", C.c_double), ("beta1", C.c_double), ("beta2", C.c_double),
+                ("eps", C.c_double), ("seed", C.c_uint64)]
 
 
 class KernelDesc(C.Structure):
@@ -121,6 +131,20 @@ def load_library(path: str = LIB_PATH):
     lib.bbkde_device_info.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     lib.bbkde_cv_batch.argtypes = [vp, C.c_int, C.c_int, C.POINTER(Dataset), C.c_int, _dp,
                                    C.c_int, _dp, C.c_int, _dp, _dp]
+    fp = C.POINTER(C.c_float)
+    lib.bbkde_surrogate_create.argtypes = [C.c_int, C.c_uint64, C.POINTER(vp)]
+    lib.bbkde_surrogate_destroy.argtypes = [vp]
+    lib.bbkde_surrogate_last_error.restype = C.c_char_p
+    lib.bbkde_surrogate_last_error.argtypes = [vp]
+    lib.bbkde_surrogate_num_params.restype = C.c_int
+    lib.bbkde_surrogate_set_params.argtypes = [vp, fp, fp]
+    lib.bbkde_surrogate_get_params.argtypes = [vp, fp, fp]
+    lib.bbkde_surrogate_gradient.argtypes = [vp, i64, _dp, _dp, fp, _dp]
+    lib.bbkde_surrogate_train.argtypes = [vp, i64, _dp, _dp, C.POINTER(TrainConfig), _dp]
+    lib.bbkde_surrogate_predict.argtypes = [vp, i64, _dp, _dp]
+    lib.bbkde_surrogate_predict_device.argtypes = [vp, i64, vp, vp]
+    lib.bbkde_surrogate_save.argtypes = [vp, C.c_char_p]
+    lib.bbkde_surrogate_load.argtypes = [vp, C.c_char_p]
     lib.bbkde_eval_noalloc.argtypes = [kd, i64, vp, vp, vp, vp, i64, vp, vp, C.c_int, vp, vp,
                                        C.c_char_p, i64]
     _lib = lib
@@ -300,3 +324,79 @@ def eval_noalloc(desc: KernelDesc, n_ref: int, ref_x: int, ref_y: int | None, re
                                 n_query, query_x, query_y, int(normalized), out, stream,
                                 buf, len(buf))
     return rc, buf.value.decode()
+
+
+def _fp(a):
+    return None if a is None else a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+class Surrogate:
+    """The learned log-density network (2 -> 128 -> 128 -> 128 -> 1, SiLU)."""
+
+    def __init__(self, device: int = 0, seed: int = 1):
+        self.lib = load_library()
+        h = C.c_void_p()
+        rc = self.lib.bbkde_surrogate_create(device, seed, C.byref(h))
+        if rc != OK:
+            raise BBKDEError(rc, "bbkde_surrogate_create failed: " +
+                             self.lib.bbkde_status_string(rc).decode())
+        self.h = h
+        self.n_params = int(self.lib.bbkde_surrogate_num_params())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.bbkde_surrogate_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc == OK:
+            return
+        msg = (self.lib.bbkde_surrogate_last_error(self.h) or b"").decode()
+        if rc == INVALID_ARGUMENT:
+            raise InvalidArgument(rc, msg)
+        raise BBKDEError(rc, msg)
+
+    def params(self):
+        p = np.empty(self.n_params, dtype=np.float32)
+        norm = np.empty(6, dtype=np.float32)
+        self._check(self.lib.bbkde_surrogate_get_params(self.h, _fp(p), _fp(norm)))
+        return p, norm
+
+    def set_params(self, p, norm=None):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        norm = None if norm is None else np.ascontiguousarray(norm, dtype=np.float32)
+        self._check(self.lib.bbkde_surrogate_set_params(self.h, _fp(p), _fp(norm)))
+
+    def gradient(self, xy, target):
+        xy, target = _c(xy).reshape(-1, 2), _c(target)
+        g = np.empty(self.n_params, dtype=np.float32)
+        loss = C.c_double()
+        self._check(self.lib.bbkde_surrogate_gradient(self.h, xy.shape[0], _p(xy), _p(target),
+                                                      _fp(g), C.byref(loss)))
+        return g, loss.value
+
+    def train(self, xy, target, steps=2000, batch=8192, lr=2e-3, lr_final=1e-5, seed=7):
+        xy, target = _c(xy).reshape(-1, 2), _c(target)
+        cfg = TrainConfig(steps, batch, lr, lr_final, 0.0, 0.0, 0.0, seed)
+        loss = C.c_double()
+        self._check(self.lib.bbkde_surrogate_train(self.h, xy.shape[0], _p(xy), _p(target),
+                                                   C.byref(cfg), C.byref(loss)))
+        return loss.value
+
+    def predict(self, xy):
+        xy = _c(xy).reshape(-1, 2)
+        out = np.empty(xy.shape[0])
+        self._check(self.lib.bbkde_surrogate_predict(self.h, xy.shape[0], _p(xy), _p(out)))
+        return out
+
+    def save(self, path):
+        self._check(self.lib.bbkde_surrogate_save(self.h, str(path).encode()))
+
+    def load(self, path):
+        self._check(self.lib.bbkde_surrogate_load(self.h, str(path).encode()))

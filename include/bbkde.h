@@ -204,6 +204,63 @@ BBKDE_API int bbkde_cv_batch(bbkde_ctx *ctx, int kind, int n_sets, const bbkde_d
                              int n_hx, const double *hx, int n_hy, const double *hy,
                              int precision, double *lik_out, double *lsq_out);
 
+/* ---- learned log-density surrogate ---------------------------------------- */
+
+/* A small network (2 -> 128 -> 128 -> 128 -> 1, SiLU) for log-density, trained
+ * with hand-written BF16 tensor-core forward / backward kernels (FP32 accumulate)
+ * on exact densities computed by the pair sums, and evaluated with a fused BF16
+ * tensor-core inference kernel. No reference counterpart: the reference evaluates
+ * every query with a density sum (KernelDensityImpl.h:1157-1231); the surrogate
+ * stands in for that sum on dense query grids, with the exact sum as its fallback
+ * and judge (bbkde_surrogate_eval_grid). */
+typedef struct bbkde_surrogate bbkde_surrogate;
+
+typedef struct {
+  int64_t steps;     /* optimiser steps */
+  int64_t batch;     /* points per step (>= 64) */
+  double lr;         /* initial learning rate (Adam) */
+  double lr_final;   /* learning rate at the last step (cosine decay) */
+  double beta1, beta2, eps;   /* Adam; 0 selects 0.9, 0.999, 1e-8 */
+  uint64_t seed;     /* mini-batch sampling seed */
+} bbkde_train_config;
+
+/* Create a surrogate on `device` with seeded Glorot-uniform weights. */
+BBKDE_API int bbkde_surrogate_create(int device, uint64_t seed, bbkde_surrogate **out);
+BBKDE_API int bbkde_surrogate_destroy(bbkde_surrogate *s);
+BBKDE_API const char *bbkde_surrogate_last_error(const bbkde_surrogate *s);
+
+/* Number of FP32 parameters: W1[128][2] b1[128] W2[128][128] b2[128]
+ * W3[128][128] b3[128] w4[128] b4. norm6 = {cx, cy, sx, sy, mu, sigma}: the
+ * network sees ((x - cx) sx, (y - cy) sy) and predicts (log f - mu) / sigma. */
+BBKDE_API int bbkde_surrogate_num_params(void);
+BBKDE_API int bbkde_surrogate_set_params(bbkde_surrogate *s, const float *params,
+                                         const float *norm6);
+BBKDE_API int bbkde_surrogate_get_params(bbkde_surrogate *s, float *params, float *norm6);
+
+/* Gradient of the mean squared error in normalised units over all n points
+ * (host xy AoS, host log-density targets), one forward + backward pass on the
+ * tensor cores without an update; grad has bbkde_surrogate_num_params() floats. */
+BBKDE_API int bbkde_surrogate_gradient(bbkde_surrogate *s, int64_t n, const double *xy,
+                                       const double *target, float *grad, double *loss);
+
+/* Train on n (xy, log-density) rows; sets the input / output normalisation from
+ * the data. final_loss = the last step's mini-batch loss (normalised units). */
+BBKDE_API int bbkde_surrogate_train(bbkde_surrogate *s, int64_t n, const double *xy,
+                                    const double *target, const bbkde_train_config *cfg,
+                                    double *final_loss);
+
+/* Predicted log-density: host arrays, synchronous. */
+BBKDE_API int bbkde_surrogate_predict(bbkde_surrogate *s, int64_t n, const double *xy,
+                                      double *out);
+/* Device float2 points -> device floats, asynchronous on the surrogate's stream. */
+BBKDE_API int bbkde_surrogate_predict_device(bbkde_surrogate *s, int64_t n, const void *xy_f2,
+                                             float *out);
+
+/* Checkpoint: magic "BBKDEMLP", version, parameter count, normalisation, FP32
+ * parameters (little-endian). */
+BBKDE_API int bbkde_surrogate_save(bbkde_surrogate *s, const char *path);
+BBKDE_API int bbkde_surrogate_load(bbkde_surrogate *s, const char *path);
+
 /* ---- introspection ------------------------------------------------------- */
 
 /* Device time (ms, CUDA events on the launching stream) and pair count of the
