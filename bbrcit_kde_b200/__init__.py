@@ -40,8 +40,12 @@ EXPORTED = [
     "bbkde_surrogate_last_error", "bbkde_surrogate_num_params", "bbkde_surrogate_set_params",
     "bbkde_surrogate_get_params", "bbkde_surrogate_gradient", "bbkde_surrogate_train",
     "bbkde_surrogate_predict", "bbkde_surrogate_predict_device", "bbkde_surrogate_save",
-    "bbkde_surrogate_load",
+    "bbkde_surrogate_load", "bbkde_surrogate_set_inference", "bbkde_eval_culled",
+    "bbkde_eval_grid",
 ]
+
+# Dense-grid modes (bbkde_grid_config.mode).
+GRID_EXACT, GRID_SURROGATE, GRID_ANCHORED = 0, 1, 2
 
 
 class Dataset(C.Structure):
@@ -53,6 +57,34 @@ class TrainConfig(C.Structure):
     _fields_ = [("steps", C.c_int64), ("batch", C.c_int64), ("lr", C.c_double),
                 ("lr_final", C.c_double), ("beta1", C.c_double), ("beta2", C.c_double),
                 ("eps", C.c_double), ("seed", C.c_uint64)]
+
+
+class CullStats(C.Structure):
+    _fields_ = [("kernel_ms", C.c_double), ("pairs", C.c_double), ("full_pairs", C.c_double),
+                ("max_bound_ratio", C.c_double)]
+
+
+class Grid(C.Structure):
+    _fields_ = [("nx", C.c_int64), ("ny", C.c_int64), ("x0", C.c_double), ("x1", C.c_double),
+                ("y0", C.c_double), ("y1", C.c_double)]
+
+
+class GridConfig(C.Structure):
+    _fields_ = [("mode", C.c_int), ("tile", C.c_int), ("probes", C.c_int),
+                ("exact_culled", C.c_int), ("rel_tol", C.c_double), ("low_frac", C.c_double),
+                ("cull_rel", C.c_double)]
+
+
+class GridStats(C.Structure):
+    _fields_ = [("tiles", C.c_int64), ("tiles_low", C.c_int64), ("tiles_flagged", C.c_int64),
+                ("tiles_surrogate", C.c_int64), ("exact_points", C.c_int64),
+                ("pairs", C.c_double), ("max_probe_err", C.c_double),
+                ("max_bound_ratio", C.c_double), ("ms_total", C.c_double),
+                ("ms_predict", C.c_double), ("ms_probe", C.c_double),
+                ("ms_fallback", C.c_double)]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
 
 
 class KernelDesc(C.Structure):
@@ -147,6 +179,11 @@ def load_library(path: str = LIB_PATH):
     lib.bbkde_surrogate_load.argtypes = [vp, C.c_char_p]
     lib.bbkde_eval_noalloc.argtypes = [kd, i64, vp, vp, vp, vp, i64, vp, vp, C.c_int, vp, vp,
                                        C.c_char_p, i64]
+    lib.bbkde_surrogate_set_inference.argtypes = [vp, C.c_int]
+    lib.bbkde_eval_culled.argtypes = [vp, kd, C.c_int, C.c_double, vp, C.c_int,
+                                      C.POINTER(CullStats)]
+    lib.bbkde_eval_grid.argtypes = [vp, vp, kd, C.POINTER(Grid), C.POINTER(GridConfig), vp,
+                                    C.POINTER(GridStats)]
     _lib = lib
     return lib
 
@@ -296,6 +333,29 @@ class Context:
                                             _p(hy), precision, _p(lik), _p(lsq)))
         return lik[:n], lsq[:n]
 
+    def eval_culled(self, desc: KernelDesc, rel_tol=1e-7, normalized=True):
+        """Culled direct evaluation of every query; returns (values, CullStats)."""
+        n = self.size(QUERY)
+        out = np.empty(max(n, 1))
+        st = CullStats()
+        self._check(self.lib.bbkde_eval_culled(self.h, C.byref(desc), int(normalized), rel_tol,
+                                               out.ctypes.data, 0, C.byref(st)))
+        return out[:n], st
+
+    def eval_grid(self, desc: KernelDesc, grid, out_ptr: int, surrogate=None,
+                  mode=GRID_EXACT, tile=16, probes=5, exact_culled=True, rel_tol=5e-4,
+                  low_frac=1e-4, cull_rel=1e-7) -> GridStats:
+        """Density on a dense grid into device memory out_ptr (nx * ny doubles).
+
+        grid = (nx, ny, x0, x1, y0, y1). Returns the GridStats."""
+        g = Grid(*grid)
+        cfg = GridConfig(mode, tile, probes, int(exact_culled), rel_tol, low_frac, cull_rel)
+        st = GridStats()
+        sh = surrogate.h if surrogate is not None else None
+        self._check(self.lib.bbkde_eval_grid(self.h, sh, C.byref(desc), C.byref(g), C.byref(cfg),
+                                             out_ptr, C.byref(st)))
+        return st
+
     def set_launch_variant(self, variant: int):
         """-1 = autotune (default); 0..n-1 forces a launch shape."""
         self._check(self.lib.bbkde_ctx_set_launch_variant(self.h, variant))
@@ -394,6 +454,10 @@ class Surrogate:
         out = np.empty(xy.shape[0])
         self._check(self.lib.bbkde_surrogate_predict(self.h, xy.shape[0], _p(xy), _p(out)))
         return out
+
+    def set_inference(self, split_activations: bool):
+        """False: BF16 activations (as trained); True: two-term BF16 activations."""
+        self._check(self.lib.bbkde_surrogate_set_inference(self.h, int(split_activations)))
 
     def save(self, path):
         self._check(self.lib.bbkde_surrogate_save(self.h, str(path).encode()))

@@ -21,9 +21,14 @@
 #include <tuple>
 #include <vector>
 
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_select.cuh>
+
 #include "../../include/bbkde.h"
 #include "kde_device.cuh"
 #include "kde_cv_batch.cuh"
+#include "kde_culled.cuh"
+#include "kde_grid.cuh"
 
 using namespace bbkde;
 
@@ -69,6 +74,14 @@ struct PackCache {
   DevBuf rec, ext;
 };
 
+// Morton-sorted FP32 records of the reference set and their culling tiles,
+// valid for the packed records with the same key.
+struct CullCache {
+  PackKey key;
+  DevBuf rec, ext, tiles;
+  int n_tiles = 0;
+};
+
 struct QueryCache {
   int set = -1;
   uint64_t coord_version = ~0ull;
@@ -101,6 +114,15 @@ struct bbkde_ctx {
       cv_part, cv_hist, cv_out, cv_parts;
   cudaGraphExec_t cv_graph = nullptr;
   std::vector<uint64_t> cv_graph_key;
+  // culled evaluation: sorted references, sort scratch, sorted queries, per-block
+  // bounds; dense-grid pipeline buffers
+  CullCache cull;
+  DevBuf ms_keys, ms_keys2, ms_perm, ms_perm2, ms_box, ms_tmp, cq_x, cq_y, cq_out, cb_bound,
+      cb_smin, cb_tiles, cb_stats;
+  DevBuf gr_pred, gr_order, gr_tmin, gr_tmax, gr_bad, gr_terr, gr_flag, gr_flag_ord, gr_list,
+      gr_nsel, gr_counts, gr_gmax, gr_anc_order, gr_anc_exact, gr_anc_net, gr_resid, gr_pq_x,
+      gr_pq_y, gr_pq_idx, gr_pq_exact;
+  cudaEvent_t ev3 = nullptr;
   std::string err;
 };
 
@@ -656,7 +678,7 @@ int bbkde_ctx_create(int device, bbkde_ctx **out) {
     }
     c->stream = c->own_stream;
     if (cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
-        cudaEventCreate(&c->ev2) != cudaSuccess) {
+        cudaEventCreate(&c->ev2) != cudaSuccess || cudaEventCreate(&c->ev3) != cudaSuccess) {
       rc = BBKDE_CUDA_ERROR;
       break;
     }
@@ -689,7 +711,17 @@ int bbkde_ctx_destroy(bbkde_ctx *c) {
                     &c->cv_counter, &c->cv_h, &c->cv_lut, &c->cv_part, &c->cv_hist,
                     &c->cv_out, &c->cv_parts})
     release(*b);
+  for (DevBuf *b : {&c->cull.rec, &c->cull.ext, &c->cull.tiles, &c->ms_keys, &c->ms_keys2,
+                    &c->ms_perm, &c->ms_perm2, &c->ms_box, &c->ms_tmp, &c->cq_x, &c->cq_y,
+                    &c->cq_out, &c->cb_bound, &c->cb_smin, &c->cb_tiles, &c->cb_stats,
+                    &c->gr_pred, &c->gr_order, &c->gr_tmin, &c->gr_tmax, &c->gr_bad,
+                    &c->gr_terr, &c->gr_flag, &c->gr_flag_ord, &c->gr_list, &c->gr_nsel,
+                    &c->gr_counts, &c->gr_gmax, &c->gr_anc_order, &c->gr_anc_exact,
+                    &c->gr_anc_net, &c->gr_resid, &c->gr_pq_x, &c->gr_pq_y, &c->gr_pq_idx,
+                    &c->gr_pq_exact})
+    release(*b);
   if (c->cv_graph) cudaGraphExecDestroy(c->cv_graph);
+  if (c->ev3) cudaEventDestroy(c->ev3);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->ev2) cudaEventDestroy(c->ev2);
@@ -1251,6 +1283,503 @@ extern "C" int bbkde_cv_batch(bbkde_ctx *c, int kind, int n_sets, const bbkde_da
   c->last_ms = ms;
   c->last_pairs = sum_pairs;
   c->last_launches = 2;
+  return BBKDE_OK;
+}
+
+// ===========================================================================
+// Culled direct evaluation (bbkde_eval_culled) and dense grids (bbkde_eval_grid)
+// ===========================================================================
+namespace bbkde {
+int surrogate_infer(bbkde_surrogate *s, cudaStream_t st, int64_t n, const float2 *xy,
+                    int64_t gnx, double gx0, double gdx, double gy0, double gdy, float *out);
+int surrogate_device(const bbkde_surrogate *s);
+}  // namespace bbkde
+
+namespace {
+
+// Near-field width of the culled sum in log2 units: the first pass sums every
+// tile whose bound is within 2^-24 of the block's largest.
+constexpr float kCullCut = 24.0f;
+
+// Morton order of n points (x[i * stride], y[i * stride]; y null for 1-D):
+// *perm_out = the sorted permutation (valid until the next sort).
+int morton_sort(bbkde_ctx *c, const float *x, const float *y, int stride, int64_t n,
+                const int **perm_out) {
+  if (n > INT32_MAX) return fail(c, BBKDE_OUT_OF_RANGE, "more than 2^31 - 1 points");
+  TRY(ensure(c, c->ms_keys, (size_t)n * sizeof(unsigned)));
+  TRY(ensure(c, c->ms_keys2, (size_t)n * sizeof(unsigned)));
+  TRY(ensure(c, c->ms_perm, (size_t)n * sizeof(int)));
+  TRY(ensure(c, c->ms_perm2, (size_t)n * sizeof(int)));
+  TRY(ensure(c, c->ms_box, 4 * sizeof(unsigned)));
+  CUDA_TRY(c, cudaMemsetAsync(c->ms_box.p, 0xff, 2 * sizeof(unsigned), c->stream));
+  CUDA_TRY(c, cudaMemsetAsync(c->ms_box.as<unsigned>() + 2, 0, 2 * sizeof(unsigned), c->stream));
+  const unsigned gb = std::min<unsigned>(grid1d(n), (unsigned)c->sm_count * 8);
+  k_bbox<<<gb, 256, 0, c->stream>>>(x, y, stride, n, c->ms_box.as<unsigned>());
+  COUNT_LAUNCH(c);
+  k_morton<<<grid1d(n), 256, 0, c->stream>>>(x, y, stride, n, c->ms_box.as<unsigned>(),
+                                             c->ms_keys.as<unsigned>(), c->ms_perm.as<int>());
+  COUNT_LAUNCH(c);
+  CUDA_TRY(c, cudaGetLastError());
+  size_t tmp = 0;
+  CUDA_TRY(c, cub::DeviceRadixSort::SortPairs(nullptr, tmp, c->ms_keys.as<unsigned>(),
+                                              c->ms_keys2.as<unsigned>(), c->ms_perm.as<int>(),
+                                              c->ms_perm2.as<int>(), (int)n, 0, 32, c->stream));
+  TRY(ensure(c, c->ms_tmp, tmp));
+  CUDA_TRY(c, cub::DeviceRadixSort::SortPairs(c->ms_tmp.p, tmp, c->ms_keys.as<unsigned>(),
+                                              c->ms_keys2.as<unsigned>(), c->ms_perm.as<int>(),
+                                              c->ms_perm2.as<int>(), (int)n, 0, 32, c->stream));
+  c->launch_total += 4;   // CUB's onesweep radix sort: histogram + passes
+  *perm_out = c->ms_perm2.as<int>();
+  return BBKDE_OK;
+}
+
+// Sorted records and culling tiles of the reference set for `r` (cached).
+int ensure_culled(bbkde_ctx *c, const Resolved &r) {
+  TRY(ensure_pack(c, r, false));
+  CullCache &cc = c->cull;
+  if (cc.key == c->pack32.key) return BBKDE_OK;
+  const int64_t n = c->sets[BBKDE_REFERENCE].n;
+  cc.n_tiles = (int)((n + kRefTile - 1) / kRefTile);
+  if (n > 0) {
+    TRY(ensure(c, cc.rec, (size_t)n * sizeof(float4)));
+    TRY(ensure(c, cc.ext, (size_t)n * sizeof(float)));
+    TRY(ensure(c, cc.tiles, (size_t)cc.n_tiles * sizeof(RefTile)));
+    const float *rx = c->pack32.rec.as<float>();
+    const int *perm = nullptr;
+    TRY(morton_sort(c, rx, r.dim == 2 ? rx + 1 : nullptr, 4, n, &perm));
+    k_gather_rec<<<grid1d(n), 256, 0, c->stream>>>(c->pack32.rec.as<float4>(),
+                                                   c->pack32.ext.as<float>(), perm, n,
+                                                   cc.rec.as<float4>(), cc.ext.as<float>());
+    COUNT_LAUNCH(c);
+    const float *tex = (op_has_extra(r.op) && r.dim == 2) ? cc.ext.as<float>() : nullptr;
+    const unsigned tb = grid1d((int64_t)cc.n_tiles * 32);
+    if (r.dim == 2)
+      k_ref_tiles<2><<<tb, 256, 0, c->stream>>>(cc.rec.as<float4>(), tex, n, cc.n_tiles,
+                                                cc.tiles.as<RefTile>());
+    else
+      k_ref_tiles<1><<<tb, 256, 0, c->stream>>>(cc.rec.as<float4>(), tex, n, cc.n_tiles,
+                                                cc.tiles.as<RefTile>());
+    COUNT_LAUNCH(c);
+    CUDA_TRY(c, cudaGetLastError());
+  }
+  cc.key = c->pack32.key;
+  return BBKDE_OK;
+}
+
+// Launch shapes of the culled sum: 0 = 1024 queries per block (128 threads x 8),
+// 1 = 256 queries per block (64 threads x 4).
+constexpr int kCullQpb[2] = {1024, 256};
+
+template <int OP, int D>
+void launch_cull_op(int shape, unsigned nblk, cudaStream_t st, const CullArgs &a) {
+  if (shape == 0)
+    k_pair_sum_culled<OP, D, 8, 128, 4><<<nblk, 128, 0, st>>>(a);
+  else
+    k_pair_sum_culled<OP, D, 4, 64, 8><<<nblk, 64, 0, st>>>(a);
+}
+
+// One culled (or, with full, complete) sum over nblk query blocks; adds its
+// statistics (pairs at tile granularity, worst bound ratio) to *pairs, *ratio.
+int launch_culled(bbkde_ctx *c, const Resolved &r, int shape, unsigned nblk,
+                  const CullQueries &q, double rel, bool full, double *pairs, double *ratio) {
+  if (nblk == 0) return BBKDE_OK;
+  TRY(ensure(c, c->cb_bound, (size_t)nblk * sizeof(double)));
+  TRY(ensure(c, c->cb_smin, (size_t)nblk * sizeof(double)));
+  TRY(ensure(c, c->cb_tiles, (size_t)nblk * sizeof(int)));
+  TRY(ensure(c, c->cb_stats, 2 * sizeof(double)));
+  CullArgs a;
+  a.refs = c->cull.rec.as<float4>();
+  a.extra = c->cull.ext.as<float>();
+  a.tiles = c->cull.tiles.as<RefTile>();
+  a.n_tiles = c->cull.n_tiles;
+  a.n_ref = c->sets[BBKDE_REFERENCE].n;
+  a.cut = full ? INFINITY : kCullCut;
+  a.rel = rel;
+  a.q = q;
+  a.blk_bound = c->cb_bound.as<double>();
+  a.blk_smin = c->cb_smin.as<double>();
+  a.blk_tiles = c->cb_tiles.as<int>();
+  const bool d2 = r.dim == 2;
+  switch (r.op) {
+    case OP_GAUSS_ISO:
+      d2 ? launch_cull_op<OP_GAUSS_ISO, 2>(shape, nblk, c->stream, a)
+         : launch_cull_op<OP_GAUSS_ISO, 1>(shape, nblk, c->stream, a);
+      break;
+    case OP_GAUSS_PROD: launch_cull_op<OP_GAUSS_PROD, 2>(shape, nblk, c->stream, a); break;
+    case OP_EPAN_ISO:
+      d2 ? launch_cull_op<OP_EPAN_ISO, 2>(shape, nblk, c->stream, a)
+         : launch_cull_op<OP_EPAN_ISO, 1>(shape, nblk, c->stream, a);
+      break;
+    case OP_EPAN_PROD: launch_cull_op<OP_EPAN_PROD, 2>(shape, nblk, c->stream, a); break;
+    default: return fail(c, BBKDE_UNSUPPORTED, "culled sum: unsupported kernel");
+  }
+  COUNT_LAUNCH(c);
+  k_cull_stats<<<1, 256, 0, c->stream>>>(a.blk_bound, a.blk_smin, a.blk_tiles, (int)nblk,
+                                         c->cb_stats.as<double>());
+  COUNT_LAUNCH(c);
+  CUDA_TRY(c, cudaGetLastError());
+  double st[2];
+  CUDA_TRY(c, cudaMemcpyAsync(st, c->cb_stats.p, sizeof(st), cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  if (pairs) *pairs += st[1] * kRefTile * kCullQpb[shape];
+  if (ratio) *ratio = std::max(*ratio, st[0]);
+  return BBKDE_OK;
+}
+
+int culled_kernel_ok(bbkde_ctx *c, const Resolved &r) {
+  if (r.op == OP_EPAN_CONV)
+    return fail(c, BBKDE_UNSUPPORTED,
+                "culled sum: the Epanechnikov convolution kernels are not supported");
+  return BBKDE_OK;
+}
+
+}  // namespace
+
+extern "C" int bbkde_eval_culled(bbkde_ctx *c, const bbkde_kernel_desc *k, int normalized,
+                                 double rel_tol, double *out, int out_on_device,
+                                 bbkde_cull_stats *stats) {
+  TRY(check_ctx(c));
+  if (!out) return fail(c, BBKDE_INVALID_ARGUMENT, "output pointer is NULL");
+  if (!(rel_tol > 0.0 && rel_tol < 1.0))
+    return fail(c, BBKDE_INVALID_ARGUMENT, "rel_tol must be in (0, 1)");
+  Resolved r;
+  TRY(resolve(c, k, r));
+  TRY(culled_kernel_ok(c, r));
+  const PointSet &rs = c->sets[BBKDE_REFERENCE], &qs = c->sets[BBKDE_QUERY];
+  if ((rs.n > 0 && rs.dim != r.dim) || (qs.n > 0 && qs.dim != r.dim))
+    return fail(c, BBKDE_INVALID_ARGUMENT, "point dimension does not match the kernel");
+  bbkde_cull_stats st = {0.0, 0.0, (double)rs.n * (double)qs.n, 0.0};
+  const int64_t nq = qs.n;
+  if (nq == 0) {
+    if (stats) *stats = st;
+    return BBKDE_OK;
+  }
+  double *dst = out;
+  if (!out_on_device) {
+    TRY(ensure(c, c->out_dev, (size_t)nq * sizeof(double)));
+    dst = c->out_dev.as<double>();
+  }
+  if (rs.n == 0) {
+    CUDA_TRY(c, cudaMemsetAsync(dst, 0, (size_t)nq * sizeof(double), c->stream));
+  } else {
+    TRY(ensure_culled(c, r));
+    const void *qx = nullptr, *qy = nullptr;
+    TRY(ensure_queries(c, BBKDE_QUERY, false, &qx, &qy));
+    const float *fx = static_cast<const float *>(qx), *fy = static_cast<const float *>(qy);
+    const int *perm = nullptr;
+    TRY(morton_sort(c, fx, r.dim == 2 ? fy : nullptr, 1, nq, &perm));
+    TRY(ensure(c, c->cq_x, (size_t)nq * sizeof(float)));
+    TRY(ensure(c, c->cq_y, (size_t)nq * sizeof(float)));
+    TRY(ensure(c, c->cq_out, (size_t)nq * sizeof(double)));
+    k_gather_xy<<<grid1d(nq), 256, 0, c->stream>>>(fx, r.dim == 2 ? fy : nullptr, perm, nq,
+                                                   c->cq_x.as<float>(), c->cq_y.as<float>());
+    COUNT_LAUNCH(c);
+    CullQueries q = {};
+    q.mode = 0;
+    q.qx = c->cq_x.as<float>();
+    q.qy = c->cq_y.as<float>();
+    q.count = nq;
+    q.out = c->cq_out.as<double>();
+    q.scale = normalized ? r.norm : 1.0;
+    const unsigned nblk = (unsigned)((nq + kCullQpb[0] - 1) / kCullQpb[0]);
+    CUDA_TRY(c, cudaEventRecord(c->ev0, c->stream));
+    TRY(launch_culled(c, r, 0, nblk, q, rel_tol, false, &st.pairs, &st.max_bound_ratio));
+    CUDA_TRY(c, cudaEventRecord(c->ev1, c->stream));
+    k_scatter<<<grid1d(nq), 256, 0, c->stream>>>(c->cq_out.as<double>(), perm, nq, dst);
+    COUNT_LAUNCH(c);
+    CUDA_TRY(c, cudaGetLastError());
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    float ms = 0.f;
+    CUDA_TRY(c, cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    st.kernel_ms = ms;
+  }
+  if (!out_on_device)
+    CUDA_TRY(c, cudaMemcpyAsync(out, dst, (size_t)nq * sizeof(double), cudaMemcpyDeviceToHost,
+                                c->stream));
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  c->last_ms = st.kernel_ms;
+  c->last_pairs = st.pairs;
+  c->last_launches = 2;
+  if (stats) *stats = st;
+  return BBKDE_OK;
+}
+
+namespace {
+
+// Tile numbers of g in Morton order of their coordinates -> order (ntiles ints).
+int tile_order(bbkde_ctx *c, const GridDesc &g, DevBuf &order) {
+  const int64_t nt = (int64_t)g.ntx * g.nty;
+  TRY(ensure(c, c->ms_keys, (size_t)nt * sizeof(unsigned)));
+  TRY(ensure(c, c->ms_keys2, (size_t)nt * sizeof(unsigned)));
+  TRY(ensure(c, c->ms_perm, (size_t)nt * sizeof(int)));
+  TRY(ensure(c, order, (size_t)nt * sizeof(int)));
+  k_tile_keys<<<grid1d(nt), 256, 0, c->stream>>>(g, c->ms_keys.as<unsigned>(),
+                                                 c->ms_perm.as<int>());
+  COUNT_LAUNCH(c);
+  CUDA_TRY(c, cudaGetLastError());
+  size_t tmp = 0;
+  CUDA_TRY(c, cub::DeviceRadixSort::SortPairs(nullptr, tmp, c->ms_keys.as<unsigned>(),
+                                              c->ms_keys2.as<unsigned>(), c->ms_perm.as<int>(),
+                                              order.as<int>(), (int)nt, 0, 32, c->stream));
+  TRY(ensure(c, c->ms_tmp, tmp));
+  CUDA_TRY(c, cub::DeviceRadixSort::SortPairs(c->ms_tmp.p, tmp, c->ms_keys.as<unsigned>(),
+                                              c->ms_keys2.as<unsigned>(), c->ms_perm.as<int>(),
+                                              order.as<int>(), (int)nt, 0, 32, c->stream));
+  c->launch_total += 4;
+  return BBKDE_OK;
+}
+
+GridDesc make_grid(int64_t nx, int64_t ny, double x0, double dx, double y0, double dy, int tile) {
+  GridDesc g;
+  g.nx = nx;
+  g.ny = ny;
+  g.x0 = x0;
+  g.dx = dx;
+  g.y0 = y0;
+  g.dy = dy;
+  g.tile = tile;
+  g.ntx = (int)((nx + tile - 1) / tile);
+  g.nty = (int)((ny + tile - 1) / tile);
+  return g;
+}
+
+// Exact sums at the points of every listed tile of g (results row-major into out).
+int grid_exact(bbkde_ctx *c, const Resolved &r, const GridDesc &g, const int *list, int64_t n,
+               double rel, bool full, double *out, double *pairs, double *ratio) {
+  CullQueries q = {};
+  q.mode = 1;
+  q.tile_list = list;
+  q.tile = g.tile;
+  q.ntx = g.ntx;
+  q.gnx = g.nx;
+  q.gny = g.ny;
+  q.gx0 = g.x0;
+  q.gdx = g.dx;
+  q.gy0 = g.y0;
+  q.gdy = g.dy;
+  q.out = out;
+  q.scale = r.norm;
+  const int shape = g.tile == 32 ? 0 : 1;
+  return launch_culled(c, r, shape, (unsigned)n, q, rel, full, pairs, ratio);
+}
+
+}  // namespace
+
+extern "C" int bbkde_eval_grid(bbkde_ctx *c, bbkde_surrogate *sur, const bbkde_kernel_desc *k,
+                               const bbkde_grid *grid, const bbkde_grid_config *cfg,
+                               double *out, bbkde_grid_stats *stats) {
+  TRY(check_ctx(c));
+  if (!grid || !cfg || !out) return fail(c, BBKDE_INVALID_ARGUMENT, "NULL argument");
+  if (grid->nx < 1 || grid->ny < 1 || !(grid->x1 > grid->x0) || !(grid->y1 > grid->y0) ||
+      !std::isfinite(grid->x0) || !std::isfinite(grid->x1) || !std::isfinite(grid->y0) ||
+      !std::isfinite(grid->y1))
+    return fail(c, BBKDE_INVALID_ARGUMENT, "grid: need nx, ny >= 1 and finite x0 < x1, y0 < y1");
+  const int mode = cfg->mode, T = cfg->tile, P = cfg->probes;
+  if (mode < BBKDE_GRID_EXACT || mode > BBKDE_GRID_ANCHORED)
+    return fail(c, BBKDE_INVALID_ARGUMENT, "grid: unknown mode");
+  if (T != 16 && T != 32) return fail(c, BBKDE_INVALID_ARGUMENT, "grid: tile must be 16 or 32");
+  if (P != 1 && P != 5 && P != 9)
+    return fail(c, BBKDE_INVALID_ARGUMENT, "grid: probes must be 1, 5 or 9");
+  if (!(cfg->rel_tol > 0) || !(cfg->low_frac >= 0 && cfg->low_frac < 1) ||
+      !(cfg->cull_rel > 0 && cfg->cull_rel < 1))
+    return fail(c, BBKDE_INVALID_ARGUMENT,
+                "grid: need rel_tol > 0, 0 <= low_frac < 1, 0 < cull_rel < 1");
+  if (mode == BBKDE_GRID_SURROGATE && !sur)
+    return fail(c, BBKDE_INVALID_ARGUMENT, "grid: surrogate mode needs a surrogate");
+  if (mode != BBKDE_GRID_EXACT && sur && bbkde::surrogate_device(sur) != c->device)
+    return fail(c, BBKDE_INVALID_ARGUMENT, "grid: surrogate lives on another device");
+  Resolved r;
+  TRY(resolve(c, k, r));
+  TRY(culled_kernel_ok(c, r));
+  if (r.dim != 2) return fail(c, BBKDE_INVALID_ARGUMENT, "grid: the kernel must be 2-D");
+  const PointSet &rs = c->sets[BBKDE_REFERENCE];
+  if (rs.n > 0 && rs.dim != 2)
+    return fail(c, BBKDE_INVALID_ARGUMENT, "grid: the reference set must be 2-D");
+  const GridDesc g = make_grid(grid->nx, grid->ny, grid->x0, (grid->x1 - grid->x0) / grid->nx,
+                               grid->y0, (grid->y1 - grid->y0) / grid->ny, T);
+  if (g.ntx > 65535 || g.nty > 65535 || (int64_t)g.ntx * g.nty > (int64_t)1 << 30)
+    return fail(c, BBKDE_OUT_OF_RANGE, "grid: too many tiles");
+  const int64_t npts = g.nx * g.ny, ntiles = (int64_t)g.ntx * g.nty;
+  const bool full = cfg->exact_culled == 0;
+  bbkde_grid_stats st = {};
+  st.tiles = ntiles;
+  if (rs.n == 0) {
+    CUDA_TRY(c, cudaMemsetAsync(out, 0, (size_t)npts * sizeof(double), c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    st.tiles_flagged = ntiles;
+    if (stats) *stats = st;
+    return BBKDE_OK;
+  }
+  TRY(ensure_culled(c, r));
+  TRY(tile_order(c, g, c->gr_order));
+  TRY(ensure(c, c->gr_flag, (size_t)ntiles * sizeof(int)));
+  TRY(ensure(c, c->gr_flag_ord, (size_t)ntiles * sizeof(int)));
+  TRY(ensure(c, c->gr_list, (size_t)ntiles * sizeof(int)));
+  TRY(ensure(c, c->gr_nsel, sizeof(int)));
+  TRY(ensure(c, c->gr_counts, 3 * sizeof(unsigned long long)));
+  TRY(ensure(c, c->gr_gmax, sizeof(float)));
+  TRY(ensure(c, c->gr_tmin, (size_t)ntiles * sizeof(float)));
+  TRY(ensure(c, c->gr_tmax, (size_t)ntiles * sizeof(float)));
+  TRY(ensure(c, c->gr_bad, (size_t)ntiles * sizeof(int)));
+  TRY(ensure(c, c->gr_terr, (size_t)ntiles * sizeof(unsigned)));
+  CUDA_TRY(c, cudaMemsetAsync(c->gr_counts.p, 0, 3 * sizeof(unsigned long long), c->stream));
+  CUDA_TRY(c, cudaEventRecord(c->ev0, c->stream));
+
+  FlagArgs fa;
+  fa.g = g;
+  fa.order = c->gr_order.as<int>();
+  fa.tmin = c->gr_tmin.as<float>();
+  fa.bad = c->gr_bad.as<int>();
+  fa.terr = c->gr_terr.as<unsigned>();
+  fa.gmax = c->gr_gmax.as<float>();
+  fa.log_low = cfg->low_frac > 0 ? (float)std::log(cfg->low_frac) : -INFINITY;
+  fa.rel_tol = (float)cfg->rel_tol;
+  fa.all = mode == BBKDE_GRID_EXACT;
+  fa.flag = c->gr_flag.as<int>();
+  fa.flag_ord = c->gr_flag_ord.as<int>();
+  fa.counts = c->gr_counts.as<unsigned long long>();
+
+  if (mode == BBKDE_GRID_EXACT) {
+    CUDA_TRY(c, cudaEventRecord(c->ev1, c->stream));
+    CUDA_TRY(c, cudaEventRecord(c->ev2, c->stream));
+  } else {
+    // 1. Prediction at every point (log-density).
+    TRY(ensure(c, c->gr_pred, (size_t)npts * sizeof(float)));
+    float *pred = c->gr_pred.as<float>();
+    if (sur) {
+      TRY(bbkde::surrogate_infer(sur, c->stream, npts, nullptr, g.nx, g.x0, g.dx, g.y0, g.dy,
+                                 pred) == BBKDE_OK
+              ? BBKDE_OK
+              : fail(c, BBKDE_CUDA_ERROR, "grid: surrogate inference failed"));
+      COUNT_LAUNCH(c);
+    } else {
+      CUDA_TRY(c, cudaMemsetAsync(pred, 0, (size_t)npts * sizeof(float), c->stream));
+    }
+    const float *resid = nullptr;
+    int64_t n_anchor = 0;
+    if (mode == BBKDE_GRID_ANCHORED) {
+      // Anchors at the tile corners: a grid offset by half a point spacing.
+      const GridDesc ga = make_grid(g.ntx + 1, g.nty + 1, g.x0 - 0.5 * g.dx, T * g.dx,
+                                    g.y0 - 0.5 * g.dy, T * g.dy, 16);
+      n_anchor = ga.nx * ga.ny;
+      TRY(ensure(c, c->gr_anc_exact, (size_t)n_anchor * sizeof(double)));
+      TRY(ensure(c, c->gr_anc_net, (size_t)n_anchor * sizeof(float)));
+      TRY(ensure(c, c->gr_resid, (size_t)n_anchor * sizeof(float)));
+      if (sur) {
+        TRY(bbkde::surrogate_infer(sur, c->stream, n_anchor, nullptr, ga.nx, ga.x0, ga.dx, ga.y0,
+                                   ga.dy, c->gr_anc_net.as<float>()) == BBKDE_OK
+                ? BBKDE_OK
+                : fail(c, BBKDE_CUDA_ERROR, "grid: surrogate inference failed"));
+        COUNT_LAUNCH(c);
+      }
+      TRY(tile_order(c, ga, c->gr_anc_order));
+      TRY(grid_exact(c, r, ga, c->gr_anc_order.as<int>(), (int64_t)ga.ntx * ga.nty,
+                     cfg->cull_rel, full, c->gr_anc_exact.as<double>(), &st.pairs,
+                     &st.max_bound_ratio));
+      k_anchor_residual<<<grid1d(n_anchor), 256, 0, c->stream>>>(
+          c->gr_anc_exact.as<double>(), sur ? c->gr_anc_net.as<float>() : nullptr, n_anchor,
+          c->gr_resid.as<float>());
+      COUNT_LAUNCH(c);
+      resid = c->gr_resid.as<float>();
+    }
+    k_tile_reduce<<<(unsigned)ntiles, 256, 0, c->stream>>>(g, pred, resid, c->gr_tmin.as<float>(),
+                                                         c->gr_tmax.as<float>(),
+                                                         c->gr_bad.as<int>());
+    COUNT_LAUNCH(c);
+    k_max_finite<<<1, 1024, 0, c->stream>>>(c->gr_tmax.as<float>(), (int)ntiles,
+                                            c->gr_gmax.as<float>());
+    COUNT_LAUNCH(c);
+    CUDA_TRY(c, cudaGetLastError());
+    CUDA_TRY(c, cudaEventRecord(c->ev1, c->stream));
+    // 2. Held-out probes, exact, in Morton tile order (compact query blocks).
+    const int64_t np = ntiles * P;
+    TRY(ensure(c, c->gr_pq_x, (size_t)np * sizeof(float)));
+    TRY(ensure(c, c->gr_pq_y, (size_t)np * sizeof(float)));
+    TRY(ensure(c, c->gr_pq_idx, (size_t)np * sizeof(int64_t)));
+    TRY(ensure(c, c->gr_pq_exact, (size_t)np * sizeof(double)));
+    k_make_probes<<<grid1d(np), 256, 0, c->stream>>>(g, c->gr_order.as<int>(), P,
+                                                     c->gr_pq_x.as<float>(), c->gr_pq_y.as<float>(),
+                                                     c->gr_pq_idx.as<int64_t>());
+    COUNT_LAUNCH(c);
+    CullQueries q = {};
+    q.mode = 0;
+    q.qx = c->gr_pq_x.as<float>();
+    q.qy = c->gr_pq_y.as<float>();
+    q.count = np;
+    q.out = c->gr_pq_exact.as<double>();
+    q.scale = r.norm;
+    TRY(launch_culled(c, r, 1, (unsigned)((np + kCullQpb[1] - 1) / kCullQpb[1]), q, cfg->cull_rel,
+                      full, &st.pairs, &st.max_bound_ratio));
+    CUDA_TRY(c, cudaMemsetAsync(c->gr_terr.p, 0, (size_t)ntiles * sizeof(unsigned), c->stream));
+    k_probe_check<<<grid1d(np), 256, 0, c->stream>>>(pred, c->gr_pq_idx.as<int64_t>(),
+                                                     c->gr_pq_exact.as<double>(),
+                                                     c->gr_order.as<int>(), P, np,
+                                                     c->gr_terr.as<unsigned>());
+    COUNT_LAUNCH(c);
+    CUDA_TRY(c, cudaGetLastError());
+    CUDA_TRY(c, cudaEventRecord(c->ev2, c->stream));
+    st.exact_points = n_anchor + np;
+  }
+  // 3. Decisions, predicted values, exact fallback on the flagged tiles.
+  k_flag_tiles<<<grid1d(ntiles), 256, 0, c->stream>>>(fa);
+  COUNT_LAUNCH(c);
+  if (mode != BBKDE_GRID_EXACT) {
+    const unsigned ab = std::min<unsigned>(grid1d(npts), (unsigned)c->sm_count * 16);
+    k_apply<<<ab, 256, 0, c->stream>>>(g, c->gr_pred.as<float>(), c->gr_flag.as<int>(), out);
+    COUNT_LAUNCH(c);
+  }
+  CUDA_TRY(c, cudaGetLastError());
+  size_t tmp = 0;
+  CUDA_TRY(c, cub::DeviceSelect::Flagged(nullptr, tmp, c->gr_order.as<int>(),
+                                         c->gr_flag_ord.as<int>(), c->gr_list.as<int>(),
+                                         c->gr_nsel.as<int>(), (int)ntiles, c->stream));
+  TRY(ensure(c, c->ms_tmp, tmp));
+  CUDA_TRY(c, cub::DeviceSelect::Flagged(c->ms_tmp.p, tmp, c->gr_order.as<int>(),
+                                         c->gr_flag_ord.as<int>(), c->gr_list.as<int>(),
+                                         c->gr_nsel.as<int>(), (int)ntiles, c->stream));
+  c->launch_total += 2;
+  int nsel = 0;
+  unsigned long long counts[3] = {0, 0, 0};
+  CUDA_TRY(c, cudaMemcpyAsync(&nsel, c->gr_nsel.p, sizeof(int), cudaMemcpyDeviceToHost,
+                              c->stream));
+  CUDA_TRY(c, cudaMemcpyAsync(counts, c->gr_counts.p, sizeof(counts), cudaMemcpyDeviceToHost,
+                              c->stream));
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  TRY(grid_exact(c, r, g, c->gr_list.as<int>(), nsel, cfg->cull_rel, full, out, &st.pairs,
+                 &st.max_bound_ratio));
+  CUDA_TRY(c, cudaEventRecord(c->ev3, c->stream));
+  // Points in the flagged tiles (edge tiles may be partial).
+  std::vector<int> flags((size_t)ntiles);
+  CUDA_TRY(c, cudaMemcpyAsync(flags.data(), c->gr_flag.p, (size_t)ntiles * sizeof(int),
+                              cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  int64_t fb_points = 0;
+  for (int64_t t = 0; t < ntiles; ++t) {
+    if (!flags[(size_t)t]) continue;
+    const int64_t tx = t % g.ntx, ty = t / g.ntx;
+    fb_points += std::min<int64_t>(T, g.nx - tx * T) * std::min<int64_t>(T, g.ny - ty * T);
+  }
+  float ms = 0.f;
+  CUDA_TRY(c, cudaEventElapsedTime(&ms, c->ev0, c->ev3));
+  st.ms_total = ms;
+  CUDA_TRY(c, cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+  st.ms_predict = ms;
+  CUDA_TRY(c, cudaEventElapsedTime(&ms, c->ev1, c->ev2));
+  st.ms_probe = ms;
+  CUDA_TRY(c, cudaEventElapsedTime(&ms, c->ev2, c->ev3));
+  st.ms_fallback = ms;
+  st.tiles_low = (int64_t)counts[0];
+  st.tiles_flagged = (int64_t)counts[1];
+  st.tiles_surrogate = ntiles - st.tiles_flagged;
+  st.exact_points += fb_points;
+  unsigned eb = (unsigned)counts[2];
+  float pe = 0.f;
+  std::memcpy(&pe, &eb, sizeof(pe));
+  st.max_probe_err = mode == BBKDE_GRID_EXACT ? 0.0 : (double)pe;
+  c->last_ms = st.ms_total;
+  c->last_pairs = st.pairs;
+  c->last_launches = 0;
+  if (stats) *stats = st;
   return BBKDE_OK;
 }
 

@@ -57,10 +57,12 @@ __device__ __forceinline__ void mma16816(float (&d)[4], const uint32_t (&a)[4], 
       : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
-__device__ __forceinline__ float silu(float z) { return z / (1.0f + __expf(-z)); }
+// z sigmoid(z) with the fast reciprocal (__fdividef, 2 ulp): for z < -88 the
+// denominator is +inf and the result is -0.
+__device__ __forceinline__ float silu(float z) { return __fdividef(z, 1.0f + __expf(-z)); }
 // d silu / dz = s (1 + z (1 - s)), s = sigmoid(z)
 __device__ __forceinline__ float silu_grad(float z) {
-  float s = 1.0f / (1.0f + __expf(-z));
+  float s = __fdividef(1.0f, 1.0f + __expf(-z));
   return s * (1.0f + z * (1.0f - s));
 }
 
@@ -152,15 +154,61 @@ struct InferArgs {
   const float *params;          // FP32 master (W1, b's, w4, b4)
   const __nv_bfloat16 *w2, *w3; // BF16 [128][128]
   Norm norm;
-  const float2 *xy;             // query coordinates
+  const float2 *xy;             // query coordinates, or null for a grid:
+  int64_t gnx;                  //   point p at (gx0 + (p % gnx) gdx, gy0 + (p / gnx) gdy)
+  double gx0, gdx, gy0, gdy;
   int64_t n;
   float *out;                   // predicted log-density
 };
 
-constexpr int kInferWarps = 8;
+// Two-term BF16 activations: a = hi + lo with hi = bf16(a), lo = bf16(a - hi),
+// both multiplied by the same BF16 weights (relative activation error ~2^-17
+// instead of 2^-9, at twice the tensor-core work).
+__device__ __forceinline__ void to_a_split(const Frag &f, uint32_t (&hi)[8][4],
+                                           uint32_t (&lo)[8][4]) {
+#pragma unroll
+  for (int kk = 0; kk < 8; ++kk) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int j = 2 * kk + (q >> 1), e = 2 * (q & 1);
+      const __nv_bfloat162 h = __floats2bfloat162_rn(f.v[j][e], f.v[j][e + 1]);
+      const float2 hf = __bfloat1622float2(h);
+      hi[kk][q] = *reinterpret_cast<const uint32_t *>(&h);
+      lo[kk][q] = pack_bf16(f.v[j][e] - hf.x, f.v[j][e + 1] - hf.y);
+    }
+  }
+}
+
+__device__ __forceinline__ void layer_fwd_split(const uint32_t (&hi)[8][4],
+                                                const uint32_t (&lo)[8][4],
+                                                const __nv_bfloat16 *W, const float *bias,
+                                                Frag &out, int g, int t) {
+#pragma unroll
+  for (int j = 0; j < 16; ++j) {
+    const float b0 = bias[8 * j + 2 * t], b1 = bias[8 * j + 2 * t + 1];
+    out.v[j][0] = b0;
+    out.v[j][1] = b1;
+    out.v[j][2] = b0;
+    out.v[j][3] = b1;
+  }
+#pragma unroll
+  for (int kk = 0; kk < 8; ++kk) {
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      const __nv_bfloat16 *row = W + (8 * j + g) * kLd + 16 * kk + 2 * t;
+      const uint32_t b0 = *reinterpret_cast<const uint32_t *>(row);
+      const uint32_t b1 = *reinterpret_cast<const uint32_t *>(row + 8);
+      mma16816(out.v[j], lo[kk], b0, b1);
+      mma16816(out.v[j], hi[kk], b0, b1);
+    }
+  }
+}
+
+constexpr int kInferWarps = 4;
 constexpr size_t kInferSmem =
     2 * kH * kLd * sizeof(__nv_bfloat16) + (kH * 2 + 3 * kH + kH) * sizeof(float);
 
+template <bool kSplit>
 __global__ void __launch_bounds__(kInferWarps * 32) k_mlp_infer(InferArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   __nv_bfloat16 *W2 = reinterpret_cast<__nv_bfloat16 *>(smem);
@@ -187,19 +235,36 @@ __global__ void __launch_bounds__(kInferWarps * 32) k_mlp_infer(InferArgs a) {
   const int64_t nwarps = (int64_t)gridDim.x * kInferWarps;
   for (int64_t tile = warp0; tile < tiles; tile += nwarps) {
     const int64_t p0 = tile * 16 + g, p1 = p0 + 8;
-    const float2 q0 = p0 < a.n ? a.xy[p0] : make_float2(0.f, 0.f);
-    const float2 q1 = p1 < a.n ? a.xy[p1] : make_float2(0.f, 0.f);
+    float2 q0 = make_float2(0.f, 0.f), q1 = q0;
+    if (a.xy) {
+      if (p0 < a.n) q0 = a.xy[p0];
+      if (p1 < a.n) q1 = a.xy[p1];
+    } else {
+      q0 = make_float2((float)(a.gx0 + (double)(p0 % a.gnx) * a.gdx),
+                       (float)(a.gy0 + (double)(p0 / a.gnx) * a.gdy));
+      q1 = make_float2((float)(a.gx0 + (double)(p1 % a.gnx) * a.gdx),
+                       (float)(a.gy0 + (double)(p1 / a.gnx) * a.gdy));
+    }
     const float x0 = (q0.x - a.norm.cx) * a.norm.sx, y0 = (q0.y - a.norm.cy) * a.norm.sy;
     const float x1 = (q1.x - a.norm.cx) * a.norm.sx, y1 = (q1.y - a.norm.cy) * a.norm.sy;
     Frag f;
-    uint32_t A[8][4];
     layer1(W1, b1, x0, y0, x1, y1, f, t);
     silu_inplace(f);
-    to_a(f, A);
-    layer_fwd(A, W2, b2, f, g, t);
-    silu_inplace(f);
-    to_a(f, A);
-    layer_fwd(A, W3, b3, f, g, t);
+    if constexpr (kSplit) {
+      uint32_t Ah[8][4], Al[8][4];
+      to_a_split(f, Ah, Al);
+      layer_fwd_split(Ah, Al, W2, b2, f, g, t);
+      silu_inplace(f);
+      to_a_split(f, Ah, Al);
+      layer_fwd_split(Ah, Al, W3, b3, f, g, t);
+    } else {
+      uint32_t A[8][4];
+      to_a(f, A);
+      layer_fwd(A, W2, b2, f, g, t);
+      silu_inplace(f);
+      to_a(f, A);
+      layer_fwd(A, W3, b3, f, g, t);
+    }
     silu_inplace(f);
     float lo, hi;
     layer4(f, w4, b4, lo, hi, t);
@@ -451,7 +516,7 @@ __global__ void __launch_bounds__(kTrainWarps * 32) k_mlp_train(TrainArgs a) {
   }
   // ---- vectors on the CUDA cores: db1..3, dW1, dw4, db4 (fixed-order sums) ----
   for (int n = tid; n < kH; n += blockDim.x) {
-    float s1 = 0.f, s2 = 0.f, s3 = 0.f, w1x = 0.f, w1y = 0.f, sw4 = 0.f;
+    float s1 = 0.f, s2 = 0.f, s3 = 0.f, w1x = 0.f, w1y = 0.f;
     for (int p = 0; p < kTrainPts; ++p) {
       const float g1 = __bfloat162float(Z1[p * kLd + n]);
       s1 += g1;
@@ -465,7 +530,6 @@ __global__ void __launch_bounds__(kTrainWarps * 32) k_mlp_train(TrainArgs a) {
     gp[kOffB3 + n] = s3;
     gp[kOffW1 + 2 * n] = w1x;
     gp[kOffW1 + 2 * n + 1] = w1y;
-    (void)sw4;
   }
   // dw4[n] = sum_p dy_p * a3[p][n]; db4 = sum_p dy_p; loss = sum_p e_p^2 / batch.
   if (t == 0) {
@@ -485,9 +549,8 @@ __global__ void __launch_bounds__(kTrainWarps * 32) k_mlp_train(TrainArgs a) {
   }
   __syncthreads();
   if (tid == 0) {
-    float s = 0.f, sd = 0.f;
+    float s = 0.f;
     for (int p = 0; p < kTrainPts; ++p) s += red[p];
-    (void)sd;
     a.loss_part[blockIdx.x] = s * inv_b;
   }
   __syncthreads();

@@ -35,6 +35,7 @@ struct bbkde_surrogate {
   float *pred = nullptr;
   size_t pred_cap = 0;
   int64_t adam_step = 0;
+  int split = 0;   // inference with two-term BF16 activations
   std::string err;
 };
 
@@ -200,7 +201,9 @@ int bbkde_surrogate_create(int device, uint64_t seed, bbkde_surrogate **out) {
     }
     if (cudaFuncSetAttribute(k_mlp_train, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)kTrainSmem) != cudaSuccess ||
-        cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(k_mlp_infer<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)kInferSmem) != cudaSuccess ||
+        cudaFuncSetAttribute(k_mlp_infer<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)kInferSmem) != cudaSuccess) {
       rc = BBKDE_CUDA_ERROR;
       break;
@@ -390,19 +393,26 @@ int bbkde_surrogate_train(bbkde_surrogate *s, int64_t n, const double *xy, const
   return BBKDE_OK;
 }
 
-// Predicted log-density at device points (float2) into device floats, on the
-// surrogate's stream (asynchronous).
-int bbkde_surrogate_predict_device(bbkde_surrogate *s, int64_t n, const void *xy_f2,
-                                   float *out) {
-  if (!s || n < 0 || (n > 0 && (!xy_f2 || !out))) return BBKDE_INVALID_ARGUMENT;
+}  // extern "C"
+
+namespace bbkde {
+
+// Inference launch on `st`: points from xy (float2) or, with xy null, from the
+// grid (gnx; gx0, gdx, gy0, gdy). Used by the dense-grid pipeline.
+int surrogate_infer(bbkde_surrogate *s, cudaStream_t st, int64_t n, const float2 *xy,
+                    int64_t gnx, double gx0, double gdx, double gy0, double gdy, float *out) {
   if (n == 0) return BBKDE_OK;
-  S_CUDA(s, cudaSetDevice(s->device));
   InferArgs a;
   a.params = s->params;
   a.w2 = s->w2;
   a.w3 = s->w3;
   a.norm = s->norm;
-  a.xy = static_cast<const float2 *>(xy_f2);
+  a.xy = xy;
+  a.gnx = gnx > 0 ? gnx : 1;
+  a.gx0 = gx0;
+  a.gdx = gdx;
+  a.gy0 = gy0;
+  a.gdy = gdy;
   a.n = n;
   a.out = out;
   int sms = 148;
@@ -410,19 +420,43 @@ int bbkde_surrogate_predict_device(bbkde_surrogate *s, int64_t n, const void *xy
   const int64_t tiles = (n + 15) / 16;
   const int64_t want = (tiles + kInferWarps - 1) / kInferWarps;
   const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)sms * 8));
-  k_mlp_infer<<<grid, kInferWarps * 32, kInferSmem, s->stream>>>(a);
+  if (s->split)
+    k_mlp_infer<true><<<grid, kInferWarps * 32, kInferSmem, st>>>(a);
+  else
+    k_mlp_infer<false><<<grid, kInferWarps * 32, kInferSmem, st>>>(a);
   S_CUDA(s, cudaGetLastError());
   return BBKDE_OK;
+}
+
+int surrogate_device(const bbkde_surrogate *s) { return s->device; }
+
+}  // namespace bbkde
+
+extern "C" {
+
+int bbkde_surrogate_set_inference(bbkde_surrogate *s, int split_activations) {
+  if (!s || (split_activations != 0 && split_activations != 1)) return BBKDE_INVALID_ARGUMENT;
+  s->split = split_activations;
+  return BBKDE_OK;
+}
+
+// Predicted log-density at device points (float2) into device floats, on the
+// surrogate's stream (asynchronous).
+int bbkde_surrogate_predict_device(bbkde_surrogate *s, int64_t n, const void *xy_f2,
+                                   float *out) {
+  if (!s || n < 0 || (n > 0 && (!xy_f2 || !out))) return BBKDE_INVALID_ARGUMENT;
+  if (n == 0) return BBKDE_OK;
+  S_CUDA(s, cudaSetDevice(s->device));
+  return bbkde::surrogate_infer(s, s->stream, n, static_cast<const float2 *>(xy_f2), 0, 0.0,
+                                0.0, 0.0, 0.0, out);
 }
 
 int bbkde_surrogate_predict(bbkde_surrogate *s, int64_t n, const double *xy, double *out) {
   if (!s || n < 0 || (n > 0 && (!xy || !out))) return BBKDE_INVALID_ARGUMENT;
   if (n == 0) return BBKDE_OK;
   S_CUDA(s, cudaSetDevice(s->device));
-  size_t cap = s->data_cap;
   float2 *dxy = nullptr;
   S_CUDA(s, cudaMalloc(&dxy, n * sizeof(float2)));
-  (void)cap;
   std::vector<float2> hxy(n);
   for (int64_t i = 0; i < n; ++i) hxy[i] = make_float2((float)xy[2 * i], (float)xy[2 * i + 1]);
   int rc = BBKDE_OK;

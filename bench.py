@@ -60,6 +60,15 @@ def parse():
                     help="target CPU time of the bounded CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--workload", choices=["direct", "surrogate-grid"], default="direct",
+                    help="direct: adaptive pilot + evaluation, 1M x 1M (the default); "
+                         "surrogate-grid: 4M references on an 8192 x 8192 grid")
+    ap.add_argument("--grid", type=int, default=8192, help="surrogate-grid: points per axis")
+    ap.add_argument("--n-grid-ref", type=int, default=4_000_000,
+                    help="surrogate-grid: reference points")
+    ap.add_argument("--train-steps", type=int, default=30000)
+    ap.add_argument("--no-plain", action="store_true",
+                    help="surrogate-grid: skip the plain direct comparator (~1 min)")
     return ap.parse_args()
 
 
@@ -220,6 +229,8 @@ def main():
     world, rank, local = dist_env()
     if a.impl == "reference":
         return run_reference_arm(a, world, rank)
+    if a.workload == "surrogate-grid":
+        return run_surrogate_grid(a, world, rank, local)
 
     import torch
     import bbrcit_kde_b200 as bk
@@ -390,6 +401,245 @@ def main():
         "gpu_launches": int(launches),
         "error_vs_fp64": {**err, "definition": err_def,
                           "fp64_vs_cpu_oracle_pass_rate": oracle_check},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# Surrogate-grid workload: the learned log-density surrogate on a dense grid.
+# ---------------------------------------------------------------------------
+GRID_METRIC_UNIT = "queries/s"
+
+
+def _grid_errors(torch, x, ref):
+    """Relative error of x against ref over every grid point."""
+    e = ((x - ref).abs() / ref.clamp_min(1e-300)).float()
+    n = e.numel()
+    samp = e[torch.randint(0, n, (1 << 22,), device=e.device,
+                           generator=torch.Generator(device=e.device).manual_seed(5))]
+    q = torch.quantile(samp, torch.tensor([0.5, 0.999], device=e.device))
+    return {"max": float(e.max()), "median": float(q[0]), "p999": float(q[1]),
+            "frac_gt_1e-3": float((e > 1e-3).float().mean())}
+
+
+def run_surrogate_grid(a, world, rank, local):
+    """4,000,000 references from the seeded 8-component mixture, adaptive Gaussian
+    KDE (pilot h = 0.05, alpha = 0.5), density on an 8192 x 8192 grid over
+    [-4, 4]^2. One step = bbkde_eval_grid in anchored mode with the trained network
+    (two-term BF16 inference): network value + bilinear residual measured exactly
+    at the tile corners, 5 exact held-out probes per 16 x 16 tile (tolerance
+    5e-4), exact culled fallback on flagged tiles and tiles below 1e-4 of the
+    maximum. Comparators (timed once each): the plain direct sum over all grid
+    points, the culled exact sum, the same pipeline without the network, and the
+    network alone with probes (no anchors)."""
+    import torch
+    import bbrcit_kde_b200 as bk
+    from bbrcit_kde_b200 import workloads as W
+
+    torch.cuda.set_device(local)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    ctx = bk.Context(local)
+    ctx.set_stream(stream.cuda_stream)
+    sm_count, _ = ctx.device_info()
+    info = {}
+
+    refs = W.config5_refs(a.n_grid_ref)
+    if rank > 0:   # replicas: each rank its own seeded draw of the same mixture
+        rng = W.SplitMix64(W.SEED_BASE + 500 + rank)
+        refs = refs[np.argsort(rng.uniform(len(refs)))]
+    n = len(refs)
+    w = np.full(n, 1.0 / n)
+    desc = bk.kernel_desc(W.GAUSS, 2, (0.05, 0.05))
+    ctx.upload(bk.REFERENCE, refs, mass=w, weight=w)
+    t0 = time.perf_counter()
+    abw, mass, _, _ = ctx.adapt_density(desc, 0.5, bk.FP32C)
+    info["pilot_ms"] = ctx.last_launch_stats()[0]
+
+    # Training set: exact log-densities at uniform and data-sampled points.
+    rng = W.SplitMix64(0xB2000555)
+    n_tr = 2_000_000
+    uni = rng.uniform(n_tr, -4.0, 4.0).reshape(-1, 2)
+    pick = np.minimum((rng.uniform(n_tr // 2) * n).astype(np.int64), n - 1)
+    dat = refs[pick] + 0.05 * rng.normal(n_tr).reshape(-1, 2)
+    xy = W.f32(np.concatenate([uni, dat]))
+    ctx.upload(bk.QUERY, xy)
+    f = ctx.eval_all(desc)
+    info["train_targets_ms"] = ctx.last_launch_stats()[0]
+    ok = f > 0
+    sur = bk.Surrogate(local, seed=1)
+    t1 = time.perf_counter()
+    loss = sur.train(xy[ok], np.log(f[ok]), steps=a.train_steps, batch=8192, lr=3e-3,
+                     lr_final=1e-5)
+    torch.cuda.synchronize()
+    info.update(train_s=time.perf_counter() - t1, train_steps=a.train_steps, final_loss=loss,
+                train_points=int(ok.sum()))
+    sur.set_inference(True)
+
+    G = a.grid
+    grid = (G, G, -4.0, 4.0, -4.0, 4.0)
+    npts = G * G
+    out = torch.empty(npts, dtype=torch.float64, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    main_cfg = dict(surrogate=sur, mode=bk.GRID_ANCHORED, tile=16, probes=5, rel_tol=5e-4,
+                    low_frac=1e-4)
+
+    def grid_step(dst, **kw):
+        return ctx.eval_grid(desc, grid, dst.data_ptr(), **kw)
+
+    for _ in range(a.warmup):
+        grid_step(out, **main_cfg)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    launches0 = ctx.launch_count()
+    step_ms, stats = [], []
+    for _ in range(a.steps):
+        l2_flush(torch, flush)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        st = grid_step(out, **main_cfg)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        step_ms.append(e0.elapsed_time(e1))
+        stats.append(st.as_dict())
+    launches = ctx.launch_count() - launches0
+    clocks = sampler.stop()
+    total_ms = sum(step_ms)
+    value = npts * a.steps / (total_ms / 1e3)
+    main_out = out.clone()
+
+    # Comparators, each once.
+    comp = {}
+    for name, kw in [("culled_exact", dict(mode=bk.GRID_EXACT, tile=16)),
+                     ("anchored_without_network", dict(surrogate=None, mode=bk.GRID_ANCHORED,
+                                                       tile=16, probes=5, rel_tol=5e-4,
+                                                       low_frac=1e-4)),
+                     ("network_tile32", dict(main_cfg, tile=32)),
+                     ("anchored_without_network_tile32",
+                      dict(surrogate=None, mode=bk.GRID_ANCHORED, tile=32, probes=5,
+                           rel_tol=5e-4, low_frac=1e-4)),
+                     ("network_only_probes", dict(surrogate=sur, mode=bk.GRID_SURROGATE,
+                                                  tile=16, probes=5, rel_tol=5e-4,
+                                                  low_frac=1e-4))]:
+        l2_flush(torch, flush)
+        torch.cuda.synchronize()
+        dst = torch.empty(npts, dtype=torch.float64, device="cuda")
+        st = grid_step(dst, **kw)
+        comp[name] = (st.as_dict(), dst)
+
+    plain = None
+    if not a.no_plain:
+        ctx.upload(bk.QUERY, W.grid_2d(-4.0, 4.0, G, -4.0, 4.0, G))
+        plain = torch.empty(npts, dtype=torch.float64, device="cuda")
+        l2_flush(torch, flush)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ctx.eval_range_device(desc, 0, n - 1, 0, npts - 1, plain.data_ptr())
+        e1.record(stream)
+        torch.cuda.synchronize()
+        info["plain_direct_ms"] = e0.elapsed_time(e1)
+    ref = plain if plain is not None else comp["culled_exact"][1]
+    ref_name = "plain direct FP32C" if plain is not None else "culled exact FP32C"
+    errors = {"pipeline": _grid_errors(torch, main_out, ref)}
+    results = {}
+    for name, (st, dst) in comp.items():
+        errors[name] = _grid_errors(torch, dst, ref)
+        results[name] = st
+    # FP64 at 4096 grid points.
+    idx = np.sort(np.random.default_rng(3).choice(npts, 4096, replace=False))
+    pts = np.stack([-4.0 + (idx % G) * (8.0 / G), -4.0 + (idx // G) * (8.0 / G)], 1)
+    ctx.upload(bk.QUERY, W.f32(pts))
+    f64 = ctx.eval_all(desc, precision=bk.FP64)
+    tidx = torch.from_numpy(idx).cuda()
+    fp64 = {}
+    for name, arr in [("pipeline", main_out), ("reference_grid", ref),
+                      ("culled_exact", comp["culled_exact"][1])]:
+        v = arr[tidx].cpu().numpy()
+        e = np.abs(v - f64) / f64
+        fp64[name] = {"max": float(e.max()), "median": float(np.median(e))}
+    del comp
+
+    # End to end through the C ABI: the adapted reference set from pinned host
+    # memory in, the density grid to pinned host memory out.
+    e2e = None
+    if not a.no_e2e:
+        pin = lambda arr: torch.from_numpy(np.ascontiguousarray(arr)).pin_memory()  # noqa
+        h_refs, h_mass, h_abw, h_w = pin(refs), pin(mass), pin(abw), pin(w)
+        h_out = torch.empty(npts, dtype=torch.float64).pin_memory()
+
+        def e2e_step():
+            ctx.upload(bk.REFERENCE, h_refs.numpy(), mass=h_mass.numpy(), abw=h_abw.numpy(),
+                       weight=h_w.numpy())
+            grid_step(out, **main_cfg)
+            h_out.copy_(out, non_blocking=True)
+
+        for _ in range(a.warmup):
+            e2e_step()
+        torch.cuda.synchronize()
+        e2e_ms = []
+        for _ in range(a.steps):
+            l2_flush(torch, flush)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            e2e_step()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            e2e_ms.append(e0.elapsed_time(e1))
+        h2d = h_refs.numel() * 8 + 3 * n * 8
+        e2e = {"value": npts * a.steps / (sum(e2e_ms) / 1e3), "unit": GRID_METRIC_UNIT,
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(npts * 8)}
+
+    # Roofline of the culled pair sum (the exact fallback): pairs at tile
+    # granularity of the culled-exact comparator over its device time.
+    ce = results["culled_exact"]
+    peaks = measured_peaks()
+    sm_max = float(peaks.get("sm_max_mhz") or clocks.get("sm_max_mhz") or 1965.0)
+    peak = sm_count * MUFU_EX2_PER_CLK_PER_SM * sm_max * 1e6
+    ach = ce["pairs"] / (ce["ms_total"] / 1e3)
+    roofline = {"bound": "sfu", "kernel": "k_pair_sum_culled (culled exact grid)",
+                "achieved": ach / 1e9, "peak": peak / 1e9, "unit": "Geval/s",
+                "frac": ach / peak, "traffic": None,
+                "peak_basis": f"{sm_count} SMs x 16 MUFU ex2/clk x {sm_max:.0f} MHz"}
+    cpu = None
+    if rank == 0 and not a.no_cpu_baseline:
+        wl = W.Workload("cfg5", W.GAUSS, 2, (0.05, 0.05), refs, w,
+                        W.f32(pts[:2048]))
+        r = cpu_reference_rate(wl, a.cpu_seconds)
+        cpu = {"value": r["value"] / n, "unit": GRID_METRIC_UNIT, "cores": r["cores"],
+               "kind": r["kind"],
+               "sample": r["sample"] + "; queries/s = pair rate / 4M references "
+                                       "(Gaussian kernel, fixed bandwidth: same per-pair "
+                                       "cost as the adaptive sum)"}
+    ctx.close()
+    sur.close()
+    if rank != 0:
+        return 0
+    speedup = {}
+    if plain is not None:
+        pm = info["plain_direct_ms"]
+        speedup = {"pipeline_vs_plain_direct": pm / (total_ms / a.steps)}
+        for name, st in results.items():
+            speedup[f"{name}_vs_plain_direct"] = pm / st["ms_total"]
+    line = {
+        "metric": METRIC, "value": value, "unit": GRID_METRIC_UNIT, "n_gpus": world,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": total_ms / a.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+bf16",
+        "data": "synthetic (seeded splitmix64 8-component mixture, float32-representable)",
+        "config": {"workload": f"surrogate grid: adaptive Gaussian KDE of {n} refs (pilot "
+                               f"h=0.05, alpha=0.5) on a {G}x{G} grid over [-4,4]^2",
+                   "pipeline": "bbkde_eval_grid anchored mode, tile 16, 5 probes, probe "
+                               "tolerance 5e-4, low_frac 1e-4, two-term BF16 inference",
+                   "l2": "flushed between timed steps (256 MB write)"},
+        "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
+        "gpu_launches": int(launches), "step_stats": stats[-1], "comparators": results,
+        "speedup": speedup, "errors_vs": ref_name, "errors": errors, "errors_vs_fp64_4096": fp64,
+        "setup": info,
     }
     print(json.dumps(line), flush=True)
     return 0

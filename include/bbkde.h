@@ -212,7 +212,7 @@ BBKDE_API int bbkde_cv_batch(bbkde_ctx *ctx, int kind, int n_sets, const bbkde_d
  * tensor-core inference kernel. No reference counterpart: the reference evaluates
  * every query with a density sum (KernelDensityImpl.h:1157-1231); the surrogate
  * stands in for that sum on dense query grids, with the exact sum as its fallback
- * and judge (bbkde_surrogate_eval_grid). */
+ * and judge (bbkde_eval_grid). */
 typedef struct bbkde_surrogate bbkde_surrogate;
 
 typedef struct {
@@ -256,10 +256,89 @@ BBKDE_API int bbkde_surrogate_predict(bbkde_surrogate *s, int64_t n, const doubl
 BBKDE_API int bbkde_surrogate_predict_device(bbkde_surrogate *s, int64_t n, const void *xy_f2,
                                              float *out);
 
+/* Inference precision: 0 (default) = BF16 activations, as in training;
+ * 1 = two-term BF16 activations (a = hi + lo, both BF16, same BF16 weights, FP32
+ * accumulate): relative activation rounding ~2^-17 instead of ~2^-9 at twice the
+ * tensor-core work. */
+BBKDE_API int bbkde_surrogate_set_inference(bbkde_surrogate *s, int split_activations);
+
 /* Checkpoint: magic "BBKDEMLP", version, parameter count, normalisation, FP32
  * parameters (little-endian). */
 BBKDE_API int bbkde_surrogate_save(bbkde_surrogate *s, const char *path);
 BBKDE_API int bbkde_surrogate_load(bbkde_surrogate *s, const char *path);
+
+/* ---- culled direct evaluation and dense grids ------------------------------ */
+
+/* Culled direct evaluation: the QUERY set against every REFERENCE point, summing
+ * only the reference tiles (256 Morton-ordered points) that can contribute. For
+ * the Gaussian kernels the part left out is bounded, per block of queries, by
+ * rel_tol times the smallest sum in that block, so every result is within
+ * rel_tol (plus the FP32-compensated arithmetic error) of the full sum; for the
+ * Epanechnikov kernels only tiles entirely outside the support are skipped
+ * (exact). Kernels: Gaussian (1-D, 2-D), Epanechnikov (1-D, 2-D), the 2-D
+ * product kernels and the Gaussian convolution kernels; the Epanechnikov
+ * convolution kernels are BBKDE_UNSUPPORTED. No reference counterpart in this
+ * form: it plays the part of the reference's tree-pruned evaluation
+ * (KernelDensityImpl.h:548-640) with a deterministic error bound. out holds
+ * bbkde_size(QUERY) doubles, on the host unless out_on_device. */
+typedef struct {
+  double kernel_ms;        /* device time of the culled sum (CUDA events) */
+  double pairs;            /* reference-query pairs evaluated (tile granularity) */
+  double full_pairs;       /* pairs of the full sum */
+  double max_bound_ratio;  /* max over blocks of skipped bound / smallest block sum */
+} bbkde_cull_stats;
+
+BBKDE_API int bbkde_eval_culled(bbkde_ctx *ctx, const bbkde_kernel_desc *kernel, int normalized,
+                                double rel_tol, double *out, int out_on_device,
+                                bbkde_cull_stats *stats);
+
+/* A regular 2-D grid: point (i, j), 0 <= i < nx, 0 <= j < ny, at
+ * (x0 + i (x1 - x0) / nx, y0 + j (y1 - y0) / ny) (end points excluded, the
+ * reference's test grid, test/kde_test_utils.h:97-123); results row-major,
+ * index j * nx + i. */
+typedef struct {
+  int64_t nx, ny;
+  double x0, x1, y0, y1;
+} bbkde_grid;
+
+enum {
+  BBKDE_GRID_EXACT = 0,      /* the exact sum at every point */
+  BBKDE_GRID_SURROGATE = 1,  /* network value, held-out probes, exact fallback */
+  BBKDE_GRID_ANCHORED = 2    /* network + residual measured exactly at tile corners */
+};
+
+typedef struct {
+  int mode;          /* BBKDE_GRID_* */
+  int tile;          /* decision tile edge in grid points: 16 or 32 */
+  int probes;        /* held-out probes per tile: 1 (centre), 5 (+ edge midpoints)
+                        or 9 (+ quarter points) */
+  int exact_culled;  /* 1: exact parts use the culled sum; 0: the full direct sum */
+  double rel_tol;    /* a tile keeps the prediction only if every probe is within */
+  double low_frac;   /* tiles whose smallest predicted density is below low_frac
+                        times the grid's largest go exact */
+  double cull_rel;   /* bound of the culled sum (e.g. 1e-7) */
+} bbkde_grid_config;
+
+typedef struct {
+  int64_t tiles, tiles_low, tiles_flagged, tiles_surrogate;
+  int64_t exact_points;       /* points evaluated by an exact sum (anchors, probes, fallback) */
+  double pairs;               /* reference-query pairs of those sums (tile granularity) */
+  double max_probe_err;       /* largest held-out error among tiles that are not low */
+  double max_bound_ratio;     /* largest culled-sum bound ratio */
+  double ms_total, ms_predict, ms_probe, ms_fallback;   /* device time (CUDA events) */
+} bbkde_grid_stats;
+
+/* Normalised density of the REFERENCE set (with its current attributes, e.g.
+ * after bbkde_adapt_density) on a dense 2-D grid. In the surrogate modes the
+ * network `sur` predicts log-density (natural log of the normalised density,
+ * the quantity it was trained on); sur may be NULL in BBKDE_GRID_ANCHORED mode
+ * (a zero network: bilinear interpolation of the exact log-density between tile
+ * corners) and is ignored in BBKDE_GRID_EXACT mode. out_device holds nx * ny
+ * doubles in device memory. No reference counterpart. */
+BBKDE_API int bbkde_eval_grid(bbkde_ctx *ctx, bbkde_surrogate *sur,
+                              const bbkde_kernel_desc *kernel, const bbkde_grid *grid,
+                              const bbkde_grid_config *cfg, double *out_device,
+                              bbkde_grid_stats *stats);
 
 /* ---- introspection ------------------------------------------------------- */
 

@@ -1,0 +1,268 @@
+"""Culled direct sum and the dense-grid pipeline, through the C ABI.
+
+Tolerances:
+  culled sum with bound r -- against the FP64 oracle every entry passes
+      approximately_equal(rel r + 1e-6, abs 1e-8): the skipped part is at most r
+      of the sum, plus the FP32-compensated arithmetic error of the full sum
+      (the direct path's 1e-6 bar); the reported bound ratio is at most r.
+  Epanechnikov kernels -- only tiles outside the support are skipped: the
+      direct path's bar (rel 1e-6, abs 1e-8).
+  grid, exact mode -- the same bars against the direct path on the grid points.
+  grid, surrogate modes -- exact tiles at the direct path's bar; every held-out
+      probe of a kept tile within rel_tol (by construction); the share of grid
+      points off by more than rel_tol is reported and bounded.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import bbrcit_kde_b200 as bk
+from bbrcit_kde_b200 import workloads as W
+from tests.helpers import assert_parity
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+def _clustered(seed, n, dim):
+    """Tight clusters spread over a wide box: most tiles are far from most queries."""
+    rng = W.SplitMix64(seed)
+    k = 12
+    centres = rng.uniform(k * dim, -4.0, 4.0).reshape(k, dim)
+    sig = rng.uniform(k, 0.05, 0.3)
+    comp = np.minimum((rng.uniform(n) * k).astype(np.int64), k - 1)
+    pts = centres[comp] + sig[comp, None] * rng.normal(n * dim).reshape(n, dim)
+    return W.f32(pts)
+
+
+def _problem(seed, n, m, dim, adaptive):
+    rng = W.SplitMix64(seed + 1000)
+    refs = _clustered(seed, n, dim)
+    q = W.f32(rng.uniform(m * dim, -5.0, 5.0).reshape(m, dim))
+    mass = rng.uniform(n, 0.5, 2.0)
+    mass /= mass.sum()
+    abw = rng.uniform(n, 0.4, 2.5) if adaptive else None
+    return refs, q, mass, abw
+
+
+CULL_KINDS = [(W.GAUSS, 2, (0.05, 0.05)), (W.GAUSS_PROD2D, 2, (0.04, 0.09)),
+              (W.EPAN, 2, (0.1, 0.1)), (W.EPAN_PROD2D, 2, (0.12, 0.07)),
+              (W.GAUSS_PROD_CONV2D, 2, (0.04, 0.09)), (W.GAUSS, 1, (0.01, 0.01)),
+              (W.EPAN, 1, (0.03, 0.03)), (W.GAUSS_CONV1D, 1, (0.01, 0.01))]
+GAUSSIANS = (W.GAUSS, W.GAUSS_PROD2D, W.GAUSS_PROD_CONV2D, W.GAUSS_CONV1D)
+
+
+@pytest.mark.parametrize("kind,dim,h", CULL_KINDS)
+def test_culled_matches_oracle(ctx, oracle, kind, dim, h):
+    refs, q, mass, abw = _problem(40 + kind * 5 + dim, 20_011, 3_001, dim, True)
+    ctx.upload(bk.REFERENCE, refs, mass=mass, abw=abw)
+    ctx.upload(bk.QUERY, q)
+    desc = bk.kernel_desc(kind, dim, h)
+    want = oracle.direct(kind, dim, h, refs, mass, q, abw=abw)
+    rel = 1e-7
+    got, st = ctx.eval_culled(desc, rel_tol=rel)
+    assert_parity(got, want, 1e-6 + rel, 1e-8, what=f"culled kind {kind} dim {dim}")
+    assert st.max_bound_ratio <= rel
+    assert st.full_pairs == pytest.approx(20_011 * 3_001)
+
+
+@pytest.mark.parametrize("kind,dim,h", CULL_KINDS)
+@pytest.mark.parametrize("adaptive", [False, True])
+def test_culled_skips_far_tiles(ctx, kind, dim, h, adaptive):
+    """Many queries (compact query blocks): most reference tiles are skipped, and
+    the result still matches the FP64 direct path (pinned to the oracle by
+    test_direct_gpu)."""
+    refs, q, mass, abw = _problem(60 + kind * 5 + dim, 50_000, 100_000, dim, adaptive)
+    ctx.upload(bk.REFERENCE, refs, mass=mass, abw=abw)
+    ctx.upload(bk.QUERY, q)
+    desc = bk.kernel_desc(kind, dim, h)
+    want = ctx.eval_all(desc, precision=bk.FP64)
+    rel = 1e-7
+    got, st = ctx.eval_culled(desc, rel_tol=rel)
+    assert_parity(got, want, 1e-6 + rel, 1e-8, what=f"culled kind {kind} dim {dim}")
+    assert st.max_bound_ratio <= rel
+    assert st.pairs < 0.5 * st.full_pairs, (st.pairs, st.full_pairs)
+
+
+@pytest.mark.parametrize("rel", [1e-3, 1e-5])
+def test_culled_bound_holds_at_loose_tolerances(ctx, rel):
+    refs, q, mass, abw = _problem(77, 50_000, 100_000, 2, True)
+    ctx.upload(bk.REFERENCE, refs, mass=mass, abw=abw)
+    ctx.upload(bk.QUERY, q)
+    desc = bk.kernel_desc(W.GAUSS, 2, (0.05, 0.05))
+    want = ctx.eval_all(desc, precision=bk.FP64)
+    got, st = ctx.eval_culled(desc, rel_tol=rel)
+    tight, st_tight = ctx.eval_culled(desc, rel_tol=1e-7)
+    assert_parity(got, want, rel + 1e-6, 1e-8, what=f"rel {rel}")
+    assert st.max_bound_ratio <= rel
+    assert st.pairs <= st_tight.pairs
+
+
+def test_culled_deterministic_and_edge_sizes(ctx, oracle):
+    desc = bk.kernel_desc(W.GAUSS, 2, (0.1, 0.1))
+    refs, q, mass, _ = _problem(5, 5_000, 2_500, 2, False)
+    ctx.upload(bk.REFERENCE, refs, mass=mass)
+    ctx.upload(bk.QUERY, q)
+    a, _ = ctx.eval_culled(desc)
+    b, _ = ctx.eval_culled(desc)
+    np.testing.assert_array_equal(a, b)
+    # ragged sizes: one reference, 257 references, one query, empty queries
+    for n, m in [(1, 3), (257, 1), (1023, 1025)]:
+        refs, q, mass, _ = _problem(9 + n, n, m, 2, False)
+        ctx.upload(bk.REFERENCE, refs, mass=mass)
+        ctx.upload(bk.QUERY, q)
+        want = oracle.direct(W.GAUSS, 2, (0.1, 0.1), refs, mass, q)
+        got, _ = ctx.eval_culled(desc)
+        assert_parity(got, want, 1e-6 + 1e-7, 1e-8, what=f"n {n} m {m}")
+    ctx.upload(bk.QUERY, np.zeros((0, 2)))
+    got, st = ctx.eval_culled(desc)
+    assert got.shape == (0,) and st.pairs == 0
+
+
+def test_culled_rejects_epanechnikov_convolution(ctx):
+    refs, q, mass, _ = _problem(3, 1000, 100, 2, False)
+    ctx.upload(bk.REFERENCE, refs, mass=mass)
+    ctx.upload(bk.QUERY, q)
+    with pytest.raises(bk.BBKDEError) as e:
+        ctx.eval_culled(bk.kernel_desc(W.EPAN_PROD_CONV2D, 2, (0.1, 0.1)))
+    assert e.value.status == bk.UNSUPPORTED
+    with pytest.raises(bk.InvalidArgument):
+        ctx.eval_culled(bk.kernel_desc(W.GAUSS, 2, (0.1, 0.1)), rel_tol=0.0)
+
+
+# ---- dense grids ------------------------------------------------------------
+
+GRID = (250, 190, -3.0, 3.0, -2.5, 2.5)     # partial edge tiles on both axes
+
+
+def _grid_points(grid):
+    nx, ny, x0, x1, y0, y1 = grid
+    return W.grid_2d(x0, x1, nx, y0, y1, ny)
+
+
+def _setup_adaptive(ctx, n=60_000, seed=5):
+    refs = W.config5_refs(n)
+    ctx.upload(bk.REFERENCE, refs, mass=np.full(n, 1.0 / n), weight=np.full(n, 1.0 / n))
+    desc = bk.kernel_desc(W.GAUSS, 2, (0.08, 0.08))
+    ctx.adapt_density(desc, 0.5, outputs=False)
+    return desc
+
+
+def _grid_eval(ctx, desc, grid, **kw):
+    out = torch.empty(grid[0] * grid[1], dtype=torch.float64, device="cuda")
+    st = ctx.eval_grid(desc, grid, out.data_ptr(), **kw)
+    torch.cuda.synchronize()
+    return out.cpu().numpy(), st
+
+
+def _direct_on_grid(ctx, desc, grid):
+    ctx.upload(bk.QUERY, _grid_points(grid))
+    return ctx.eval_all(desc)
+
+
+def test_grid_exact_matches_direct(ctx):
+    desc = _setup_adaptive(ctx)
+    want = _direct_on_grid(ctx, desc, GRID)
+    for culled in (True, False):
+        got, st = _grid_eval(ctx, desc, GRID, mode=bk.GRID_EXACT, tile=16, exact_culled=culled)
+        assert_parity(got, want, 1e-6 + 1e-7, 1e-8, what=f"grid exact culled={culled}")
+        assert st.tiles == 16 * 12 and st.tiles_flagged == st.tiles
+        assert st.exact_points == GRID[0] * GRID[1]
+    got32, _ = _grid_eval(ctx, desc, GRID, mode=bk.GRID_EXACT, tile=32)
+    assert_parity(got32, want, 1e-6 + 1e-7, 1e-8, what="grid exact tile 32")
+
+
+def _tile_ids(grid, tile):
+    nx, ny = grid[0], grid[1]
+    i = np.arange(nx)[None, :] // tile
+    j = np.arange(ny)[:, None] // tile
+    return (j * ((nx + tile - 1) // tile) + i).ravel()
+
+
+# Dense grid at the point spacing of the 4M-point, 8192 x 8192 surrogate
+# workload (1/1024): 1M references (pilot h = 0.063, the 4M workload's 0.05
+# scaled by (4M / 1M)^(1/6)), a 2 x 2 window around one mixture component.
+FINE = (2048, 2048, -3.5, -1.5, 0.5, 2.5)
+
+
+def _setup_fine(ctx):
+    n = 1_000_000
+    refs = W.config5_refs(n)
+    ctx.upload(bk.REFERENCE, refs, mass=np.full(n, 1.0 / n), weight=np.full(n, 1.0 / n))
+    desc = bk.kernel_desc(W.GAUSS, 2, (0.063, 0.063))
+    ctx.adapt_density(desc, 0.5, outputs=False)
+    return desc, refs
+
+
+def _train(ctx, desc, refs, seed=1, steps=8000):
+    """A network trained on exact log-densities at uniform and data-sampled points."""
+    rng = W.SplitMix64(101)
+    n_u, n_d = 150_000, 150_000
+    uni = rng.uniform(2 * n_u, -4.0, 4.0).reshape(-1, 2)
+    pick = np.minimum((rng.uniform(n_d) * len(refs)).astype(np.int64), len(refs) - 1)
+    dat = refs[pick] + 0.063 * rng.normal(2 * n_d).reshape(-1, 2)
+    xy = W.f32(np.concatenate([uni, dat]))
+    ctx.upload(bk.QUERY, xy)
+    f = ctx.eval_all(desc)
+    ok = f > 0
+    s = bk.Surrogate(0, seed=seed)
+    s.train(xy[ok], np.log(f[ok]), steps=steps, batch=8192, lr=3e-3, lr_final=1e-5)
+    s.set_inference(True)
+    return s
+
+
+def _check_tiles(st, got, want, grid, tile, probe_tol):
+    """Exact tiles match the direct sum; statistics add up. (max_probe_err covers
+    every tile above the low-density cut, flagged ones included, so it may exceed
+    probe_tol.)"""
+    assert st.tiles_surrogate + st.tiles_flagged == st.tiles
+    assert st.max_probe_err > 0
+    err = np.abs(got - want) / np.maximum(want, 1e-300)
+    per_tile = np.zeros(st.tiles)
+    np.maximum.at(per_tile, _tile_ids(grid, tile), err)
+    # every flagged tile went exact (FP32-compensated bar); kept tiles may differ
+    assert np.sum(per_tile <= 1e-6 + 1e-7) >= st.tiles_flagged
+    return err
+
+
+def test_grid_anchored_without_network(ctx):
+    desc, _ = _setup_fine(ctx)
+    want = _direct_on_grid(ctx, desc, FINE)
+    got, st = _grid_eval(ctx, desc, FINE, mode=bk.GRID_ANCHORED, tile=16, probes=5,
+                         rel_tol=5e-4, low_frac=1e-4)
+    err = _check_tiles(st, got, want, FINE, 16, 5e-4)
+    assert st.tiles_surrogate > st.tiles // 2, st.as_dict()
+    assert st.exact_points < 0.5 * FINE[0] * FINE[1]
+    # probes at the centre and edge midpoints hold the whole grid near rel_tol
+    assert err.max() <= 1e-3, (err.max(), np.mean(err > 5e-4))
+    # the low-density rule: tiles below half the maximum go exact
+    got, st = _grid_eval(ctx, desc, FINE, mode=bk.GRID_ANCHORED, tile=16, probes=1,
+                         rel_tol=5e-4, low_frac=0.5)
+    assert st.tiles_low > 0 and st.tiles_flagged >= st.tiles_low
+    _check_tiles(st, got, want, FINE, 16, 5e-4)
+
+
+def test_grid_surrogate_modes_and_network_gain(ctx):
+    """The trained network against the same pipeline without it (a zero network:
+    bilinear interpolation of the exact log-density between tile corners)."""
+    desc, refs = _setup_fine(ctx)
+    s = _train(ctx, desc, refs)
+    want = _direct_on_grid(ctx, desc, FINE)
+    res = {}
+    for name, sur, mode, tile in [("surrogate", s, bk.GRID_SURROGATE, 16),
+                                  ("net16", s, bk.GRID_ANCHORED, 16),
+                                  ("zero16", None, bk.GRID_ANCHORED, 16),
+                                  ("net32", s, bk.GRID_ANCHORED, 32),
+                                  ("zero32", None, bk.GRID_ANCHORED, 32)]:
+        got, st = _grid_eval(ctx, desc, FINE, surrogate=sur, mode=mode, tile=tile, probes=5,
+                             rel_tol=5e-4, low_frac=1e-4)
+        err = _check_tiles(st, got, want, FINE, tile, 5e-4)
+        res[name] = st
+        assert err.max() <= 1e-3, (name, err.max())
+    # with the network, more 32-point tiles keep the prediction and fewer points
+    # need an exact sum than without it
+    net, zero = res["net32"], res["zero32"]
+    assert net.tiles_surrogate > zero.tiles_surrogate, (net.as_dict(), zero.as_dict())
+    assert net.exact_points < zero.exact_points
