@@ -41,7 +41,7 @@ EXPORTED = [
     "bbkde_surrogate_get_params", "bbkde_surrogate_gradient", "bbkde_surrogate_train",
     "bbkde_surrogate_predict", "bbkde_surrogate_predict_device", "bbkde_surrogate_save",
     "bbkde_surrogate_load", "bbkde_surrogate_set_inference", "bbkde_eval_culled",
-    "bbkde_eval_grid",
+    "bbkde_eval_grid", "bbkde_lsq_numint_cv",
 ]
 
 # Dense-grid modes (bbkde_grid_config.mode).
@@ -184,6 +184,7 @@ def load_library(path: str = LIB_PATH):
                                       C.POINTER(CullStats)]
     lib.bbkde_eval_grid.argtypes = [vp, vp, kd, C.POINTER(Grid), C.POINTER(GridConfig), vp,
                                     C.POINTER(GridStats)]
+    lib.bbkde_lsq_numint_cv.argtypes = [vp, kd, C.POINTER(Grid), C.c_int, _dp]
     _lib = lib
     return lib
 
@@ -355,6 +356,14 @@ class Context:
         self._check(self.lib.bbkde_eval_grid(self.h, sh, C.byref(desc), C.byref(g), C.byref(cfg),
                                              out_ptr, C.byref(st)))
         return st
+
+    def lsq_numint_cv(self, desc: KernelDesc, grid, precision=FP32C) -> float:
+        """grid = (nx, ny, x0, x1, y0, y1)."""
+        cv = np.zeros(1)
+        g = Grid(*grid)
+        self._check(self.lib.bbkde_lsq_numint_cv(self.h, C.byref(desc), C.byref(g), precision,
+                                                 _p(cv)))
+        return float(cv[0])
 
     def set_launch_variant(self, variant: int):
         """-1 = autotune (default); 0..n-1 forces a launch shape."""

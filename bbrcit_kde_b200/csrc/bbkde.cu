@@ -121,7 +121,7 @@ struct bbkde_ctx {
       cb_smin, cb_tiles, cb_stats;
   DevBuf gr_pred, gr_order, gr_tmin, gr_tmax, gr_bad, gr_terr, gr_flag, gr_flag_ord, gr_list,
       gr_nsel, gr_counts, gr_gmax, gr_anc_order, gr_anc_exact, gr_anc_net, gr_resid, gr_pq_x,
-      gr_pq_y, gr_pq_idx, gr_pq_exact;
+      gr_pq_y, gr_pq_idx, gr_pq_exact, gr_out;
   cudaEvent_t ev3 = nullptr;
   std::string err;
 };
@@ -718,7 +718,7 @@ int bbkde_ctx_destroy(bbkde_ctx *c) {
                     &c->gr_terr, &c->gr_flag, &c->gr_flag_ord, &c->gr_list, &c->gr_nsel,
                     &c->gr_counts, &c->gr_gmax, &c->gr_anc_order, &c->gr_anc_exact,
                     &c->gr_anc_net, &c->gr_resid, &c->gr_pq_x, &c->gr_pq_y, &c->gr_pq_idx,
-                    &c->gr_pq_exact})
+                    &c->gr_pq_exact, &c->gr_out})
     release(*b);
   if (c->cv_graph) cudaGraphExecDestroy(c->cv_graph);
   if (c->ev3) cudaEventDestroy(c->ev3);
@@ -1780,6 +1780,58 @@ extern "C" int bbkde_eval_grid(bbkde_ctx *c, bbkde_surrogate *sur, const bbkde_k
   c->last_pairs = st.pairs;
   c->last_launches = 0;
   if (stats) *stats = st;
+  return BBKDE_OK;
+}
+
+// Least-squares CV with numerical integration (KernelDensityImpl.h:14-97): the
+// square integral is the culled exact density on the grid (bound 1e-7) summed
+// as f^2 dx dy in FP64; the leave-one-out term is the weighted self-sum with the
+// diagonal excluded (the reference subtracts the self term, :50-60).
+extern "C" int bbkde_lsq_numint_cv(bbkde_ctx *c, const bbkde_kernel_desc *k,
+                                   const bbkde_grid *grid, int precision, double *cv_out) {
+  Resolved r;
+  TRY(self_checks(c, k, precision, r));
+  if (!cv_out || !grid) return fail(c, BBKDE_INVALID_ARGUMENT, "NULL argument");
+  if (precision != BBKDE_FP32C)
+    return fail(c, BBKDE_UNSUPPORTED,
+                "lsq_numint_cv: FP32C only (the grid term is the culled FP32 sum)");
+  if (r.dim != 2) return fail(c, BBKDE_INVALID_ARGUMENT, "lsq_numint_cv: 2-D kernels only");
+  TRY(culled_kernel_ok(c, r));
+  PointSet &s = c->sets[BBKDE_REFERENCE];
+  if (s.n == 0) { *cv_out = 0.0; return BBKDE_OK; }
+  if (grid->nx < 1 || grid->ny < 1)
+    return fail(c, BBKDE_INVALID_ARGUMENT, "grid: need nx, ny >= 1");
+  // Leave-one-out term (:40-60).
+  TRY(ensure(c, c->out_dev, (size_t)s.n * sizeof(double)));
+  TRY(pair_sum(c, r, precision, BBKDE_REFERENCE, 0, s.n - 1, 0, s.n - 1, r.norm, true,
+               c->out_dev.as<double>(), EPI_W_VALUE, s.weight.as<double>()));
+  double llo = 0.0;
+  CUDA_TRY(c, cudaMemcpy(&llo, c->scalars.p, sizeof(double), cudaMemcpyDeviceToHost));
+  const double ms_loo = c->last_ms, pairs_loo = c->last_pairs;
+  // Square integral over the grid (:62-93).
+  const int64_t npts = grid->nx * grid->ny;
+  TRY(ensure(c, c->gr_out, (size_t)npts * sizeof(double)));
+  bbkde_grid_config cfg = {BBKDE_GRID_EXACT, 16, 1, 1, 1e-3, 0.0, 1e-7};
+  bbkde_grid_stats st;
+  TRY(bbkde_eval_grid(c, nullptr, k, grid, &cfg, c->gr_out.as<double>(), &st));
+  const unsigned nb = std::min<unsigned>(grid1d(npts, kRedBlock), 4096u);
+  TRY(ensure(c, c->block_sums, (size_t)nb * sizeof(double)));
+  k_sum_sq<<<nb, kRedBlock, 0, c->stream>>>(c->gr_out.as<double>(), npts,
+                                            c->block_sums.as<double>());
+  COUNT_LAUNCH(c);
+  k_sum_blocks<<<1, kRedBlock, 0, c->stream>>>(c->block_sums.as<double>(), nb,
+                                               c->scalars.as<double>() + 2);
+  COUNT_LAUNCH(c);
+  CUDA_TRY(c, cudaGetLastError());
+  double sum_sq = 0.0;
+  CUDA_TRY(c, cudaMemcpyAsync(&sum_sq, c->scalars.as<double>() + 2, sizeof(double),
+                              cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  const double dx = (grid->x1 - grid->x0) / grid->nx, dy = (grid->y1 - grid->y0) / grid->ny;
+  *cv_out = sum_sq * dx * dy - 2 * llo;   // :95
+  c->last_ms = ms_loo + st.ms_total;
+  c->last_pairs = pairs_loo + st.pairs;
+  c->last_launches = 0;
   return BBKDE_OK;
 }
 

@@ -593,6 +593,18 @@ k_sum_blocks(const double *block_sums, int64_t n, double *result) {
   if (threadIdx.x == 0) result[0] = b;
 }
 
+// block_sums[b] = sum of v[i]^2 over block b's grid-stride share (fixed order).
+__global__ void __launch_bounds__(kRedBlock)
+k_sum_sq(const double *v, int64_t n, double *block_sums) {
+  __shared__ double sm[kRedBlock];
+  double s = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * kRedBlock + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * kRedBlock)
+    s += v[i] * v[i];
+  const double b = block_reduce_sum(s, sm);
+  if (threadIdx.x == 0) block_sums[blockIdx.x] = b;
+}
+
 // Adaptive pilot finish (KernelDensityImpl.h:330-353):
 // g = exp(logsum), abw_i = (pilot_i / g)^-alpha, mass_i = w_i abw_i^-dim.
 __global__ void k_pilot_finalize(const double *pilot, const double *w, const double *logsum,

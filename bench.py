@@ -60,9 +60,19 @@ def parse():
                     help="target CPU time of the bounded CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", choices=["direct", "surrogate-grid"], default="direct",
+    ap.add_argument("--workload",
+                    choices=["direct", "surrogate-grid", "plain-small", "cv-batch", "direct1d"],
+                    default="direct",
                     help="direct: adaptive pilot + evaluation, 1M x 1M (the default); "
-                         "surrogate-grid: 4M references on an 8192 x 8192 grid")
+                         "surrogate-grid: 4M references on an 8192 x 8192 grid; "
+                         "plain-small: 10k references on a 100 x 100 grid (latency); "
+                         "cv-batch: 16 datasets x 64 x 64 bandwidths, one launch; "
+                         "direct1d: 1-D Gaussian, 2^24 references x 2^24 queries")
+    ap.add_argument("--cv-sets", type=int, default=16, help="cv-batch: datasets")
+    ap.add_argument("--cv-size", type=int, default=0,
+                    help="cv-batch: points per dataset (0: log-uniform in [1e4, 5e5])")
+    ap.add_argument("--n1d", type=int, default=1 << 24, help="direct1d: references")
+    ap.add_argument("--m1d", type=int, default=1 << 24, help="direct1d: queries per rank")
     ap.add_argument("--grid", type=int, default=8192, help="surrogate-grid: points per axis")
     ap.add_argument("--n-grid-ref", type=int, default=4_000_000,
                     help="surrogate-grid: reference points")
@@ -231,6 +241,12 @@ def main():
         return run_reference_arm(a, world, rank)
     if a.workload == "surrogate-grid":
         return run_surrogate_grid(a, world, rank, local)
+    if a.workload == "plain-small":
+        return run_plain_small(a, world, rank, local)
+    if a.workload == "cv-batch":
+        return run_cv_batch(a, world, rank, local)
+    if a.workload == "direct1d":
+        return run_direct1d(a, world, rank, local)
 
     import torch
     import bbrcit_kde_b200 as bk
@@ -642,6 +658,214 @@ def run_surrogate_grid(a, world, rank, local):
         "setup": info,
     }
     print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# Smaller workloads: the reference's CPU-runnable case, batched cross-validation,
+# the 1-D roofline probe.
+# ---------------------------------------------------------------------------
+def _device_setup(local):
+    import torch
+    import bbrcit_kde_b200 as bk
+    torch.cuda.set_device(local)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    ctx = bk.Context(local)
+    ctx.set_stream(stream.cuda_stream)
+    return torch, bk, stream, ctx
+
+
+def _timed(torch, stream, fn, steps, warmup, flush=None):
+    """Device time (CUDA events on `stream`) of each of `steps` calls after `warmup`."""
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    ms = []
+    for _ in range(steps):
+        if flush is not None:
+            l2_flush(torch, flush)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    return ms
+
+
+def _line(a, world, metric_unit, value, ms, config, dtype, **extra):
+    d = {"metric": METRIC, "value": value, "unit": metric_unit, "n_gpus": world,
+         "steps": a.steps, "warmup": a.warmup, "ms_per_step": float(np.mean(ms)),
+         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": dtype,
+         "data": "synthetic (seeded splitmix64 mixtures, float32-representable)",
+         "config": config}
+    d.update(extra)
+    print(json.dumps(d), flush=True)
+
+
+def run_plain_small(a, world, rank, local):
+    """10,000 references (bimodal mixture, unit weights), h = 0.1 Gaussian, 100 x 100
+    grid over [-3, 3)^2: 1e8 pair evaluations per call. Launch-latency bound; the
+    line reports the device time and the end-to-end latency of one call through the
+    C ABI (upload queries from pinned host memory, evaluate, read back)."""
+    torch, bk, stream, ctx = _device_setup(local)
+    from bbrcit_kde_b200 import workloads as W
+    from bbrcit_kde_b200.parity import error_stats
+    wl = W.config1()
+    n, m = len(wl.refs), len(wl.queries)
+    w = wl.weights / wl.weights.sum()
+    desc = bk.kernel_desc(wl.kind, 2, wl.h)
+    ctx.upload(bk.REFERENCE, wl.refs, mass=w, weight=w)
+    ctx.upload(bk.QUERY, wl.queries)
+    out = torch.empty(m, dtype=torch.float64, device="cuda")
+    launches0 = ctx.launch_count()
+    ms = _timed(torch, stream,
+                lambda: ctx.eval_range_device(desc, 0, n - 1, 0, m - 1, out.data_ptr()),
+                a.steps, a.warmup)
+    launches = (ctx.launch_count() - launches0) * a.steps // (a.steps + a.warmup)
+    pin = lambda arr: torch.from_numpy(np.ascontiguousarray(arr)).pin_memory().numpy()  # noqa
+    h_q, h_out = pin(wl.queries), pin(np.empty(m))
+
+    def e2e_step():
+        ctx.upload(bk.QUERY, h_q)
+        ctx.eval_range(desc, 0, n - 1, 0, m - 1, True, bk.FP32C, out=h_out)
+
+    e2e_ms = _timed(torch, stream, e2e_step, a.steps, a.warmup)
+    got = ctx.eval_all(desc)
+    f64 = ctx.eval_all(desc, precision=bk.FP64)
+    from oracle.pyoracle import Oracle
+    want = Oracle().direct(wl.kind, 2, wl.h, wl.refs, w, wl.queries)
+    cpu = cpu_reference_rate(wl, min(a.cpu_seconds, 4.0)) if not a.no_cpu_baseline else None
+    ctx.close()
+    pairs = float(n) * m
+    _line(a, world, UNIT, pairs * world / (np.mean(ms) / 1e3), ms,
+          {"workload": "plain 2-D Gaussian, 10k bimodal refs, h=0.1, 100x100 grid on "
+                       "[-3,3)^2 (1e8 evals per call)"}, "f32",
+          latency_us={"device": float(np.median(ms) * 1e3),
+                      "e2e_c_abi": float(np.median(e2e_ms) * 1e3)},
+          e2e={"value": pairs * world / (np.mean(e2e_ms) / 1e3), "unit": UNIT,
+               "h2d_bytes_per_step": int(h_q.nbytes), "d2h_bytes_per_step": int(h_out.nbytes)},
+          gpu_launches=int(launches),
+          cpu_baseline=cpu,
+          error_vs_reference_fp64=error_stats(got, want),
+          fp64_path_vs_oracle_max_rel=float(np.max(np.abs(f64 - want) / want)))
+    return 0
+
+
+def run_cv_batch(a, world, rank, local):
+    """Batched cross-validation: 16 datasets (log-uniform sizes in [1e4, 5e5], 3-component
+    mixtures), Epanechnikov product kernel, 64 x 64 log-spaced (hx, hy) over [0.01, 1]^2:
+    LOO likelihood and LSQ-convolution scores for every (dataset, hx, hy) in one
+    persistent graph-captured launch. One step = one bbkde_cv_batch call."""
+    torch, bk, stream, ctx = _device_setup(local)
+    from bbrcit_kde_b200 import workloads as W
+    sizes = [a.cv_size] * a.cv_sets if a.cv_size else None
+    sets = W.config3_datasets(n_sets=a.cv_sets, sizes=sizes)
+    if rank > 0:
+        sets = [s[np.argsort(W.SplitMix64(W.SEED_BASE + 300 + rank).uniform(len(s)))]
+                for s in sets]
+    hb = W.config3_bandwidths()
+    ds = [(s, None) for s in sets]
+    res = {}
+    launches0 = ctx.launch_count()
+
+    def step():
+        res["out"] = ctx.cv_batch(bk.EPANECHNIKOV_PRODUCT_2D, ds, hb, hb)
+
+    ms = _timed(torch, stream, step, a.steps, a.warmup)
+    launches = (ctx.launch_count() - launches0) // (a.steps + a.warmup)
+    _, pairs, _ = ctx.last_launch_stats()
+    lik, lsq = res["out"]
+    # Exactness: a few (dataset, hx, hy) against the per-bandwidth FP64 pair sums.
+    small = int(np.argmin([len(s) for s in sets]))
+    s0 = sets[small]
+    w0 = np.full(len(s0), 1.0 / len(s0))
+    ctx.upload(bk.REFERENCE, s0, mass=w0, weight=w0)
+    checks = []
+    for ia, ib in [(0, 0), (20, 45), (41, 49), (63, 63)]:
+        d = bk.kernel_desc(bk.EPANECHNIKOV_PRODUCT_2D, 2, (hb[ia], hb[ib]))
+        l64 = ctx.likelihood_cv(d, bk.FP64)
+        q64 = ctx.lsq_conv_cv(d, bk.FP64)
+        lg, qg = lik[small, ia, ib], lsq[small, ia, ib]
+        checks.append({"hx": hb[ia], "hy": hb[ib],
+                       "lik_rel": (abs(lg - l64) / abs(l64)) if np.isfinite(l64) else
+                       (0.0 if lg == l64 else 1.0),
+                       "lsq_rel": abs(qg - q64) / abs(q64)})
+    cpu = None
+    if rank == 0 and not a.no_cpu_baseline:
+        from oracle.pyoracle import Reference
+        if Reference.available():
+            ref = Reference()
+            s1 = s0[:10_000]
+            d = (hb[41], hb[49])
+            t0 = time.perf_counter()
+            ref.likelihood_cv(bk.EPANECHNIKOV_PRODUCT_2D, 2, d, s1, np.ones(len(s1)))
+            ref.lsq_conv_cv(bk.EPANECHNIKOV_PRODUCT_2D, 2, d, s1, np.ones(len(s1)))
+            dt = time.perf_counter() - t0
+            cpu = {"value": float(len(s1)) ** 2 * 2 / dt, "unit": "(pair, bandwidth, kernel) "
+                   "items/s", "cores": 1, "kind": "reference",
+                   "sample": f"likelihood_cross_validate + lsq_convolution_cross_validate of "
+                             f"one 10k-point dataset at one (hx, hy) = {d} (rel = abs = 0, "
+                             f"single-threaded dual tree), {dt:.1f} s"}
+    ctx.close()
+    items = pairs * hb.size * hb.size * 2
+    _line(a, world, "(pair, bandwidth, kernel) items/s", items * world / (np.mean(ms) / 1e3),
+          ms, {"workload": f"batched CV: {len(sets)} datasets (sizes {min(map(len, sets))}.."
+                           f"{max(map(len, sets))}), Epanechnikov product, 64x64 (hx,hy) "
+                           f"log-spaced on [0.01,1]^2, likelihood + LSQ-conv",
+               "pairs": pairs, "bandwidths": int(hb.size ** 2)}, "fixed-point int64 + f64",
+          gpu_launches=int(launches), exactness_vs_fp64_per_bandwidth=checks, cpu_baseline=cpu,
+          pairs_per_s=pairs * world / (np.mean(ms) / 1e3))
+    return 0
+
+
+def run_direct1d(a, world, rank, local):
+    """1-D Gaussian roofline probe: 2^24 references (5-component mixture), h = 0.02,
+    2^24 uniform queries on [-6, 6]; FP32-compensated direct sum."""
+    torch, bk, stream, ctx = _device_setup(local)
+    from bbrcit_kde_b200 import workloads as W
+    from bbrcit_kde_b200.parity import error_stats
+    wl = W.config4(n=a.n1d, m=a.m1d)
+    if rank > 0:
+        rng = W.SplitMix64(W.SEED_BASE + 400 + rank)
+        wl.queries = W.f32(rng.uniform(a.m1d, -6.0, 6.0)).reshape(-1, 1)
+    n, m = len(wl.refs), len(wl.queries)
+    w = np.full(n, 1.0 / n)
+    desc = bk.kernel_desc(wl.kind, 1, wl.h)
+    ctx.upload(bk.REFERENCE, wl.refs, mass=w, weight=w)
+    ctx.upload(bk.QUERY, wl.queries)
+    sm_count, _ = ctx.device_info()
+    out = torch.empty(m, dtype=torch.float64, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    sampler = ClockSampler(local)
+    kernel_ms = []
+
+    def step():
+        ctx.eval_range_device(desc, 0, n - 1, 0, m - 1, out.data_ptr())
+        kernel_ms.append(ctx.last_launch_stats()[0])
+
+    sampler.start()
+    ms = _timed(torch, stream, step, a.steps, a.warmup, flush)
+    clocks = sampler.stop()
+    pairs = float(n) * m
+    # error vs FP64 on 4096 queries
+    q0 = m // 2
+    f32 = ctx.eval_range(desc, 0, n - 1, q0, q0 + 4095)
+    f64 = ctx.eval_range(desc, 0, n - 1, q0, q0 + 4095, True, bk.FP64)
+    ctx.close()
+    peaks = measured_peaks()
+    sm_max = float(peaks.get("sm_max_mhz") or clocks.get("sm_max_mhz") or 1965.0)
+    peak = sm_count * MUFU_EX2_PER_CLK_PER_SM * sm_max * 1e6
+    kms = float(np.mean(kernel_ms[-a.steps:]))
+    _line(a, world, UNIT, pairs * world / (np.mean(ms) / 1e3), ms,
+          {"workload": f"1-D Gaussian, h=0.02, {n} refs (5-component mixture), {m} uniform "
+                       f"queries on [-6,6] per rank", "l2": "flushed between timed steps"},
+          "f32", clocks=clocks,
+          roofline={"bound": "sfu", "achieved": pairs / (kms / 1e3) / 1e9, "peak": peak / 1e9,
+                    "unit": "Geval/s", "frac": pairs / (kms / 1e3) / peak, "traffic": None},
+          error_vs_fp64=error_stats(f32, f64))
     return 0
 
 

@@ -340,6 +340,16 @@ BBKDE_API int bbkde_eval_grid(bbkde_ctx *ctx, bbkde_surrogate *sur,
                               const bbkde_grid_config *cfg, double *out_device,
                               bbkde_grid_stats *stats);
 
+/* Least-squares cross-validation with numerical integration of f^2
+ * (lsq_numint_cross_validate, KernelDensity.h:24-39, KernelDensityImpl.h:14-97):
+ * sum over the grid of f(p)^2 dx dy minus twice the weighted leave-one-out density
+ * sum of the REFERENCE set. 2-D kernels (Gaussian, Epanechnikov and their
+ * products), BBKDE_FP32C only: the grid term is the culled FP32-compensated sum
+ * (bound 1e-7 of each value). The reference's tree tolerances and leaf size have
+ * no counterpart (the sums are exact). */
+BBKDE_API int bbkde_lsq_numint_cv(bbkde_ctx *ctx, const bbkde_kernel_desc *kernel,
+                                  const bbkde_grid *grid, int precision, double *cv_out);
+
 /* ---- introspection ------------------------------------------------------- */
 
 /* Device time (ms, CUDA events on the launching stream) and pair count of the

@@ -269,3 +269,35 @@ int kde_oracle_lsq_conv_cv(int kind, int conv_kind, int dim, const double *h, in
   free(f);
   return 0;
 }
+
+/* KernelDensityImpl.h:14-97: LOO term over the self sums (:47-60), square
+ * integral over the grid (:66-94; grid built at :69-75 with y outer, x inner). */
+int kde_oracle_lsq_numint_cv(int kind, const double *h, int64_t n, const double *r,
+                             const double *w, const double *mass, const double *abw,
+                             double x0, double x1, int steps_x, double y0, double y1,
+                             int steps_y, int loo_mode, double *cv_out, int nthreads) {
+  const int64_t m = (int64_t)steps_x * steps_y;
+  double *f = (double *)malloc(sizeof(double) * (size_t)((n ? n : 1) + m + 2 * m));
+  if (!f) return 7;
+  double *fg = f + (n ? n : 1), *q = fg + m;
+  const double c = kde_oracle_normalization(kind, 2, h);
+  int rc = kde_oracle_self(kind, 2, h, n, r, mass, abw, loo_mode == 1, 1, f, nthreads);
+  const double dx = (x1 - x0) / steps_x, dy = (y1 - y0) / steps_y;
+  for (int j = 0; j < steps_y; ++j)
+    for (int i = 0; i < steps_x; ++i) {
+      q[2 * ((int64_t)j * steps_x + i)] = x0 + i * dx;
+      q[2 * ((int64_t)j * steps_x + i) + 1] = y0 + j * dy;
+    }
+  if (!rc) rc = kde_oracle_direct(kind, 2, h, n, r, mass, abw, m, q, 1, 1, fg, nthreads);
+  if (rc) { free(f); return rc; }
+  double llo = 0.0, sq = 0.0;
+  for (int64_t i = 0; i < n; ++i) {
+    double v = f[i];
+    if (loo_mode == 0) v -= mass[i] * c;                      /* :55-56 */
+    llo += w[i] * v;                                          /* :59 */
+  }
+  for (int64_t k = 0; k < m; ++k) sq += fg[k] * fg[k] * dx * dy;   /* :86-92 */
+  *cv_out = sq - 2 * llo;                                     /* :95 */
+  free(f);
+  return 0;
+}

@@ -64,6 +64,14 @@ int kde_oracle_lsq_conv_cv(int kind, int conv_kind, int dim, const double *h, in
                            const double *abw, int loo_mode, int gauss_conv_quirk,
                            double *cv_out, int nthreads);
 
+/* Least-squares CV with numerical integration (KernelDensityImpl.h:14-97), 2-D:
+ * sum over the steps_x x steps_y grid (x0 + i (x1 - x0) / steps_x, ...; end points
+ * excluded) of f^2 dx dy, minus 2 sum_i w_i (f_i - mass_i C). */
+int kde_oracle_lsq_numint_cv(int kind, const double *h, int64_t n, const double *r,
+                             const double *w, const double *mass, const double *abw,
+                             double x0, double x1, int steps_x, double y0, double y1,
+                             int steps_y, int loo_mode, double *cv_out, int nthreads);
+
 #ifdef __cplusplus
 }
 #endif

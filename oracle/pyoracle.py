@@ -62,6 +62,9 @@ class Oracle:
         lib.kde_oracle_lsq_conv_cv.argtypes = [C.c_int, C.c_int, C.c_int, _dp, C.c_int64,
                                                _dp, _dp, _dp, _dp, C.c_int, C.c_int, _dp,
                                                C.c_int]
+        lib.kde_oracle_lsq_numint_cv.argtypes = [C.c_int, _dp, C.c_int64, _dp, _dp, _dp, _dp,
+                                                 C.c_double, C.c_double, C.c_int, C.c_double,
+                                                 C.c_double, C.c_int, C.c_int, _dp, C.c_int]
         self.lib = lib
 
     @staticmethod
@@ -138,6 +141,19 @@ class Oracle:
         return float(cv[0])
 
 
+    def lsq_numint_cv(self, kind, h, refs, w, mass, grid, abw=None, loo_mode=1, nthreads=None):
+        """grid = (steps_x, steps_y, x0, x1, y0, y1)."""
+        refs, w, mass, abw = _c(refs), _c(w), _c(mass), _c(abw)
+        sx, sy, x0, x1, y0, y1 = grid
+        cv = np.zeros(1)
+        hh = self._h(h)
+        rc = self.lib.kde_oracle_lsq_numint_cv(kind, _p(hh), refs.shape[0], _p(refs), _p(w),
+                                               _p(mass), _p(abw), x0, x1, sx, y0, y1, sy,
+                                               loo_mode, _p(cv), nthreads or nthreads_default())
+        assert rc == 0, rc
+        return float(cv[0])
+
+
 class Reference:
     """The reference's own KernelDensity<> (FP64 CPU), compiled from its headers."""
 
@@ -151,6 +167,9 @@ class Reference:
         lib.ref_kde_likelihood_cv.argtypes = [C.c_int, C.c_int, _dp, C.c_int64, _dp, _dp,
                                               C.c_double, C.c_double, C.c_double, _dp]
         lib.ref_kde_lsq_conv_cv.argtypes = lib.ref_kde_likelihood_cv.argtypes
+        lib.ref_kde_lsq_numint_cv.argtypes = [C.c_int, _dp, C.c_int64, _dp, _dp, C.c_double,
+                                              C.c_double, C.c_double, C.c_int, C.c_double,
+                                              C.c_double, C.c_int, C.c_double, C.c_double, _dp]
         lib.ref_kde_normalization.restype = C.c_double
         lib.ref_kde_normalization.argtypes = [C.c_int, C.c_int, _dp]
         lib.ref_kde_create.restype = C.c_void_p
@@ -225,5 +244,17 @@ class Reference:
         hh = Oracle._h(h)
         rc = self.lib.ref_kde_lsq_conv_cv(kind, dim, _p(hh), refs.shape[0], _p(refs), _p(w),
                                           alpha, rel, abs_, _p(cv))
+        assert rc == 0, rc
+        return float(cv[0])
+
+    def lsq_numint_cv(self, kind, h, refs, w, grid, alpha=-1.0, rel=0.0, abs_=0.0):
+        """The reference's lsq_numint_cross_validate; grid = (steps_x, steps_y, x0, x1,
+        y0, y1)."""
+        refs, w = _c(refs), _c(w)
+        sx, sy, x0, x1, y0, y1 = grid
+        cv = np.zeros(1)
+        hh = Oracle._h(h)
+        rc = self.lib.ref_kde_lsq_numint_cv(kind, _p(hh), refs.shape[0], _p(refs), _p(w),
+                                            alpha, x0, x1, sx, y0, y1, sy, rel, abs_, _p(cv))
         assert rc == 0, rc
         return float(cv[0])

@@ -166,6 +166,33 @@ int dispatch(const Req &r) {
   return 5;  // unsupported
 }
 
+// Free function lsq_numint_cross_validate (KernelDensity.h:24-39,
+// KernelDensityImpl.h:14-97) on 2-D kernels.
+struct NumintReq {
+  double x0, x1, y0, y1;
+  int sx, sy;
+};
+
+template <typename K>
+int run_numint(const Req &r, const NumintReq &g) {
+  KdeT<2, K> kde(make_points<2, K>(r.n, r.xy, r.w), 2);
+  set_bw(kde.kernel(), r.h);
+  if (r.alpha >= 0) kde.adapt_density(r.alpha, r.rel, r.abs);
+  *r.lsq_cv = lsq_numint_cross_validate(kde, g.x0, g.x1, g.sx, g.y0, g.y1, g.sy, r.rel, r.abs,
+                                        2);
+  return 0;
+}
+
+int dispatch_numint(const Req &r, const NumintReq &g) {
+  switch (r.kind) {
+    case GAUSS: return run_numint<GaussianKernel<2, double>>(r, g);
+    case EPAN: return run_numint<EpanechnikovKernel<2, double>>(r, g);
+    case GAUSS_PROD2D: return run_numint<GaussianProductKernel2d<double>>(r, g);
+    case EPAN_PROD2D: return run_numint<EpanechnikovProductKernel2d<double>>(r, g);
+  }
+  return 5;
+}
+
 int dispatch_lsq(const Req &r) {
   if (r.dim == 1) {
     switch (r.kind) {
@@ -268,6 +295,19 @@ int ref_kde_lsq_conv_cv(int kind, int dim, const double *h, int64_t n,
     Req r{kind, dim, h, n, xy, w, alpha, rel, abs, 0, nullptr, nullptr,
           nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, cv, 1};
     return dispatch_lsq(r);
+  } catch (const std::invalid_argument &) { return 2; }
+  catch (...) { return 9; }
+}
+
+// lsq_numint_cross_validate(kde, x0, x1, sx, y0, y1, sy, rel, abs, leaf_nmax).
+int ref_kde_lsq_numint_cv(int kind, const double *h, int64_t n, const double *xy,
+                          const double *w, double alpha, double x0, double x1, int sx,
+                          double y0, double y1, int sy, double rel, double abs, double *cv) {
+  try {
+    Req r{kind, 2, h, n, xy, w, alpha, rel, abs, 0, nullptr, nullptr,
+          nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, cv, 1};
+    NumintReq g{x0, x1, y0, y1, sx, sy};
+    return dispatch_numint(r, g);
   } catch (const std::invalid_argument &) { return 2; }
   catch (...) { return 9; }
 }

@@ -77,6 +77,18 @@ CV_CASES = [
 ]
 
 
+NUMINT_CASES = [
+    # (name, kind, h, alpha, grid=(steps_x, steps_y, x0, x1, y0, y1)) on the
+    # config-2 style set of 3000 points: lsq_numint_cross_validate
+    ("numint_gaussprod2d", W.GAUSS_PROD2D, (0.1, 0.15), -1.0, (64, 48, -3.0, 3.0, -2.5, 2.5)),
+    ("numint_epanprod2d", W.EPAN_PROD2D, (0.4, 0.3), -1.0, (64, 48, -3.0, 3.0, -2.5, 2.5)),
+    ("numint_gauss2d", W.GAUSS, (0.12, 0.12), -1.0, (80, 80, -3.0, 3.0, -3.0, 3.0)),
+    ("numint_epan2d", W.EPAN, (0.3, 0.3), -1.0, (80, 80, -3.0, 3.0, -3.0, 3.0)),
+    ("numint_adaptive_gaussprod2d", W.GAUSS_PROD2D, (0.1, 0.15), 0.5,
+     (64, 48, -3.0, 3.0, -2.5, 2.5)),
+]
+
+
 def main() -> int:
     build()
     ref = Reference()
@@ -101,6 +113,12 @@ def main() -> int:
                             h=np.array(h, float), n=len(refs),
                             input_digest=digest(refs, wl.weights), likelihood=lik, lsq=lsq)
         print(name, lik, lsq)
+    for name, kind, h, alpha, grid in NUMINT_CASES:
+        cv = ref.lsq_numint_cv(kind, h, wl.refs, wl.weights, grid, alpha=alpha)
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), kind=kind, dim=2,
+                            h=np.array(h, float), alpha=alpha, grid=np.array(grid, float),
+                            n=len(wl.refs), input_digest=digest(wl.refs, wl.weights), cv=cv)
+        print(name, cv)
     return 0
 
 

@@ -36,6 +36,23 @@ CV_CASES = {
 }
 
 
+NUMINT_CASES = {
+    # name -> (kind, h, alpha, grid=(steps_x, steps_y, x0, x1, y0, y1))
+    "numint_gaussprod2d": (W.GAUSS_PROD2D, (0.1, 0.15), -1.0, (64, 48, -3.0, 3.0, -2.5, 2.5)),
+    "numint_epanprod2d": (W.EPAN_PROD2D, (0.4, 0.3), -1.0, (64, 48, -3.0, 3.0, -2.5, 2.5)),
+    "numint_gauss2d": (W.GAUSS, (0.12, 0.12), -1.0, (80, 80, -3.0, 3.0, -3.0, 3.0)),
+    "numint_epan2d": (W.EPAN, (0.3, 0.3), -1.0, (80, 80, -3.0, 3.0, -3.0, 3.0)),
+    "numint_adaptive_gaussprod2d": (W.GAUSS_PROD2D, (0.1, 0.15), 0.5,
+                                    (64, 48, -3.0, 3.0, -2.5, 2.5)),
+}
+
+
+def numint_inputs(name):
+    kind, h, alpha, grid = NUMINT_CASES[name]
+    wl = W.config2(n=3000, m=1)
+    return kind, h, alpha, grid, wl.refs, wl.weights
+
+
 def digest(*arrays) -> str:
     h = hashlib.sha256()
     for a in arrays:

@@ -7,8 +7,9 @@ import pytest
 
 import bbrcit_kde_b200 as bk
 from bbrcit_kde_b200 import workloads as W
-from tests.helpers import (ADAPTIVE_CASES, CV_CASES, adaptive_inputs, assert_parity, cv_inputs,
-                           load_golden, match_by_coords)
+from tests.helpers import (ADAPTIVE_CASES, CV_CASES, NUMINT_CASES, adaptive_inputs,
+                           assert_parity, cv_inputs, load_golden, match_by_coords,
+                           numint_inputs)
 
 pytestmark = pytest.mark.gpu
 
@@ -103,3 +104,23 @@ def test_lsq_requires_a_convolution_kernel(ctx):
     ctx.upload(bk.REFERENCE, np.zeros((4, 2)), mass=np.full(4, 0.25))
     with pytest.raises(bk.BBKDEError):
         ctx.lsq_conv_cv(bk.kernel_desc(W.GAUSS, 2, (0.3,)))   # no 2-D iso conv kernel
+
+
+@pytest.mark.parametrize("name", sorted(NUMINT_CASES))
+def test_lsq_numint_matches_golden(ctx, name):
+    """bbkde_lsq_numint_cv against the reference's lsq_numint_cross_validate.
+    Tolerance: 2e-6 relative -- FP32-compensated sums (1e-7 per density value,
+    culled grid bound 1e-7) in both terms of sq - 2 llo, whose magnitudes are
+    close to |cv| here."""
+    g = load_golden(name)
+    kind, h, alpha, grid, refs, w = numint_inputs(name)
+    wn = w / w.sum()
+    ctx.upload(bk.REFERENCE, refs, mass=wn, weight=wn)
+    desc = bk.kernel_desc(kind, 2, h)
+    if alpha >= 0:
+        ctx.adapt_density(desc, alpha, bk.FP32C, outputs=False)
+    sx, sy, x0, x1, y0, y1 = grid
+    got = ctx.lsq_numint_cv(desc, (sx, sy, x0, x1, y0, y1))
+    assert got == pytest.approx(float(g["cv"]), rel=2e-6)
+    with pytest.raises(bk.BBKDEError):
+        ctx.lsq_numint_cv(desc, (sx, sy, x0, x1, y0, y1), precision=bk.FP64)

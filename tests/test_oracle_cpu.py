@@ -12,7 +12,8 @@ import numpy as np
 import pytest
 
 from bbrcit_kde_b200 import workloads as W
-from tests.helpers import (ADAPTIVE_CASES, CV_CASES, PLAIN_CASES, adaptive_inputs, cv_inputs,
+from tests.helpers import (ADAPTIVE_CASES, CV_CASES, NUMINT_CASES, PLAIN_CASES, adaptive_inputs,
+                           cv_inputs, numint_inputs,
                            digest, load_golden, match_by_coords, plain_inputs)
 
 TOL = 1e-12   # FP64 vs FP64: only summation order differs
@@ -97,6 +98,22 @@ def test_kernels_integrate_to_one(oracle):
         assert vals.sum() * 0.04 ** 2 == pytest.approx(target, rel=5e-3), kind
     vals = oracle.direct(W.GAUSS_PROD_CONV2D, 2, (0.7, 0.9), one2, np.ones(1), g, quirk=False)
     assert vals.sum() * 0.04 ** 2 == pytest.approx(1.0, rel=5e-3)
+
+
+@pytest.mark.parametrize("name", sorted(NUMINT_CASES))
+@pytest.mark.parametrize("loo_mode", [0, 1])
+def test_oracle_lsq_numint_matches_golden(oracle, name, loo_mode):
+    """lsq_numint_cross_validate (KernelDensityImpl.h:14-97) against the value the
+    reference's own function produced (tests/golden/make_golden.py)."""
+    g = load_golden(name)
+    kind, h, alpha, grid, refs, w = numint_inputs(name)
+    assert g["input_digest"] == digest(refs, w)
+    wn = w / w.sum()
+    mass, abw = wn, None
+    if alpha >= 0:
+        _, abw, mass, _ = oracle.adapt(kind, 2, h, refs, wn, alpha)
+    got = oracle.lsq_numint_cv(kind, h, refs, wn, mass, grid, abw=abw, loo_mode=loo_mode)
+    assert got == pytest.approx(float(g["cv"]), rel=1e-10)
 
 
 def test_adapt_rejects_bad_alpha(oracle):
