@@ -89,6 +89,31 @@ def dist_env():
     return world, rank, local
 
 
+def rank_queries(W, wl, rank: int, m: int):
+    """Query batch of `rank`: rank 0 keeps the configuration's own queries, every
+    other rank draws its own seeded batch from the same distribution (queries are
+    independent, so ranks share no data-path collective)."""
+    if rank == 0:
+        return wl.queries
+    rng = W.SplitMix64(W.SEED_BASE + 200 + rank)
+    return W.f32(rng.uniform(2 * m, -3.0, 3.0).reshape(m, 2))
+
+
+def max_over_ranks(dist, ms: float, device) -> float:
+    """The job's time: the slowest rank's (all_reduce MAX); ms itself without dist."""
+    if dist is None:
+        return ms
+    import torch
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(units_per_rank_step: float, steps: int, world: int, total_ms: float) -> float:
+    """Units processed by all ranks divided by the (max-over-ranks) time."""
+    return units_per_rank_step * steps * world / (total_ms / 1e3)
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -262,9 +287,7 @@ def main():
                                 device_id=torch.device("cuda", local))
 
     wl = W.config2(n=a.n, m=a.m)
-    if rank > 0:   # each rank its own query batch
-        rng = W.SplitMix64(W.SEED_BASE + 200 + rank)
-        wl.queries = W.f32(rng.uniform(2 * a.m, -3.0, 3.0).reshape(a.m, 2))
+    wl.queries = rank_queries(W, wl, rank, a.m)
     wn = wl.weights / wl.weights.sum()
     n, m = len(wl.refs), len(wl.queries)
     evals_per_step = 2.0 * n * m
@@ -309,13 +332,10 @@ def main():
         kernel_launches += [s1, s2]
     launches = ctx.launch_count() - launches0
     clocks = sampler.stop()
-    total_ms = sum(step_ms)
+    total_ms = max_over_ranks(dist, sum(step_ms), "cuda")
     if dist:
-        t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
         dist.barrier()
-    value = evals_per_step * a.steps * world / (total_ms / 1e3)
+    value = whole_job_rate(evals_per_step, a.steps, world, total_ms)
 
     # roofline of the pair-sum kernel (pilot and evaluation launches)
     ach = [p / (ms / 1e3) for ms, p, _ in kernel_launches if ms > 0]
@@ -383,14 +403,10 @@ def main():
             e1.record(stream)
             torch.cuda.synchronize()
             e2e_ms.append(e0.elapsed_time(e1))
-        tot = sum(e2e_ms)
-        if dist:
-            t = torch.tensor([tot], dtype=torch.float64, device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            tot = float(t.item())
+        tot = max_over_ranks(dist, sum(e2e_ms), "cuda")
         h2d = h_refs.nbytes + 2 * h_w.nbytes + h_q.nbytes
         d2h = h_out.nbytes
-        e2e = {"value": evals_per_step * a.steps * world / (tot / 1e3), "unit": UNIT,
+        e2e = {"value": whole_job_rate(evals_per_step, a.steps, world, tot), "unit": UNIT,
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
 
     cpu = None

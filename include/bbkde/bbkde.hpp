@@ -17,9 +17,12 @@
 //   * points() is in lexicographic order with exact duplicates merged (the
 //     reference's Kd-tree merges duplicates too, Kdtree.h:365-390, but stores
 //     points in Kd-tree order).
-//   * eval(...) with rel/abs tolerances evaluates the exact direct sum, which
-//     satisfies any tolerance; query order is preserved (the reference's
-//     vector overload returns queries in Kd-tree order, KernelDensityImpl.h:642-651).
+//   * eval(...) with rel/abs tolerances runs the culled direct sum
+//     (bbkde_eval_culled: every value within rel_err of the full sum, a
+//     deterministic bound instead of the reference's tree bounds) for FP32
+//     kernels with rel_err in (0, 1), and the exact direct sum otherwise; query
+//     order is preserved (the reference's vector overload returns queries in
+//     Kd-tree order, KernelDensityImpl.h:642-651).
 //   * Kernel float type selects the device arithmetic: float kernels run the
 //     FP32-compensated path, double kernels the FP64 path (the reference runs
 //     its GPU path in the kernel's float type as well).
@@ -635,20 +638,25 @@ class KernelDensity {
     direct_eval(queries, kernel_, block_size);
   }
 
-  // Tolerance-driven evaluation: the exact direct sum meets every tolerance.
+  // Tolerance-driven evaluation (KernelDensityImpl.h:473-680): the culled sum
+  // within rel_err of the full sum (FP32 kernels), else the exact direct sum;
+  // either meets the reference's rel_err / abs_err contract.
   FloatT eval(DataPointType &p, FloatType rel_err, FloatType abs_err) const {
-    (void)rel_err; (void)abs_err;
-    return direct_eval(p);
+    std::vector<DataPointType> q(1, p);
+    eval(q, rel_err, abs_err);
+    p.attributes().set_lower(q[0].attributes().lower());
+    p.attributes().set_upper(q[0].attributes().upper());
+    return q[0].attributes().value();
   }
   void eval(std::vector<DataPointType> &queries, FloatType rel_err, FloatType abs_err,
             int leaf_nmax = 2, size_t block_size = 128) const {
-    (void)rel_err; (void)abs_err; (void)leaf_nmax;
-    direct_eval(queries, kernel_, block_size);
+    (void)abs_err; (void)leaf_nmax;
+    tolerance_eval(queries, rel_err, block_size);
   }
   void eval(KdtreeType &query_tree, FloatType rel_err, FloatType abs_err,
             size_t block_size = 128) const {
-    (void)rel_err; (void)abs_err;
-    direct_eval(query_tree.points(), kernel_, block_size);
+    (void)abs_err;
+    tolerance_eval(query_tree.points(), rel_err, block_size);
   }
 
   // adapt_density / unadapt_density (KernelDensityImpl.h:254-359)
@@ -722,6 +730,20 @@ class KernelDensity {
     return q;
   }
 
+  // Square-integral + leave-one-out CV on the device (bbkde_lsq_numint_cv); false
+  // when the kernel or precision has no device path (the caller then sums on
+  // the host over direct evaluations).
+  bool device_lsq_numint(double x0, double x1, int sx, double y0, double y1, int sy,
+                         double &cv) const {
+    bbkde_kernel_desc k = kernel_.bbkde_desc();
+    if (D != 2 || precision_ != BBKDE_FP32C || k.kind == BBKDE_EPANECHNIKOV_PRODUCT_CONV_2D)
+      return false;
+    bbkde_ctx *c = refs_uploaded();
+    bbkde_grid g = {(int64_t)sx, (int64_t)sy, x0, x1, y0, y1};
+    bbkde_detail::check(bbkde_lsq_numint_cv(c, &k, &g, precision_, &cv), c);
+    return true;
+  }
+
   // Direct evaluation with an arbitrary kernel (used by the numerical-integration
   // least-squares CV below, as the reference's template helper is).
   template <typename KernT>
@@ -747,6 +769,26 @@ class KernelDensity {
   }
 
  private:
+  void tolerance_eval(std::vector<DataPointType> &queries, FloatType rel_err,
+                      size_t block_size) const {
+    bbkde_kernel_desc k = kernel_.bbkde_desc();
+    const bool culled = precision_ == BBKDE_FP32C && rel_err > 0 && rel_err < 1 &&
+                        k.kind != BBKDE_EPANECHNIKOV_PRODUCT_CONV_2D &&
+                        k.kind != BBKDE_EPANECHNIKOV_CONV_1D && size() > 0;
+    if (!culled || queries.empty()) {
+      direct_eval(queries, kernel_, block_size);
+      return;
+    }
+    bbkde_ctx *c = refs_uploaded();
+    bbkde_detail::upload_points<D>(c, BBKDE_QUERY, queries, false);
+    std::vector<double> out(queries.size());
+    bbkde_detail::check(bbkde_eval_culled(c, &k, 1, double(rel_err), out.data(), 0, nullptr),
+                        c);
+    for (size_t i = 0; i < queries.size(); ++i) {
+      queries[i].attributes().set_lower(FloatT(out[i]));
+      queries[i].attributes().set_upper(FloatT(out[i]));
+    }
+  }
   void initialize_attributes(std::vector<DataPointType> &pts) {
     FloatType total = 0;
     for (const auto &p : pts) total += p.attributes().weight();
@@ -790,6 +832,9 @@ FT lsq_numint_cross_validate(const KernelDensity<2, KT, FT, AT> &kde, FT start_x
                              FT rel_err = 1e-6, FT abs_err = 1e-8, int qtree_leaf_nmax = 1024,
                              size_t block_size = 128) {
   (void)rel_err; (void)abs_err; (void)qtree_leaf_nmax;
+  double dev_cv = 0;
+  if (kde.device_lsq_numint(start_x, end_x, steps_x, start_y, end_y, steps_y, dev_cv))
+    return FT(dev_cv);
   using P = typename KernelDensity<2, KT, FT, AT>::DataPointType;
   std::vector<P> self(kde.points());
   kde.direct_eval(self, kde.kernel(), block_size);

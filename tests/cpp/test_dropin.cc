@@ -269,6 +269,56 @@ void test_one_dimensional() {
 
 }  // namespace
 
+void test_tolerance_eval_and_device_numint() {
+  // KernelDensity::eval(queries, rel_err, abs_err) with an FP32 kernel runs the
+  // culled sum (every value within rel_err of the full sum); the reference's
+  // tree eval promises the same tolerance.
+  using Kern = GaussianKernel<2, float>;
+  std::mt19937 e(21);
+  std::vector<Pt> data, queries;
+  bimodal(e, data, 6000, true);
+  grid(queries, -3.0, 3.0, 120);
+  KernelDensity<2, Kern, double> kde(data);
+  kde.kernel().set_bandwidth(0.08f);
+  kde.adapt_density(0.5);
+  std::vector<Pt> got(queries);
+  kde.eval(got, 1e-6, 1e-8);
+  GaussianKernel<2, double> k(0.08f);
+  std::vector<double> cpu(queries.size()), gpu(queries.size());
+  for (size_t i = 0; i < queries.size(); ++i) {
+    cpu[i] = cpu_density(k, kde.points(), queries[i]);
+    gpu[i] = got[i].attributes().value();
+  }
+  std::string why;
+  report("KernelDensity::eval(rel 1e-6) culled", consistent(cpu, gpu, cpu.size(), why), why);
+
+  // lsq_numint_cross_validate on the device (FP32 kernel) against the host sum
+  // of the same terms over FP64 CPU densities.
+  const double x0 = -4, x1 = 4, y0 = -4, y1 = 4;
+  const int sx = 160, sy = 160;
+  double dev = lsq_numint_cross_validate(kde, x0, x1, sx, y0, y1, sy);
+  const auto &pts = kde.points();
+  double llo = 0, sq = 0;
+  for (size_t i = 0; i < pts.size(); ++i) {
+    double f = 0;
+    for (size_t j = 0; j < pts.size(); ++j)
+      if (j != i)
+        f += pts[j].attributes().mass() *
+             k.unnormalized_eval(pts[i].point(), pts[j].point(), pts[j].attributes().abw());
+    llo += pts[i].attributes().weight() * f * k.normalization();
+  }
+  const double dx = (x1 - x0) / sx, dy = (y1 - y0) / sy;
+  for (int j = 0; j < sy; ++j)
+    for (int i = 0; i < sx; ++i) {
+      Pt q = {{(double)(float)(x0 + i * dx), (double)(float)(y0 + j * dy)}};
+      double f = cpu_density(k, pts, q);
+      sq += f * f * dx * dy;
+    }
+  double want = sq - 2 * llo;
+  report("lsq_numint_cross_validate on the device", std::fabs(dev - want) < 2e-6 * std::fabs(want),
+         std::to_string(dev) + " vs " + std::to_string(want));
+}
+
 int main() {
   try {
     test_cuda_direct_kde();
@@ -276,6 +326,7 @@ int main() {
     test_cross_validation();
     test_gaussian_likelihood();
     test_one_dimensional();
+    test_tolerance_eval_and_device_numint();
   } catch (const std::exception &ex) {
     std::cout << "ERROR " << ex.what() << std::endl;
     return 2;
