@@ -41,8 +41,11 @@ EXPORTED = [
     "bbkde_surrogate_get_params", "bbkde_surrogate_gradient", "bbkde_surrogate_train",
     "bbkde_surrogate_predict", "bbkde_surrogate_predict_device", "bbkde_surrogate_save",
     "bbkde_surrogate_load", "bbkde_surrogate_set_inference", "bbkde_eval_culled",
-    "bbkde_eval_grid", "bbkde_lsq_numint_cv",
+    "bbkde_eval_grid", "bbkde_lsq_numint_cv", "bbkde_surrogate_set_engine",
 ]
+
+# Surrogate inference engines (bbkde_surrogate_set_engine).
+ENGINE_TCGEN05, ENGINE_MMA_SYNC = 0, 1
 
 # Dense-grid modes (bbkde_grid_config.mode).
 GRID_EXACT, GRID_SURROGATE, GRID_ANCHORED = 0, 1, 2
@@ -180,6 +183,7 @@ def load_library(path: str = LIB_PATH):
     lib.bbkde_eval_noalloc.argtypes = [kd, i64, vp, vp, vp, vp, i64, vp, vp, C.c_int, vp, vp,
                                        C.c_char_p, i64]
     lib.bbkde_surrogate_set_inference.argtypes = [vp, C.c_int]
+    lib.bbkde_surrogate_set_engine.argtypes = [vp, C.c_int]
     lib.bbkde_eval_culled.argtypes = [vp, kd, C.c_int, C.c_double, vp, C.c_int,
                                       C.POINTER(CullStats)]
     lib.bbkde_eval_grid.argtypes = [vp, vp, kd, C.POINTER(Grid), C.POINTER(GridConfig), vp,
@@ -467,6 +471,10 @@ class Surrogate:
     def set_inference(self, split_activations: bool):
         """False: BF16 activations (as trained); True: two-term BF16 activations."""
         self._check(self.lib.bbkde_surrogate_set_inference(self.h, int(split_activations)))
+
+    def set_engine(self, engine: int):
+        """ENGINE_TCGEN05 (default) or ENGINE_MMA_SYNC."""
+        self._check(self.lib.bbkde_surrogate_set_engine(self.h, engine))
 
     def save(self, path):
         self._check(self.lib.bbkde_surrogate_save(self.h, str(path).encode()))

@@ -1293,6 +1293,7 @@ namespace bbkde {
 int surrogate_infer(bbkde_surrogate *s, cudaStream_t st, int64_t n, const float2 *xy,
                     int64_t gnx, double gx0, double gdx, double gy0, double gdy, float *out);
 int surrogate_device(const bbkde_surrogate *s);
+int surrogate_check(bbkde_surrogate *s);
 }  // namespace bbkde
 
 namespace {
@@ -1780,6 +1781,8 @@ extern "C" int bbkde_eval_grid(bbkde_ctx *c, bbkde_surrogate *sur, const bbkde_k
   c->last_pairs = st.pairs;
   c->last_launches = 0;
   if (stats) *stats = st;
+  if (mode != BBKDE_GRID_EXACT && sur && bbkde::surrogate_check(sur) != BBKDE_OK)
+    return fail(c, BBKDE_TIMEOUT, "grid: surrogate inference wait expired");
   return BBKDE_OK;
 }
 

@@ -1,0 +1,295 @@
+// Surrogate inference on the 5th-generation tensor cores (tcgen05, sm_100a).
+//
+// Same network and arithmetic as k_mlp_infer (mlp.cuh): FP32 input layer,
+// two 128 x 128 BF16 layers with FP32 accumulation, FP32 output layer, SiLU.
+// Here the 128 x 128 layers are single tcgen05.mma instructions
+// (M = 128 points, N = 128 features, K = 16 per instruction, 8 per layer; 16 with
+// two-term activations) reading both operands from shared memory and
+// accumulating in tensor memory:
+//   * one CTA per SM, two warpgroups; each warpgroup owns a 128-point tile, a
+//     128-column FP32 accumulator in TMEM and an mbarrier, and the two share the
+//     BF16 weight matrices staged once in shared memory, so one warpgroup's
+//     epilogue (bias, SiLU, BF16 packing) overlaps the other's MMAs;
+//   * thread t of a warpgroup owns point t of its tile: it computes the input
+//     layer, writes its activation row into the A operand, and after the MMA
+//     reads its accumulator row back from TMEM lane t (tcgen05.ld 32x32b);
+//   * operands use the canonical K-major layout without swizzle: element (r, k)
+//     of a 128 x 128 BF16 matrix at byte (k / 8) * 2048 + (r / 8) * 128 +
+//     (r % 8) * 16 + (k % 8) * 2, i.e. 8 x 16-byte core matrices, 128 B apart
+//     along rows (stride byte offset) and 2048 B apart along K (leading byte
+//     offset);
+//   * every wait on an mbarrier is bounded; on expiry the kernel records an
+//     error in *status and stops issuing work.
+#pragma once
+
+#include <cstdint>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include "mlp.cuh"
+
+namespace bbkde {
+namespace mlp {
+
+constexpr int kTcRows = 128;                 // points per tile (MMA M)
+constexpr int kTcWarpgroups = 2;             // tiles in flight per CTA
+constexpr int kTcThreads = 128 * kTcWarpgroups;
+constexpr uint32_t kTcTmemCols = 128 * kTcWarpgroups;
+constexpr uint32_t kTcMatBytes = 128 * 128 * 2;   // one 128 x 128 BF16 operand
+// BF16 x BF16 -> FP32, A and B K-major, N = 128 (bits 17..22: N / 8), M = 128
+// (bits 24..28: M / 16); c_format F32 = 1 at bit 4, a/b_format BF16 = 1 at bits 7, 10.
+constexpr uint32_t kTcIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((128u >> 3) << 17) |
+                              ((128u >> 4) << 24);
+constexpr long long kTcWaitLimit = 1ll << 26;   // try_wait polls before giving up
+
+template <bool kSplit>
+struct TcSmem {
+  static constexpr size_t kW = 0;                                  // W2, W3
+  static constexpr size_t kA = 2 * kTcMatBytes;                    // per warpgroup: hi (, lo)
+  static constexpr size_t kAPerWg = (kSplit ? 2 : 1) * kTcMatBytes;
+  static constexpr size_t kF = kA + kTcWarpgroups * kAPerWg;       // FP32 vectors
+  static constexpr size_t kFloats = 2 * kH + 3 * kH + kH;          // W1, b1..b3, w4
+  static constexpr size_t kBar = kF + kFloats * sizeof(float);     // mbarriers (8 B each)
+  static constexpr size_t kTmem = kBar + 8 * kTcWarpgroups;        // TMEM base address
+  static constexpr size_t kFail = kTmem + 8;                       // per warpgroup: wait expired
+  static constexpr size_t kBytes = kFail + 4 * kTcWarpgroups;
+};
+
+__device__ __forceinline__ uint32_t tc_off(int r, int k) {
+  return (uint32_t)((k >> 3) * 2048 + (r >> 3) * 128 + (r & 7) * 16 + (k & 7) * 2);
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// Shared-memory matrix descriptor: K-major, no swizzle, LBO 2048 B, SBO 128 B,
+// descriptor version 1 (bit 46).
+__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(2048u >> 4) << 16) |
+         ((uint64_t)(128u >> 4) << 32) | (1ull << 46);
+}
+
+__device__ __forceinline__ void tc_mma(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                       uint32_t accumulate) {
+  const uint32_t zero = 0;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}\n"
+      :
+      : "r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(kTcIdesc), "r"(accumulate), "r"(zero));
+}
+
+__device__ __forceinline__ void tc_commit(uint32_t mbar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+               ::"r"(mbar)
+               : "memory");
+}
+
+// Bounded wait for the mbarrier phase `parity` to complete; false on expiry.
+__device__ __forceinline__ bool tc_wait(uint32_t mbar, uint32_t parity) {
+  for (long long i = 0; i < kTcWaitLimit; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(mbar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void fence_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void wg_sync(int wg) {
+  asm volatile("bar.sync %0, 128;" ::"r"(1 + wg) : "memory");
+}
+
+// 32 consecutive FP32 accumulator columns of this thread's TMEM lane.
+__device__ __forceinline__ void tc_ld32(uint32_t taddr, float (&v)[32]) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+      "%11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, "
+      "%28, %29, %30, %31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+        "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]),
+        "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),
+        "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// Eight activations (features k0 .. k0 + 7 of row r) into the A operand(s).
+template <bool kSplit>
+__device__ __forceinline__ void tc_store8(unsigned char *ahi, unsigned char *alo, int r, int k0,
+                                          const float *a) {
+  uint32_t hi[4], lo[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const __nv_bfloat162 h = __floats2bfloat162_rn(a[2 * i], a[2 * i + 1]);
+    hi[i] = *reinterpret_cast<const uint32_t *>(&h);
+    if (kSplit) {
+      const float2 hf = __bfloat1622float2(h);
+      lo[i] = pack_bf16(a[2 * i] - hf.x, a[2 * i + 1] - hf.y);
+    }
+  }
+  *reinterpret_cast<uint4 *>(ahi + tc_off(r, k0)) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+  if (kSplit)
+    *reinterpret_cast<uint4 *>(alo + tc_off(r, k0)) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+}
+
+struct TcArgs {
+  InferArgs in;
+  int *status;   // set to 1 if a wait expired
+};
+
+template <bool kSplit>
+__global__ void __launch_bounds__(kTcThreads, 1) k_mlp_infer_tc(TcArgs ta) {
+  using L = TcSmem<kSplit>;
+  extern __shared__ __align__(1024) unsigned char smem[];
+  const InferArgs &a = ta.in;
+  unsigned char *W2 = smem + L::kW, *W3 = W2 + kTcMatBytes;
+  float *fp = reinterpret_cast<float *>(smem + L::kF);
+  float *W1 = fp, *b1 = W1 + 2 * kH, *b2 = b1 + kH, *b3 = b2 + kH, *w4 = b3 + kH;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::kBar);
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + L::kTmem);
+  volatile int *fail = reinterpret_cast<volatile int *>(smem + L::kFail);
+
+  const int tid = threadIdx.x, wg = tid >> 7, row = tid & 127, warp = tid >> 5;
+  // Weights into the canonical layout; FP32 vectors.
+  for (int i = tid; i < kH * kH; i += kTcThreads) {
+    const int n = i / kH, k = i % kH;
+    *reinterpret_cast<__nv_bfloat16 *>(W2 + tc_off(n, k)) = a.w2[i];
+    *reinterpret_cast<__nv_bfloat16 *>(W3 + tc_off(n, k)) = a.w3[i];
+  }
+  for (int i = tid; i < 2 * kH; i += kTcThreads) W1[i] = a.params[kOffW1 + i];
+  for (int i = tid; i < kH; i += kTcThreads) {
+    b1[i] = a.params[kOffB1 + i];
+    b2[i] = a.params[kOffB2 + i];
+    b3[i] = a.params[kOffB3 + i];
+    w4[i] = a.params[kOffW4 + i];
+  }
+  if (tid < kTcWarpgroups) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bars[tid])));
+    fail[tid] = 0;
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                 ::"r"(smem_u32(tmem_slot)), "r"(kTcTmemCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  fence_async_smem();
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const float b4 = a.params[kOffB4];
+
+  unsigned char *ahi = smem + L::kA + wg * L::kAPerWg;
+  unsigned char *alo = ahi + kTcMatBytes;
+  const uint32_t tmem_d = tmem + (uint32_t)(wg * 128);          // this warpgroup's columns
+  const uint32_t taddr = tmem_d + ((uint32_t)((warp & 3) * 32) << 16);   // this warp's lanes
+  const uint32_t mbar = smem_u32(&bars[wg]);
+  const uint32_t w2s = smem_u32(W2), w3s = smem_u32(W3);
+  const uint32_t ahs = smem_u32(ahi), als = smem_u32(alo);
+  uint32_t phase = 0;
+  bool ok = true;
+
+  // One 128 x 128 layer: A (and A_lo) x W^T -> TMEM, issued by thread 0 of the
+  // warpgroup after every row is written; returns false (uniformly across the
+  // warpgroup) if a wait expired.
+  auto layer = [&](uint32_t ws) -> bool {
+    fence_async_smem();
+    tc_fence_before();
+    wg_sync(wg);
+    if (row == 0) {
+      tc_fence_after();
+#pragma unroll
+      for (int s = 0; s < kH / 16; ++s) {
+        const uint64_t bd = tc_desc(ws + s * 4096);
+        if (kSplit) tc_mma(tmem_d, tc_desc(als + s * 4096), bd, s > 0 ? 1u : 0u);
+        tc_mma(tmem_d, tc_desc(ahs + s * 4096), bd, (kSplit || s > 0) ? 1u : 0u);
+      }
+      tc_commit(mbar);
+    }
+    if (!tc_wait(mbar, phase)) fail[wg] = 1;
+    phase ^= 1u;
+    tc_fence_after();
+    wg_sync(wg);          // every thread of the warpgroup has waited: one verdict
+    return fail[wg] == 0;
+  };
+
+  const int64_t tiles = (a.n + kTcRows - 1) / kTcRows;
+  for (int64_t tile = (int64_t)blockIdx.x * kTcWarpgroups + wg; tile < tiles && ok;
+       tile += (int64_t)gridDim.x * kTcWarpgroups) {
+    const int64_t p = tile * kTcRows + row;
+    float2 q = make_float2(0.f, 0.f);
+    if (a.xy) {
+      if (p < a.n) q = a.xy[p];
+    } else {
+      q = make_float2((float)(a.gx0 + (double)(p % a.gnx) * a.gdx),
+                      (float)(a.gy0 + (double)(p / a.gnx) * a.gdy));
+    }
+    const float x = (q.x - a.norm.cx) * a.norm.sx, y = (q.y - a.norm.cy) * a.norm.sy;
+    // Input layer (FP32) -> A.
+#pragma unroll 1
+    for (int k0 = 0; k0 < kH; k0 += 8) {
+      float v[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int n = k0 + i;
+        v[i] = silu(fmaf(W1[2 * n], x, fmaf(W1[2 * n + 1], y, b1[n])));
+      }
+      tc_store8<kSplit>(ahi, alo, row, k0, v);
+    }
+    // Hidden layer 2 -> A, hidden layer 3 -> output.
+    float out = 0.f;
+#pragma unroll 1
+    for (int l = 0; l < 2 && ok; ++l) {
+      if (!layer(l == 0 ? w2s : w3s)) { ok = false; break; }
+      const float *bias = l == 0 ? b2 : b3;
+#pragma unroll 1
+      for (int c = 0; c < kH; c += 32) {
+        float v[32];
+        tc_ld32(taddr + (uint32_t)c, v);
+#pragma unroll
+        for (int i = 0; i < 32; ++i) v[i] = silu(v[i] + bias[c + i]);
+        if (l == 0) {
+#pragma unroll
+          for (int j = 0; j < 32; j += 8) tc_store8<kSplit>(ahi, alo, row, c + j, v + j);
+        } else {
+#pragma unroll
+          for (int i = 0; i < 32; ++i) out = fmaf(w4[c + i], v[i], out);
+        }
+      }
+    }
+    if (ok && p < a.n) a.out[p] = a.norm.mu + a.norm.sigma * (out + b4);
+  }
+  if (!ok && row == 0) atomicExch(ta.status, 1);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(kTcTmemCols));
+}
+
+}  // namespace mlp
+}  // namespace bbkde

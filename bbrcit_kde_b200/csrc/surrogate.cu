@@ -16,6 +16,7 @@
 
 #include "../../include/bbkde.h"
 #include "mlp.cuh"
+#include "mlp_tc.cuh"
 
 using namespace bbkde::mlp;
 
@@ -36,6 +37,8 @@ struct bbkde_surrogate {
   size_t pred_cap = 0;
   int64_t adam_step = 0;
   int split = 0;   // inference with two-term BF16 activations
+  int engine = BBKDE_ENGINE_TCGEN05;
+  int *status = nullptr;   // device flag set by the tcgen05 kernel if a wait expired
   std::string err;
 };
 
@@ -195,7 +198,9 @@ int bbkde_surrogate_create(int device, uint64_t seed, bbkde_surrogate **out) {
         cudaMalloc(&s->grad, kParams * sizeof(float)) != cudaSuccess ||
         cudaMalloc(&s->loss, sizeof(float)) != cudaSuccess ||
         cudaMalloc(&s->w2, kH * kH * sizeof(__nv_bfloat16)) != cudaSuccess ||
-        cudaMalloc(&s->w3, kH * kH * sizeof(__nv_bfloat16)) != cudaSuccess) {
+        cudaMalloc(&s->w3, kH * kH * sizeof(__nv_bfloat16)) != cudaSuccess ||
+        cudaMalloc(&s->status, sizeof(int)) != cudaSuccess ||
+        cudaMemset(s->status, 0, sizeof(int)) != cudaSuccess) {
       rc = BBKDE_ALLOC_FAILED;
       break;
     }
@@ -204,7 +209,11 @@ int bbkde_surrogate_create(int device, uint64_t seed, bbkde_surrogate **out) {
         cudaFuncSetAttribute(k_mlp_infer<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)kInferSmem) != cudaSuccess ||
         cudaFuncSetAttribute(k_mlp_infer<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)kInferSmem) != cudaSuccess) {
+                             (int)kInferSmem) != cudaSuccess ||
+        cudaFuncSetAttribute(k_mlp_infer_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)TcSmem<false>::kBytes) != cudaSuccess ||
+        cudaFuncSetAttribute(k_mlp_infer_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)TcSmem<true>::kBytes) != cudaSuccess) {
       rc = BBKDE_CUDA_ERROR;
       break;
     }
@@ -235,7 +244,7 @@ int bbkde_surrogate_destroy(bbkde_surrogate *s) {
   for (void *p : {(void *)s->params, (void *)s->m, (void *)s->v, (void *)s->grad,
                   (void *)s->loss, (void *)s->w2, (void *)s->w3, (void *)s->grad_part,
                   (void *)s->loss_part, (void *)s->index, (void *)s->xy, (void *)s->target,
-                  (void *)s->pred})
+                  (void *)s->pred, (void *)s->status})
     if (p) cudaFree(p);
   if (s->stream) cudaStreamDestroy(s->stream);
   delete s;
@@ -417,14 +426,41 @@ int surrogate_infer(bbkde_surrogate *s, cudaStream_t st, int64_t n, const float2
   a.out = out;
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
-  const int64_t tiles = (n + 15) / 16;
-  const int64_t want = (tiles + kInferWarps - 1) / kInferWarps;
-  const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)sms * 8));
-  if (s->split)
-    k_mlp_infer<true><<<grid, kInferWarps * 32, kInferSmem, st>>>(a);
-  else
-    k_mlp_infer<false><<<grid, kInferWarps * 32, kInferSmem, st>>>(a);
+  if (s->engine == BBKDE_ENGINE_TCGEN05) {
+    // One CTA per SM, two 128-point tiles in flight per CTA.
+    const int64_t tiles = (n + kTcRows - 1) / kTcRows;
+    const int64_t want = (tiles + kTcWarpgroups - 1) / kTcWarpgroups;
+    const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(want, sms));
+    TcArgs ta;
+    ta.in = a;
+    ta.status = s->status;
+    if (s->split)
+      k_mlp_infer_tc<true><<<grid, kTcThreads, TcSmem<true>::kBytes, st>>>(ta);
+    else
+      k_mlp_infer_tc<false><<<grid, kTcThreads, TcSmem<false>::kBytes, st>>>(ta);
+  } else {
+    const int64_t tiles = (n + 15) / 16;
+    const int64_t want = (tiles + kInferWarps - 1) / kInferWarps;
+    const unsigned grid =
+        (unsigned)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)sms * 8));
+    if (s->split)
+      k_mlp_infer<true><<<grid, kInferWarps * 32, kInferSmem, st>>>(a);
+    else
+      k_mlp_infer<false><<<grid, kInferWarps * 32, kInferSmem, st>>>(a);
+  }
   S_CUDA(s, cudaGetLastError());
+  return BBKDE_OK;
+}
+
+// After the stream has been synchronised: BBKDE_TIMEOUT if an inference kernel
+// gave up waiting on the tensor cores (the flag is cleared).
+int surrogate_check(bbkde_surrogate *s) {
+  int flag = 0;
+  S_CUDA(s, cudaMemcpy(&flag, s->status, sizeof(int), cudaMemcpyDeviceToHost));
+  if (flag) {
+    cudaMemset(s->status, 0, sizeof(int));
+    return sfail(s, BBKDE_TIMEOUT, "surrogate inference: tensor-core wait expired");
+  }
   return BBKDE_OK;
 }
 
@@ -437,6 +473,13 @@ extern "C" {
 int bbkde_surrogate_set_inference(bbkde_surrogate *s, int split_activations) {
   if (!s || (split_activations != 0 && split_activations != 1)) return BBKDE_INVALID_ARGUMENT;
   s->split = split_activations;
+  return BBKDE_OK;
+}
+
+int bbkde_surrogate_set_engine(bbkde_surrogate *s, int engine) {
+  if (!s || (engine != BBKDE_ENGINE_TCGEN05 && engine != BBKDE_ENGINE_MMA_SYNC))
+    return BBKDE_INVALID_ARGUMENT;
+  s->engine = engine;
   return BBKDE_OK;
 }
 
@@ -474,6 +517,7 @@ int bbkde_surrogate_predict(bbkde_surrogate *s, int64_t n, const double *xy, dou
     rc = BBKDE_CUDA_ERROR;
   cudaFree(dxy);
   if (rc != BBKDE_OK) return sfail(s, rc, "surrogate_predict failed");
+  S_TRY(bbkde::surrogate_check(s));
   for (int64_t i = 0; i < n; ++i) out[i] = hp[i];
   return BBKDE_OK;
 }

@@ -262,6 +262,12 @@ BBKDE_API int bbkde_surrogate_predict_device(bbkde_surrogate *s, int64_t n, cons
  * tensor-core work. */
 BBKDE_API int bbkde_surrogate_set_inference(bbkde_surrogate *s, int split_activations);
 
+/* Inference kernel: BBKDE_ENGINE_TCGEN05 (default; tcgen05.mma with TMEM
+ * accumulators, 128-point tiles) or BBKDE_ENGINE_MMA_SYNC (mma.sync.m16n8k16,
+ * 16 points per warp). Same arithmetic; results agree to FP32 summation order. */
+enum { BBKDE_ENGINE_TCGEN05 = 0, BBKDE_ENGINE_MMA_SYNC = 1 };
+BBKDE_API int bbkde_surrogate_set_engine(bbkde_surrogate *s, int engine);
+
 /* Checkpoint: magic "BBKDEMLP", version, parameter count, normalisation, FP32
  * parameters (little-endian). */
 BBKDE_API int bbkde_surrogate_save(bbkde_surrogate *s, const char *path);

@@ -47,11 +47,14 @@ def silu_grad(z):
     return s * (1.0 + z * (1.0 - s))
 
 
-def forward(p, xin, emulate_bf16=False):
-    """xin: (n, 2) normalised inputs. Returns (y, cache)."""
+def forward(p, xin, emulate_bf16=False, bf16_weights=None):
+    """xin: (n, 2) normalised inputs. emulate_bf16 rounds the hidden weights and the
+    activations feeding the tensor-core layers to BF16; bf16_weights (default: the
+    same) rounds only the weights. Returns (y, cache)."""
     g = unpack(p)
     q = bf16 if emulate_bf16 else (lambda a: a)
-    W2, W3 = q(g["W2"]), q(g["W3"])
+    qw = bf16 if (emulate_bf16 if bf16_weights is None else bf16_weights) else (lambda a: a)
+    W2, W3 = qw(g["W2"]), qw(g["W3"])
     z1 = xin @ g["W1"].T + g["b1"]
     a1 = silu(z1)
     z2 = q(a1) @ W2.T + g["b2"]

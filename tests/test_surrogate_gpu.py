@@ -33,6 +33,31 @@ def test_forward_matches_fp64_with_bf16_rounding():
     np.testing.assert_allclose(got, want, rtol=0, atol=2e-3 * (np.abs(want).max() + 1))
 
 
+@pytest.mark.parametrize("split", [False, True])
+def test_tcgen05_inference_matches_mma_sync_and_fp64(split):
+    """The tcgen05 (TMEM) inference kernel against the mma.sync kernel and the
+    FP64 restatement. Tolerances: with BF16 activations a last-bit difference in
+    an FP32 accumulator can flip one BF16 rounding (2^-9 relative on one
+    activation), so the engines agree to 2e-3 of the output scale as the FP64
+    check does; with two-term activations (rounding ~2^-17) to 1e-4."""
+    s = bk.Surrogate(0, seed=5)
+    s.set_inference(split)
+    p, norm = s.params()
+    rng = W.SplitMix64(15)
+    xy = rng.uniform(2 * 5003, -4, 4).reshape(-1, 2)      # ragged: 39 tiles + 11 points
+    s.set_engine(bk.ENGINE_TCGEN05)
+    tc = s.predict(xy)
+    s.set_engine(bk.ENGINE_MMA_SYNC)
+    ms = s.predict(xy)
+    scale = np.abs(ms).max() + 1
+    tol = 1e-4 if split else 2e-3
+    np.testing.assert_allclose(tc, ms, rtol=0, atol=tol * scale)
+    y, _ = mlp_ref.forward(p.astype(np.float64), _norm_inputs(xy, norm), emulate_bf16=not split,
+                           bf16_weights=True)
+    want = norm[4] + norm[5] * y
+    np.testing.assert_allclose(tc, want, rtol=0, atol=2e-3 * scale)
+
+
 def test_gradient_matches_fp64_backprop():
     s = bk.Surrogate(0, seed=11)
     p, norm = s.params()
