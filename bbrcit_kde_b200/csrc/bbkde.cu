@@ -354,9 +354,12 @@ struct Variant {
   int qpt;     // queries per thread
   int block;   // threads per block
   int minb;    // __launch_bounds__ minimum resident blocks per SM
+  int poly;    // every poly-th reference's exponentials on the FP32 pipe (0: none)
 };
-constexpr Variant kVariants[] = {{8, 256, 2}, {4, 256, 3}, {8, 128, 4}, {4, 128, 6}};
-constexpr int kNumVariants = 4;
+constexpr Variant kVariants[] = {{8, 256, 2, 0}, {4, 256, 3, 0}, {8, 128, 4, 0},
+                                 {4, 128, 6, 0}, {8, 256, 2, 8}, {8, 128, 4, 8},
+                                 {8, 128, 4, 4}};
+constexpr int kNumVariants = 7;
 constexpr int kDefaultVariant = 0;
 constexpr int kTile = 256;
 constexpr int kBlock64 = 128;
@@ -391,10 +394,10 @@ Plan plan_launch(const bbkde_ctx *c, int64_t n_ref, int64_t q_count, int q_per_b
   return p;
 }
 
-template <int OP, int D, int QPT, int BLOCK, int MINB>
+template <int OP, int D, int QPT, int BLOCK, int MINB, int POLY = 0>
 void launch_shape(dim3 grid, cudaStream_t st, const SumArgs &a) {
   if constexpr (op_packed(OP))
-    k_pair_sum_f32x2<OP, D, QPT, BLOCK, kTile, MINB><<<grid, BLOCK, 0, st>>>(a);
+    k_pair_sum_f32x2<OP, D, QPT, BLOCK, kTile, MINB, POLY><<<grid, BLOCK, 0, st>>>(a);
   else
     k_pair_sum_f32<OP, D, QPT, BLOCK, kTile, MINB><<<grid, BLOCK, 0, st>>>(a);
 }
@@ -405,7 +408,10 @@ void launch_f32(int variant, dim3 grid, cudaStream_t st, const SumArgs &a) {
     case 0: launch_shape<OP, D, 8, 256, 2>(grid, st, a); break;
     case 1: launch_shape<OP, D, 4, 256, 3>(grid, st, a); break;
     case 2: launch_shape<OP, D, 8, 128, 4>(grid, st, a); break;
-    default: launch_shape<OP, D, 4, 128, 6>(grid, st, a); break;
+    case 3: launch_shape<OP, D, 4, 128, 6>(grid, st, a); break;
+    case 4: launch_shape<OP, D, 8, 256, 2, 8>(grid, st, a); break;
+    case 5: launch_shape<OP, D, 8, 128, 4, 8>(grid, st, a); break;
+    default: launch_shape<OP, D, 8, 128, 4, 4>(grid, st, a); break;
   }
 }
 template <int OP, int D>

@@ -269,7 +269,31 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_pair_sum_f32(SumArgs a) {
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
 
-template <int OP, int D>
+// 2^x on the FP32 pipe for two lanes, x <= 0 -- the alternative to MUFU.EX2 that
+// lets the pair sum spread its exponentials over two pipes. Range reduction by the
+// 1.5 * 2^23 shift (t = x + 1.5 * 2^23 holds n = round(x) in its low mantissa bits,
+// f = x - n in [-1/2, 1/2] exactly), 2^f by a degree-5 polynomial (coefficients
+// fitted for minimum relative error on [-1/2, 1/2] by Lawson's iteratively
+// reweighted least squares: 7.5e-8 in exact arithmetic, 2.1e-7 evaluated with FP32
+// FMAs), 2^n added into the exponent field (the 0x4B400000 of t shifts out of a
+// 32-bit word, leaving n << 23). x is clamped at -125 so the result is a normal
+// number: a pair that MUFU.EX2 flushes to zero contributes at most 2^-125 * mass.
+__device__ __forceinline__ float2 exp2_poly2(float2 x) {
+  x.x = fmaxf(x.x, -125.0f);
+  x.y = fmaxf(x.y, -125.0f);
+  const float2 t = __fadd2_rn(x, f2(12582912.0f));
+  const float2 n = __fadd2_rn(t, f2(-12582912.0f));
+  const float2 f = __ffma2_rn(n, f2(-1.0f), x);
+  float2 p = __ffma2_rn(f2(1.327644451521337e-3f), f, f2(9.67553723603487e-3f));
+  p = __ffma2_rn(p, f, f2(5.550713464617729e-2f));
+  p = __ffma2_rn(p, f, f2(2.4022120237350464e-1f));
+  p = __ffma2_rn(p, f, f2(6.931469440460205e-1f));
+  p = __ffma2_rn(p, f, f2(1.0000001192092896f));
+  return make_float2(__uint_as_float(__float_as_uint(p.x) + (__float_as_uint(t.x) << 23)),
+                     __uint_as_float(__float_as_uint(p.y) + (__float_as_uint(t.y) << 23)));
+}
+
+template <int OP, int D, bool POLY = false>
 __device__ __forceinline__ float2 pair_u2(const float2 qx, const float2 qy, const float4 &r0,
                                           const float4 &r1, const float4 &r2) {
   const float2 nrx = make_float2(r0.x, r0.y);
@@ -281,11 +305,11 @@ __device__ __forceinline__ float2 pair_u2(const float2 qx, const float2 qy, cons
     if (OP == OP_GAUSS_ISO) {
       float2 d2 = __ffma2_rn(dy, dy, __fmul2_rn(dx, dx));
       float2 e = __fmul2_rn(d2, s);
-      return make_float2(ex2_approx(e.x), ex2_approx(e.y));
+      return POLY ? exp2_poly2(e) : make_float2(ex2_approx(e.x), ex2_approx(e.y));
     } else if (OP == OP_GAUSS_PROD) {
       const float2 sy = make_float2(r2.x, r2.y);
       float2 e = __ffma2_rn(__fmul2_rn(dy, dy), sy, __fmul2_rn(__fmul2_rn(dx, dx), s));
-      return make_float2(ex2_approx(e.x), ex2_approx(e.y));
+      return POLY ? exp2_poly2(e) : make_float2(ex2_approx(e.x), ex2_approx(e.y));
     } else if (OP == OP_EPAN_ISO) {
       float2 d2 = __ffma2_rn(dy, dy, __fmul2_rn(dx, dx));
       float2 u = __ffma2_rn(d2, s, f2(1.0f));
@@ -300,7 +324,7 @@ __device__ __forceinline__ float2 pair_u2(const float2 qx, const float2 qy, cons
   } else {
     if (OP == OP_GAUSS_ISO || OP == OP_GAUSS_PROD) {
       float2 e = __fmul2_rn(__fmul2_rn(dx, dx), s);
-      return make_float2(ex2_approx(e.x), ex2_approx(e.y));
+      return POLY ? exp2_poly2(e) : make_float2(ex2_approx(e.x), ex2_approx(e.y));
     } else {
       float2 u = __ffma2_rn(__fmul2_rn(dx, dx), s, f2(1.0f));
       return make_float2(fmaxf(u.x, 0.0f), fmaxf(u.y, 0.0f));
@@ -312,9 +336,28 @@ __host__ __device__ constexpr bool op_packed(int op) {
   return op == OP_GAUSS_ISO || op == OP_GAUSS_PROD || op == OP_EPAN_ISO || op == OP_EPAN_PROD;
 }
 
-template <int OP, int D, int QPT, int BLOCK, int TILE, int MINB>
+// One reference (shared-memory record j) against this thread's query pairs.
+template <int OP, int D, int NP, bool POLY, bool EXT>
+__device__ __forceinline__ void ref_pairs(const float4 *s_r0, const float4 *s_r1,
+                                          const float4 *s_r2, int j, const float2 (&qx)[NP],
+                                          const float2 (&qy)[NP], float2 (&acc)[NP]) {
+  const float4 r0 = s_r0[j];
+  const float4 r1 = s_r1[j];
+  const float4 r2 = EXT ? s_r2[j] : r1;
+  const float2 m = make_float2(r1.x, r1.y);
+#pragma unroll
+  for (int p = 0; p < NP; ++p)
+    acc[p] = __ffma2_rn(m, pair_u2<OP, D, POLY>(qx[p], qy[p], r0, r1, r2), acc[p]);
+}
+
+// POLY_EVERY > 0: for the Gaussians, every POLY_EVERY-th reference of a chunk takes
+// its exponentials from exp2_poly2 (FP32 pipe) instead of MUFU.EX2, so that both
+// pipes share the work (1 in 8 balances them: the MUFU bound alone is 16 pairs
+// per clock per SM, the joint bound ~18.3).
+template <int OP, int D, int QPT, int BLOCK, int TILE, int MINB, int POLY_EVERY = 0>
 __global__ void __launch_bounds__(BLOCK, MINB) k_pair_sum_f32x2(SumArgs a) {
   static_assert(QPT % 2 == 0, "queries are processed in pairs");
+  static_assert(POLY_EVERY == 0 || kChunk % POLY_EVERY == 0, "poly stride divides a chunk");
   static_assert(TILE % kChunk == 0 && TILE % BLOCK == 0, "tile shape");
   constexpr int NP = QPT / 2;
   constexpr bool kExt = op_has_extra(OP) && D == 2;
@@ -374,15 +417,19 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_pair_sum_f32x2(SumArgs a) {
 #pragma unroll
       for (int p = 0; p < NP; ++p) acc[p] = f2(0.0f);
       if (!diag) {
+        if constexpr (POLY_EVERY == 0 || !(OP == OP_GAUSS_ISO || OP == OP_GAUSS_PROD)) {
 #pragma unroll 4
-        for (int j = 0; j < kChunk; ++j) {
-          const float4 r0 = s_r0[j0 + j];
-          const float4 r1 = s_r1[j0 + j];
-          const float4 r2 = kExt ? s_r2[j0 + j] : r1;
-          const float2 m = make_float2(r1.x, r1.y);
+          for (int j = 0; j < kChunk; ++j)
+            ref_pairs<OP, D, NP, false, kExt>(s_r0, s_r1, s_r2, j0 + j, qx, qy, acc);
+        } else {
+#pragma unroll 1
+          for (int j = 0; j < kChunk; j += POLY_EVERY) {
 #pragma unroll
-          for (int p = 0; p < NP; ++p)
-            acc[p] = __ffma2_rn(m, pair_u2<OP, D>(qx[p], qy[p], r0, r1, r2), acc[p]);
+            for (int jj = 0; jj < POLY_EVERY - 1; ++jj)
+              ref_pairs<OP, D, NP, false, kExt>(s_r0, s_r1, s_r2, j0 + j + jj, qx, qy, acc);
+            ref_pairs<OP, D, NP, true, kExt>(s_r0, s_r1, s_r2, j0 + j + POLY_EVERY - 1, qx, qy,
+                                             acc);
+          }
         }
       } else {
         // Diagonal tile of a self-evaluation: zero the mass of the pair r == q.

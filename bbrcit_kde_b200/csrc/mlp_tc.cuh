@@ -162,7 +162,7 @@ struct TcArgs {
 template <bool kSplit>
 __global__ void __launch_bounds__(kTcThreads, 1) k_mlp_infer_tc(TcArgs ta) {
   using L = TcSmem<kSplit>;
-  extern __shared__ __align__(1024) unsigned char smem[];
+  extern __shared__ __align__(16) unsigned char smem[];   // 16 B: no-swizzle operands
   const InferArgs &a = ta.in;
   unsigned char *W2 = smem + L::kW, *W3 = W2 + kTcMatBytes;
   float *fp = reinterpret_cast<float *>(smem + L::kF);

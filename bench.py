@@ -42,10 +42,28 @@ METRIC = ("2D KDE queries/s (kernel evals/s vs FP32 roofline), direct vs surroga
           "stated rel err")
 UNIT = "kernel evals/s"
 MUFU_EX2_PER_CLK_PER_SM = 16
-# DRAM bytes per launch of the pair-sum kernel on this workload, from one ncu
-# capture (dram__bytes_read.sum + dram__bytes_write.sum), scaled to a full launch:
-# profiles/pair_sum_f32_gaussiso_1M.md. None until measured.
-TRAFFIC_BYTES_PER_LAUNCH = None
+# FP32-pipe poly stride of each pair-sum launch shape (bbkde_launch_variants order):
+# every k-th reference's exponentials on the FP32 pipe, 0 = all on MUFU.
+VARIANT_POLY = [0, 0, 0, 0, 8, 8, 4]
+
+
+def pair_sum_bound_per_clk_per_sm(poly: int, fma_cycles: float = 12.0) -> tuple[float, str]:
+    """Pairs per clock per SM the packed Gaussian pair sum can reach. Per warp and
+    per 64 pairs (two queries per packed instruction) the main path issues
+    fma_cycles / 2 packed FP32 instructions (2 FMA-pipe cycles each: 12 cycles for
+    the 2-D isotropic kernel, 8 in 1-D) and 2 MUFU.EX2 (8 cycles each on a
+    4-lane-per-clock unit: 16 cycles); the polynomial exp2 costs 8 packed
+    instructions (16 cycles) instead of the 2 MUFU operations. 4 SMSPs per SM."""
+    mufu = 4 * 64 / (16.0 * (1 - 1 / poly)) if poly else 4 * 64 / 16.0
+    fma = 4 * 64 / (fma_cycles + (16.0 / poly if poly else 0.0))
+    bound = "sfu" if mufu <= fma else "fma"
+    if poly:
+        bound = "sfu+fma (exp2 split: MUFU and FP32 polynomial)"
+    return min(mufu, fma), bound
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per full-size launch of
+# the pair-sum kernel on this workload, from one ncu capture of the pilot and the
+# evaluation launch (57.40 MB and 55.27 MB): profiles/pair_sum_f32x2_adaptive_gaussprod2d_1M.md.
+TRAFFIC_BYTES_PER_LAUNCH = 56_335_000
 
 
 def parse():
@@ -343,16 +361,22 @@ def main():
     kernel_ms = float(np.mean([ms for ms, _, _ in kernel_launches]))
     peaks = measured_peaks()
     sm_max = float(peaks.get("sm_max_mhz") or clocks.get("sm_max_mhz") or 1965.0)
-    peak = sm_count * MUFU_EX2_PER_CLK_PER_SM * sm_max * 1e6
+    _, variant = ctx.launch_variants()
+    poly = VARIANT_POLY[variant] if 0 <= variant < len(VARIANT_POLY) else 0
+    per_clk, bound = pair_sum_bound_per_clk_per_sm(poly)
+    peak = sm_count * per_clk * sm_max * 1e6
+    mufu_peak = sm_count * MUFU_EX2_PER_CLK_PER_SM * sm_max * 1e6
     observed = clocks.get("sm_mhz")
     roofline = {
-        "bound": "sfu", "achieved": achieved / 1e9, "peak": peak / 1e9, "unit": "Geval/s",
+        "bound": bound, "achieved": achieved / 1e9, "peak": peak / 1e9, "unit": "Geval/s",
         "frac": achieved / peak,
-        "peak_basis": f"{sm_count} SMs x {MUFU_EX2_PER_CLK_PER_SM} MUFU ex2/clk x "
-                      f"{sm_max:.0f} MHz (sm_max_mhz, MEASURED_PEAKS.json); one ex2 per "
-                      f"pair evaluation",
-        "frac_at_observed_clock": (achieved / (sm_count * MUFU_EX2_PER_CLK_PER_SM * observed
-                                               * 1e6)) if observed else None,
+        "peak_basis": f"{sm_count} SMs x {per_clk:.2f} pairs/clk x {sm_max:.0f} MHz "
+                      f"(sm_max_mhz, MEASURED_PEAKS.json); launch shape {variant} "
+                      f"(FP32-pipe exp2 every {poly or 'no'} reference); MUFU alone: "
+                      f"16 ex2/clk/SM",
+        "frac_of_mufu_only_bound": achieved / mufu_peak,
+        "frac_at_observed_clock": (achieved / (sm_count * per_clk * observed * 1e6))
+        if observed else None,
         "kernel_ms_per_launch": kernel_ms,
         "pairs_per_launch": float(kernel_launches[0][1]),
         "traffic": TRAFFIC_BYTES_PER_LAUNCH,
@@ -868,19 +892,25 @@ def run_direct1d(a, world, rank, local):
     pairs = float(n) * m
     # error vs FP64 on 4096 queries
     q0 = m // 2
+    _, variant = ctx.launch_variants()
     f32 = ctx.eval_range(desc, 0, n - 1, q0, q0 + 4095)
     f64 = ctx.eval_range(desc, 0, n - 1, q0, q0 + 4095, True, bk.FP64)
     ctx.close()
     peaks = measured_peaks()
     sm_max = float(peaks.get("sm_max_mhz") or clocks.get("sm_max_mhz") or 1965.0)
-    peak = sm_count * MUFU_EX2_PER_CLK_PER_SM * sm_max * 1e6
+    poly = VARIANT_POLY[variant] if 0 <= variant < len(VARIANT_POLY) else 0
+    per_clk, bound = pair_sum_bound_per_clk_per_sm(poly, fma_cycles=8.0)
+    peak = sm_count * per_clk * sm_max * 1e6
     kms = float(np.mean(kernel_ms[-a.steps:]))
     _line(a, world, UNIT, pairs * world / (np.mean(ms) / 1e3), ms,
           {"workload": f"1-D Gaussian, h=0.02, {n} refs (5-component mixture), {m} uniform "
                        f"queries on [-6,6] per rank", "l2": "flushed between timed steps"},
           "f32", clocks=clocks,
-          roofline={"bound": "sfu", "achieved": pairs / (kms / 1e3) / 1e9, "peak": peak / 1e9,
-                    "unit": "Geval/s", "frac": pairs / (kms / 1e3) / peak, "traffic": None},
+          roofline={"bound": bound, "achieved": pairs / (kms / 1e3) / 1e9, "peak": peak / 1e9,
+                    "unit": "Geval/s", "frac": pairs / (kms / 1e3) / peak, "traffic": None,
+                    "launch_shape": variant,
+                    "frac_of_mufu_only_bound": pairs / (kms / 1e3) /
+                    (sm_count * MUFU_EX2_PER_CLK_PER_SM * sm_max * 1e6)},
           error_vs_fp64=error_stats(f32, f64))
     return 0
 

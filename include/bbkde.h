@@ -368,7 +368,9 @@ BBKDE_API int bbkde_last_launch_stats(const bbkde_ctx *ctx, double *kernel_ms, d
 BBKDE_API int64_t bbkde_launch_count(const bbkde_ctx *ctx);
 
 /* Launch shapes of the FP32 pair-sum kernels (queries per thread x threads per
- * block). By default (variant -1) the context autotunes: for problems of at least
+ * block, and for the Gaussians whether every 8th or 4th reference's exponentials
+ * run on the FP32 pipe instead of MUFU.EX2). By default (variant -1) the context
+ * autotunes: for problems of at least
  * 2e10 pairs it times every shape on a slice of the problem once per problem
  * class (kernel, dimension, self-evaluation, log2 sizes) and keeps the fastest.
  * A variant in [0, n_variants) forces that shape. No reference counterpart: the
