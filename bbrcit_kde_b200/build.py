@@ -68,6 +68,26 @@ def build(force: bool = False, ptxas_info: bool = False, verbose: bool = False) 
     return LIB
 
 
+GRID_SEARCH_SRC = os.path.join(PKG, "grid_search", "grid_search.cc")
+GRID_SEARCH = os.path.join(LIBDIR, "grid_search")
+
+
+def build_grid_search(force: bool = False) -> str:
+    """The grid_search command-line driver: plain g++ over the C ABI, rpath to lib/."""
+    lib = build()
+    if (not force and os.path.exists(GRID_SEARCH) and
+            os.path.getmtime(GRID_SEARCH) >= max(os.path.getmtime(GRID_SEARCH_SRC),
+                                                 os.path.getmtime(lib))):
+        return GRID_SEARCH
+    cxx = shutil.which("g++") or "g++"
+    tmp = GRID_SEARCH + ".tmp"
+    subprocess.check_call([cxx, "-std=c++11", "-O2", "-Wall", "-Wextra", "-Werror",
+                           GRID_SEARCH_SRC, "-o", tmp, "-L", LIBDIR, "-lbbkde",
+                           "-Wl,-rpath,$ORIGIN"])
+    os.replace(tmp, GRID_SEARCH)
+    return GRID_SEARCH
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--force", action="store_true")
@@ -75,6 +95,7 @@ def main(argv=None) -> int:
     ap.add_argument("-v", "--verbose", action="store_true")
     a = ap.parse_args(argv)
     print(build(force=a.force, ptxas_info=a.ptxas_info, verbose=a.verbose))
+    print(build_grid_search(force=a.force))
     return 0
 
 

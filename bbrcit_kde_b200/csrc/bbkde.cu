@@ -1587,6 +1587,9 @@ extern "C" int bbkde_eval_grid(bbkde_ctx *c, bbkde_surrogate *sur, const bbkde_k
   if (T != 16 && T != 32) return fail(c, BBKDE_INVALID_ARGUMENT, "grid: tile must be 16 or 32");
   if (P != 1 && P != 5 && P != 9)
     return fail(c, BBKDE_INVALID_ARGUMENT, "grid: probes must be 1, 5 or 9");
+  const int interp = cfg->interp == 0 ? 1 : cfg->interp;
+  if (interp != 1 && interp != 3)
+    return fail(c, BBKDE_INVALID_ARGUMENT, "grid: interp must be 1 (bilinear) or 3 (bicubic)");
   if (!(cfg->rel_tol > 0) || !(cfg->low_frac >= 0 && cfg->low_frac < 1) ||
       !(cfg->cull_rel > 0 && cfg->cull_rel < 1))
     return fail(c, BBKDE_INVALID_ARGUMENT,
@@ -1689,7 +1692,8 @@ extern "C" int bbkde_eval_grid(bbkde_ctx *c, bbkde_surrogate *sur, const bbkde_k
       COUNT_LAUNCH(c);
       resid = c->gr_resid.as<float>();
     }
-    k_tile_reduce<<<(unsigned)ntiles, 256, 0, c->stream>>>(g, pred, resid, c->gr_tmin.as<float>(),
+    k_tile_reduce<<<(unsigned)ntiles, 256, 0, c->stream>>>(g, pred, resid, interp,
+                                                         c->gr_tmin.as<float>(),
                                                          c->gr_tmax.as<float>(),
                                                          c->gr_bad.as<int>());
     COUNT_LAUNCH(c);
@@ -1820,7 +1824,7 @@ extern "C" int bbkde_lsq_numint_cv(bbkde_ctx *c, const bbkde_kernel_desc *k,
   // Square integral over the grid (:62-93).
   const int64_t npts = grid->nx * grid->ny;
   TRY(ensure(c, c->gr_out, (size_t)npts * sizeof(double)));
-  bbkde_grid_config cfg = {BBKDE_GRID_EXACT, 16, 1, 1, 1e-3, 0.0, 1e-7};
+  bbkde_grid_config cfg = {BBKDE_GRID_EXACT, 16, 1, 1, 1e-3, 0.0, 1e-7, 1};
   bbkde_grid_stats st;
   TRY(bbkde_eval_grid(c, nullptr, k, grid, &cfg, c->gr_out.as<double>(), &st));
   const unsigned nb = std::min<unsigned>(grid1d(npts, kRedBlock), 4096u);

@@ -357,7 +357,7 @@ __device__ __forceinline__ void ref_pairs(const float4 *s_r0, const float4 *s_r1
 template <int OP, int D, int QPT, int BLOCK, int TILE, int MINB, int POLY_EVERY = 0>
 __global__ void __launch_bounds__(BLOCK, MINB) k_pair_sum_f32x2(SumArgs a) {
   static_assert(QPT % 2 == 0, "queries are processed in pairs");
-  static_assert(POLY_EVERY == 0 || kChunk % POLY_EVERY == 0, "poly stride divides a chunk");
+  static_assert(kChunk % (POLY_EVERY > 0 ? POLY_EVERY : 1) == 0, "poly stride divides a chunk");
   static_assert(TILE % kChunk == 0 && TILE % BLOCK == 0, "tile shape");
   constexpr int NP = QPT / 2;
   constexpr bool kExt = op_has_extra(OP) && D == 2;

@@ -50,22 +50,39 @@ __global__ void k_anchor_residual(const double *exact, const float *net, int64_t
   resid[i] = ok ? (float)(log(f) - (net ? (double)net[i] : 0.0)) : NAN;
 }
 
-// One block per tile: pred += bilinear residual (anchored mode), tile min / max
-// of pred, bad flag for non-finite values.
-__global__ void k_tile_reduce(GridDesc g, float *pred, const float *resid, float *tmin,
-                              float *tmax, int *bad) {
+// Catmull-Rom weights of the four samples at -1, 0, 1, 2 for a point at t in [0, 1].
+__device__ __forceinline__ void cr_weights(float t, float (&w)[4]) {
+  const float t2 = t * t, t3 = t2 * t;
+  w[0] = 0.5f * (-t3 + 2.f * t2 - t);
+  w[1] = 0.5f * (3.f * t3 - 5.f * t2 + 2.f);
+  w[2] = 0.5f * (-3.f * t3 + 4.f * t2 + t);
+  w[3] = 0.5f * (t3 - t2);
+}
+
+// One block per tile: pred += interpolated residual (anchored mode: bilinear
+// between the tile's 4 corner anchors, or bicubic Catmull-Rom over the 4 x 4
+// anchors around the tile, clamped at the grid's edge), tile min / max of pred,
+// bad flag for non-finite values (a NaN anchor makes its tiles exact).
+__global__ void k_tile_reduce(GridDesc g, float *pred, const float *resid, int interp,
+                              float *tmin, float *tmax, int *bad) {
   __shared__ float s_mn[32], s_mx[32];
   __shared__ int s_bad[32];
+  __shared__ float s_r[4][4];
   const int t = blockIdx.x;
   const int tx = t % g.ntx, ty = t / g.ntx;
-  float r00 = 0.f, r10 = 0.f, r01 = 0.f, r11 = 0.f;
-  if (resid) {
-    const int64_t aw = g.ntx + 1;
-    r00 = resid[(int64_t)ty * aw + tx];
-    r10 = resid[(int64_t)ty * aw + tx + 1];
-    r01 = resid[(int64_t)(ty + 1) * aw + tx];
-    r11 = resid[(int64_t)(ty + 1) * aw + tx + 1];
+  if (resid && threadIdx.x < 16) {
+    const int a = threadIdx.x & 3, c = threadIdx.x >> 2;
+    int ax, ay;
+    if (interp == 3) {
+      ax = min(max(tx - 1 + a, 0), g.ntx);
+      ay = min(max(ty - 1 + c, 0), g.nty);
+    } else {   // bilinear: the corners at slots 1 and 2
+      ax = tx + (a >= 2 ? 1 : 0);
+      ay = ty + (c >= 2 ? 1 : 0);
+    }
+    s_r[c][a] = resid[(int64_t)ay * (g.ntx + 1) + ax];
   }
+  __syncthreads();
   float mn = INFINITY, mx = -INFINITY;
   int b = 0;
   const int T = g.tile;
@@ -77,7 +94,20 @@ __global__ void k_tile_reduce(GridDesc g, float *pred, const float *resid, float
     float v = pred[p];
     if (resid) {
       const float u = (li + 0.5f) / T, w = (lj + 0.5f) / T;
-      v += (1.f - w) * ((1.f - u) * r00 + u * r10) + w * ((1.f - u) * r01 + u * r11);
+      if (interp == 3) {
+        float wu[4], wv[4];
+        cr_weights(u, wu);
+        cr_weights(w, wv);
+        float acc = 0.f;
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+          acc += wv[c] * (wu[0] * s_r[c][0] + wu[1] * s_r[c][1] + wu[2] * s_r[c][2] +
+                          wu[3] * s_r[c][3]);
+        v += acc;
+      } else {
+        v += (1.f - w) * ((1.f - u) * s_r[1][1] + u * s_r[1][2]) +
+             w * ((1.f - u) * s_r[2][1] + u * s_r[2][2]);
+      }
       pred[p] = v;
     }
     if (!(v > -INFINITY && v < INFINITY)) b = 1;   // also catches NaN

@@ -483,7 +483,7 @@ def run_surrogate_grid(a, world, rank, local):
     """4,000,000 references from the seeded 8-component mixture, adaptive Gaussian
     KDE (pilot h = 0.05, alpha = 0.5), density on an 8192 x 8192 grid over
     [-4, 4]^2. One step = bbkde_eval_grid in anchored mode with the trained network
-    (two-term BF16 inference): network value + bilinear residual measured exactly
+    (two-term BF16 inference): network value + bicubic residual measured exactly
     at the tile corners, 5 exact held-out probes per 16 x 16 tile (tolerance
     5e-4), exact culled fallback on flagged tiles and tiles below 1e-4 of the
     maximum. Comparators (timed once each): the plain direct sum over all grid
@@ -539,7 +539,7 @@ def run_surrogate_grid(a, world, rank, local):
     out = torch.empty(npts, dtype=torch.float64, device="cuda")
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     main_cfg = dict(surrogate=sur, mode=bk.GRID_ANCHORED, tile=16, probes=5, rel_tol=5e-4,
-                    low_frac=1e-4)
+                    low_frac=1e-4, interp=3)
 
     def grid_step(dst, **kw):
         return ctx.eval_grid(desc, grid, dst.data_ptr(), **kw)
@@ -570,16 +570,19 @@ def run_surrogate_grid(a, world, rank, local):
     # Comparators, each once.
     comp = {}
     for name, kw in [("culled_exact", dict(mode=bk.GRID_EXACT, tile=16)),
-                     ("anchored_without_network", dict(surrogate=None, mode=bk.GRID_ANCHORED,
-                                                       tile=16, probes=5, rel_tol=5e-4,
-                                                       low_frac=1e-4)),
-                     ("network_tile32", dict(main_cfg, tile=32)),
-                     ("anchored_without_network_tile32",
-                      dict(surrogate=None, mode=bk.GRID_ANCHORED, tile=32, probes=5,
-                           rel_tol=5e-4, low_frac=1e-4)),
+                     ("anchored_without_network", dict(main_cfg, surrogate=None)),
+                     ("network_bilinear", dict(main_cfg, interp=1)),
+                     ("anchored_without_network_bilinear",
+                      dict(main_cfg, surrogate=None, interp=1)),
+                     ("network_bilinear_tile32", dict(main_cfg, tile=32, interp=1)),
+                     ("anchored_without_network_bilinear_tile32",
+                      dict(main_cfg, surrogate=None, tile=32, interp=1)),
                      ("network_only_probes", dict(surrogate=sur, mode=bk.GRID_SURROGATE,
                                                   tile=16, probes=5, rel_tol=5e-4,
-                                                  low_frac=1e-4))]:
+                                                  low_frac=1e-4)),
+                     ("network_tile32", dict(main_cfg, tile=32)),
+                     ("anchored_without_network_tile32",
+                      dict(main_cfg, surrogate=None, tile=32))]:
         l2_flush(torch, flush)
         torch.cuda.synchronize()
         dst = torch.empty(npts, dtype=torch.float64, device="cuda")
@@ -689,8 +692,9 @@ def run_surrogate_grid(a, world, rank, local):
         "data": "synthetic (seeded splitmix64 8-component mixture, float32-representable)",
         "config": {"workload": f"surrogate grid: adaptive Gaussian KDE of {n} refs (pilot "
                                f"h=0.05, alpha=0.5) on a {G}x{G} grid over [-4,4]^2",
-                   "pipeline": "bbkde_eval_grid anchored mode, tile 16, 5 probes, probe "
-                               "tolerance 5e-4, low_frac 1e-4, two-term BF16 inference",
+                   "pipeline": "bbkde_eval_grid anchored mode, bicubic residual, tile 16, "
+                               "5 probes, probe tolerance 5e-4, low_frac 1e-4, two-term BF16 "
+                               "inference on tcgen05",
                    "l2": "flushed between timed steps (256 MB write)"},
         "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
         "gpu_launches": int(launches), "step_stats": stats[-1], "comparators": results,

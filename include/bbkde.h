@@ -323,6 +323,9 @@ typedef struct {
   double low_frac;   /* tiles whose smallest predicted density is below low_frac
                         times the grid's largest go exact */
   double cull_rel;   /* bound of the culled sum (e.g. 1e-7) */
+  int interp;        /* anchored mode: residual between the anchors, 1 = bilinear over
+                        the tile's corners, 3 = bicubic (Catmull-Rom) over the 4 x 4
+                        anchors around the tile; 0 = 1 */
 } bbkde_grid_config;
 
 typedef struct {

@@ -237,6 +237,13 @@ def test_grid_anchored_without_network(ctx):
     assert st.exact_points < 0.5 * FINE[0] * FINE[1]
     # probes at the centre and edge midpoints hold the whole grid near rel_tol
     assert err.max() <= 1e-3, (err.max(), np.mean(err > 5e-4))
+    # bicubic interpolation of the residual over the 4 x 4 anchors: same guarantees
+    got3, st3 = _grid_eval(ctx, desc, FINE, mode=bk.GRID_ANCHORED, tile=16, probes=5,
+                           rel_tol=5e-4, low_frac=1e-4, interp=3)
+    err3 = _check_tiles(st3, got3, want, FINE, 16, 5e-4)
+    assert err3.max() <= 1e-3 and st3.tiles_surrogate > st.tiles // 2, st3.as_dict()
+    with pytest.raises(bk.InvalidArgument):
+        _grid_eval(ctx, desc, FINE, mode=bk.GRID_ANCHORED, interp=2)
     # the low-density rule: tiles below half the maximum go exact
     got, st = _grid_eval(ctx, desc, FINE, mode=bk.GRID_ANCHORED, tile=16, probes=1,
                          rel_tol=5e-4, low_frac=0.5)
@@ -266,3 +273,12 @@ def test_grid_surrogate_modes_and_network_gain(ctx):
     net, zero = res["net32"], res["zero32"]
     assert net.tiles_surrogate > zero.tiles_surrogate, (net.as_dict(), zero.as_dict())
     assert net.exact_points < zero.exact_points
+    # the same with the bicubic residual interpolation (the pipeline's default)
+    sts = {}
+    for name, sur in [("net", s), ("zero", None)]:
+        got, sts[name] = _grid_eval(ctx, desc, FINE, surrogate=sur, mode=bk.GRID_ANCHORED,
+                                    tile=16, probes=5, rel_tol=5e-4, low_frac=1e-4, interp=3)
+        err = _check_tiles(sts[name], got, want, FINE, 16, 5e-4)
+        assert err.max() <= 1e-3, (name, err.max())
+    assert sts["net"].exact_points <= sts["zero"].exact_points, \
+        (sts["net"].as_dict(), sts["zero"].as_dict())
