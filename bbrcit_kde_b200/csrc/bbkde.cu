@@ -28,6 +28,7 @@
 #include "kde_device.cuh"
 #include "kde_cv_batch.cuh"
 #include "kde_culled.cuh"
+#include "kde_culled_sep.cuh"
 #include "kde_grid.cuh"
 
 using namespace bbkde;
@@ -78,8 +79,9 @@ struct PackCache {
 // valid for the packed records with the same key.
 struct CullCache {
   PackKey key;
-  DevBuf rec, ext, tiles;
+  DevBuf rec, ext, tiles, groups;
   int n_tiles = 0;
+  int n_groups = 0;
 };
 
 struct QueryCache {
@@ -120,8 +122,8 @@ struct bbkde_ctx {
   DevBuf ms_keys, ms_keys2, ms_perm, ms_perm2, ms_box, ms_tmp, cq_x, cq_y, cq_out, cb_bound,
       cb_smin, cb_tiles, cb_stats;
   DevBuf gr_pred, gr_order, gr_tmin, gr_tmax, gr_bad, gr_terr, gr_flag, gr_flag_ord, gr_list,
-      gr_nsel, gr_counts, gr_gmax, gr_anc_order, gr_anc_exact, gr_anc_net, gr_resid, gr_pq_x,
-      gr_pq_y, gr_pq_idx, gr_pq_exact, gr_out;
+      gr_nsel, gr_counts, gr_gmax, gr_lat_order, gr_lat_exact, gr_lat_net, gr_q_order, gr_q_exact,
+      gr_q_net, gr_resid, gr_out;
   cudaEvent_t ev3 = nullptr;
   std::string err;
 };
@@ -717,14 +719,14 @@ int bbkde_ctx_destroy(bbkde_ctx *c) {
                     &c->cv_counter, &c->cv_h, &c->cv_lut, &c->cv_part, &c->cv_hist,
                     &c->cv_out, &c->cv_parts})
     release(*b);
-  for (DevBuf *b : {&c->cull.rec, &c->cull.ext, &c->cull.tiles, &c->ms_keys, &c->ms_keys2,
-                    &c->ms_perm, &c->ms_perm2, &c->ms_box, &c->ms_tmp, &c->cq_x, &c->cq_y,
-                    &c->cq_out, &c->cb_bound, &c->cb_smin, &c->cb_tiles, &c->cb_stats,
+  for (DevBuf *b : {&c->cull.rec, &c->cull.ext, &c->cull.tiles, &c->cull.groups, &c->ms_keys,
+                    &c->ms_keys2, &c->ms_perm, &c->ms_perm2, &c->ms_box, &c->ms_tmp, &c->cq_x,
+                    &c->cq_y, &c->cq_out, &c->cb_bound, &c->cb_smin, &c->cb_tiles, &c->cb_stats,
                     &c->gr_pred, &c->gr_order, &c->gr_tmin, &c->gr_tmax, &c->gr_bad,
                     &c->gr_terr, &c->gr_flag, &c->gr_flag_ord, &c->gr_list, &c->gr_nsel,
-                    &c->gr_counts, &c->gr_gmax, &c->gr_anc_order, &c->gr_anc_exact,
-                    &c->gr_anc_net, &c->gr_resid, &c->gr_pq_x, &c->gr_pq_y, &c->gr_pq_idx,
-                    &c->gr_pq_exact, &c->gr_out})
+                    &c->gr_counts, &c->gr_gmax, &c->gr_lat_order, &c->gr_lat_exact,
+                    &c->gr_lat_net, &c->gr_q_order, &c->gr_q_exact, &c->gr_q_net, &c->gr_resid,
+                    &c->gr_out})
     release(*b);
   if (c->cv_graph) cudaGraphExecDestroy(c->cv_graph);
   if (c->ev3) cudaEventDestroy(c->ev3);
@@ -1347,10 +1349,12 @@ int ensure_culled(bbkde_ctx *c, const Resolved &r) {
   if (cc.key == c->pack32.key) return BBKDE_OK;
   const int64_t n = c->sets[BBKDE_REFERENCE].n;
   cc.n_tiles = (int)((n + kRefTile - 1) / kRefTile);
+  cc.n_groups = (cc.n_tiles + kGroupTiles - 1) / kGroupTiles;
   if (n > 0) {
     TRY(ensure(c, cc.rec, (size_t)n * sizeof(float4)));
     TRY(ensure(c, cc.ext, (size_t)n * sizeof(float)));
     TRY(ensure(c, cc.tiles, (size_t)cc.n_tiles * sizeof(RefTile)));
+    TRY(ensure(c, cc.groups, (size_t)cc.n_groups * sizeof(RefTile)));
     const float *rx = c->pack32.rec.as<float>();
     const int *perm = nullptr;
     TRY(morton_sort(c, rx, r.dim == 2 ? rx + 1 : nullptr, 4, n, &perm));
@@ -1366,6 +1370,9 @@ int ensure_culled(bbkde_ctx *c, const Resolved &r) {
     else
       k_ref_tiles<1><<<tb, 256, 0, c->stream>>>(cc.rec.as<float4>(), tex, n, cc.n_tiles,
                                                 cc.tiles.as<RefTile>());
+    COUNT_LAUNCH(c);
+    k_ref_groups<<<grid1d(cc.n_groups), 256, 0, c->stream>>>(
+        cc.tiles.as<RefTile>(), cc.n_tiles, cc.n_groups, cc.groups.as<RefTile>());
     COUNT_LAUNCH(c);
     CUDA_TRY(c, cudaGetLastError());
   }
@@ -1385,10 +1392,21 @@ void launch_cull_op(int shape, unsigned nblk, cudaStream_t st, const CullArgs &a
     k_pair_sum_culled<OP, D, 4, 64, 8><<<nblk, 64, 0, st>>>(a);
 }
 
+template <int OP>
+void launch_cull_sep(int tile, unsigned nblk, cudaStream_t st, const CullArgs &a) {
+  if (tile == 32)
+    k_pair_sum_culled_sep<OP, 32><<<nblk, 32 * 32 / 8, 0, st>>>(a);
+  else
+    k_pair_sum_culled_sep<OP, 16><<<nblk, 16 * 16 / 8, 0, st>>>(a);
+}
+
 // One culled (or, with full, complete) sum over nblk query blocks; adds its
 // statistics (pairs at tile granularity, worst bound ratio) to *pairs, *ratio.
+// sep_tile > 0: grid-tile blocks of sep_tile^2 points in the factored form
+// (k_pair_sum_culled_sep); the operator must factor over the axes.
 int launch_culled(bbkde_ctx *c, const Resolved &r, int shape, unsigned nblk,
-                  const CullQueries &q, double rel, bool full, double *pairs, double *ratio) {
+                  const CullQueries &q, double rel, bool full, double *pairs, double *ratio,
+                  int sep_tile = 0) {
   if (nblk == 0) return BBKDE_OK;
   TRY(ensure(c, c->cb_bound, (size_t)nblk * sizeof(double)));
   TRY(ensure(c, c->cb_smin, (size_t)nblk * sizeof(double)));
@@ -1398,7 +1416,9 @@ int launch_culled(bbkde_ctx *c, const Resolved &r, int shape, unsigned nblk,
   a.refs = c->cull.rec.as<float4>();
   a.extra = c->cull.ext.as<float>();
   a.tiles = c->cull.tiles.as<RefTile>();
+  a.groups = c->cull.groups.as<RefTile>();
   a.n_tiles = c->cull.n_tiles;
+  a.n_groups = c->cull.n_groups;
   a.n_ref = c->sets[BBKDE_REFERENCE].n;
   a.cut = full ? INFINITY : kCullCut;
   a.rel = rel;
@@ -1407,7 +1427,14 @@ int launch_culled(bbkde_ctx *c, const Resolved &r, int shape, unsigned nblk,
   a.blk_smin = c->cb_smin.as<double>();
   a.blk_tiles = c->cb_tiles.as<int>();
   const bool d2 = r.dim == 2;
-  switch (r.op) {
+  if (sep_tile > 0) {
+    switch (r.op) {
+      case OP_GAUSS_ISO: launch_cull_sep<OP_GAUSS_ISO>(sep_tile, nblk, c->stream, a); break;
+      case OP_GAUSS_PROD: launch_cull_sep<OP_GAUSS_PROD>(sep_tile, nblk, c->stream, a); break;
+      case OP_EPAN_PROD: launch_cull_sep<OP_EPAN_PROD>(sep_tile, nblk, c->stream, a); break;
+      default: return fail(c, BBKDE_UNSUPPORTED, "culled sum: kernel does not factor");
+    }
+  } else switch (r.op) {
     case OP_GAUSS_ISO:
       d2 ? launch_cull_op<OP_GAUSS_ISO, 2>(shape, nblk, c->stream, a)
          : launch_cull_op<OP_GAUSS_ISO, 1>(shape, nblk, c->stream, a);
@@ -1550,9 +1577,11 @@ GridDesc make_grid(int64_t nx, int64_t ny, double x0, double dx, double y0, doub
   return g;
 }
 
-// Exact sums at the points of every listed tile of g (results row-major into out).
+// Exact sums at the points of every listed tile of g (results row-major into out),
+// in the factored form where the kernel factors over the axes unless pair_form.
 int grid_exact(bbkde_ctx *c, const Resolved &r, const GridDesc &g, const int *list, int64_t n,
-               double rel, bool full, double *out, double *pairs, double *ratio) {
+               double rel, bool full, double *out, double *pairs, double *ratio,
+               bool pair_form = false) {
   CullQueries q = {};
   q.mode = 1;
   q.tile_list = list;
@@ -1567,7 +1596,8 @@ int grid_exact(bbkde_ctx *c, const Resolved &r, const GridDesc &g, const int *li
   q.out = out;
   q.scale = r.norm;
   const int shape = g.tile == 32 ? 0 : 1;
-  return launch_culled(c, r, shape, (unsigned)n, q, rel, full, pairs, ratio);
+  const int sep = (!pair_form && r.dim == 2 && op_separable(r.op)) ? g.tile : 0;
+  return launch_culled(c, r, shape, (unsigned)n, q, rel, full, pairs, ratio, sep);
 }
 
 }  // namespace
@@ -1665,30 +1695,56 @@ extern "C" int bbkde_eval_grid(bbkde_ctx *c, bbkde_surrogate *sur, const bbkde_k
     } else {
       CUDA_TRY(c, cudaMemsetAsync(pred, 0, (size_t)npts * sizeof(float), c->stream));
     }
-    const float *resid = nullptr;
-    int64_t n_anchor = 0;
-    if (mode == BBKDE_GRID_ANCHORED) {
-      // Anchors at the tile corners: a grid offset by half a point spacing.
-      const GridDesc ga = make_grid(g.ntx + 1, g.nty + 1, g.x0 - 0.5 * g.dx, T * g.dx,
-                                    g.y0 - 0.5 * g.dy, T * g.dy, 16);
-      n_anchor = ga.nx * ga.ny;
-      TRY(ensure(c, c->gr_anc_exact, (size_t)n_anchor * sizeof(double)));
-      TRY(ensure(c, c->gr_anc_net, (size_t)n_anchor * sizeof(float)));
-      TRY(ensure(c, c->gr_resid, (size_t)n_anchor * sizeof(float)));
+    CUDA_TRY(c, cudaEventRecord(c->ev1, c->stream));
+    // 2. Exact values on the half-pitch lattice (anchors and probes; one regular
+    //    grid of pitch T/2 from the grid's origin, past its end by one pitch) and,
+    //    for 9 probes, on the quarter lattice; network values there.
+    const int h = T / 2;
+    const GridDesc gl = make_grid(2 * (int64_t)g.ntx + 1, 2 * (int64_t)g.nty + 1, g.x0,
+                                  h * g.dx, g.y0, h * g.dy, 16);
+    const int64_t n_lat = gl.nx * gl.ny;
+    TRY(ensure(c, c->gr_lat_exact, (size_t)n_lat * sizeof(double)));
+    TRY(tile_order(c, gl, c->gr_lat_order));
+    TRY(grid_exact(c, r, gl, c->gr_lat_order.as<int>(), (int64_t)gl.ntx * gl.nty,
+                   cfg->cull_rel, full, c->gr_lat_exact.as<double>(), &st.pairs,
+                   &st.max_bound_ratio, cfg->pair_form != 0));
+    const float *lat_net = nullptr, *q_net = nullptr;
+    if (sur) {
+      TRY(ensure(c, c->gr_lat_net, (size_t)n_lat * sizeof(float)));
+      TRY(bbkde::surrogate_infer(sur, c->stream, n_lat, nullptr, gl.nx, gl.x0, gl.dx, gl.y0,
+                                 gl.dy, c->gr_lat_net.as<float>()) == BBKDE_OK
+              ? BBKDE_OK
+              : fail(c, BBKDE_CUDA_ERROR, "grid: surrogate inference failed"));
+      COUNT_LAUNCH(c);
+      lat_net = c->gr_lat_net.as<float>();
+    }
+    int64_t n_q = 0;
+    if (P == 9) {
+      const GridDesc gq = make_grid(2 * (int64_t)g.ntx, 2 * (int64_t)g.nty, g.x0 + (T / 4) * g.dx,
+                                    h * g.dx, g.y0 + (T / 4) * g.dy, h * g.dy, 16);
+      n_q = gq.nx * gq.ny;
+      TRY(ensure(c, c->gr_q_exact, (size_t)n_q * sizeof(double)));
+      TRY(tile_order(c, gq, c->gr_q_order));
+      TRY(grid_exact(c, r, gq, c->gr_q_order.as<int>(), (int64_t)gq.ntx * gq.nty, cfg->cull_rel,
+                     full, c->gr_q_exact.as<double>(), &st.pairs, &st.max_bound_ratio,
+                     cfg->pair_form != 0));
       if (sur) {
-        TRY(bbkde::surrogate_infer(sur, c->stream, n_anchor, nullptr, ga.nx, ga.x0, ga.dx, ga.y0,
-                                   ga.dy, c->gr_anc_net.as<float>()) == BBKDE_OK
+        TRY(ensure(c, c->gr_q_net, (size_t)n_q * sizeof(float)));
+        TRY(bbkde::surrogate_infer(sur, c->stream, n_q, nullptr, gq.nx, gq.x0, gq.dx, gq.y0,
+                                   gq.dy, c->gr_q_net.as<float>()) == BBKDE_OK
                 ? BBKDE_OK
                 : fail(c, BBKDE_CUDA_ERROR, "grid: surrogate inference failed"));
         COUNT_LAUNCH(c);
+        q_net = c->gr_q_net.as<float>();
       }
-      TRY(tile_order(c, ga, c->gr_anc_order));
-      TRY(grid_exact(c, r, ga, c->gr_anc_order.as<int>(), (int64_t)ga.ntx * ga.nty,
-                     cfg->cull_rel, full, c->gr_anc_exact.as<double>(), &st.pairs,
-                     &st.max_bound_ratio));
+    }
+    // 3. Anchored mode: residual at the anchors, interpolated onto the grid.
+    const float *resid = nullptr;
+    if (mode == BBKDE_GRID_ANCHORED) {
+      const int64_t n_anchor = ((int64_t)g.ntx + 1) * (g.nty + 1);
+      TRY(ensure(c, c->gr_resid, (size_t)n_anchor * sizeof(float)));
       k_anchor_residual<<<grid1d(n_anchor), 256, 0, c->stream>>>(
-          c->gr_anc_exact.as<double>(), sur ? c->gr_anc_net.as<float>() : nullptr, n_anchor,
-          c->gr_resid.as<float>());
+          c->gr_lat_exact.as<double>(), lat_net, g.ntx, g.nty, c->gr_resid.as<float>());
       COUNT_LAUNCH(c);
       resid = c->gr_resid.as<float>();
     }
@@ -1700,36 +1756,22 @@ extern "C" int bbkde_eval_grid(bbkde_ctx *c, bbkde_surrogate *sur, const bbkde_k
     k_max_finite<<<1, 1024, 0, c->stream>>>(c->gr_tmax.as<float>(), (int)ntiles,
                                             c->gr_gmax.as<float>());
     COUNT_LAUNCH(c);
-    CUDA_TRY(c, cudaGetLastError());
-    CUDA_TRY(c, cudaEventRecord(c->ev1, c->stream));
-    // 2. Held-out probes, exact, in Morton tile order (compact query blocks).
-    const int64_t np = ntiles * P;
-    TRY(ensure(c, c->gr_pq_x, (size_t)np * sizeof(float)));
-    TRY(ensure(c, c->gr_pq_y, (size_t)np * sizeof(float)));
-    TRY(ensure(c, c->gr_pq_idx, (size_t)np * sizeof(int64_t)));
-    TRY(ensure(c, c->gr_pq_exact, (size_t)np * sizeof(double)));
-    k_make_probes<<<grid1d(np), 256, 0, c->stream>>>(g, c->gr_order.as<int>(), P,
-                                                     c->gr_pq_x.as<float>(), c->gr_pq_y.as<float>(),
-                                                     c->gr_pq_idx.as<int64_t>());
-    COUNT_LAUNCH(c);
-    CullQueries q = {};
-    q.mode = 0;
-    q.qx = c->gr_pq_x.as<float>();
-    q.qy = c->gr_pq_y.as<float>();
-    q.count = np;
-    q.out = c->gr_pq_exact.as<double>();
-    q.scale = r.norm;
-    TRY(launch_culled(c, r, 1, (unsigned)((np + kCullQpb[1] - 1) / kCullQpb[1]), q, cfg->cull_rel,
-                      full, &st.pairs, &st.max_bound_ratio));
-    CUDA_TRY(c, cudaMemsetAsync(c->gr_terr.p, 0, (size_t)ntiles * sizeof(unsigned), c->stream));
-    k_probe_check<<<grid1d(np), 256, 0, c->stream>>>(pred, c->gr_pq_idx.as<int64_t>(),
-                                                     c->gr_pq_exact.as<double>(),
-                                                     c->gr_order.as<int>(), P, np,
-                                                     c->gr_terr.as<unsigned>());
+    // 4. Held-out probes: every tile's interpolant against the exact lattice values.
+    ProbeArgs pa;
+    pa.g = g;
+    pa.lat_exact = c->gr_lat_exact.as<double>();
+    pa.lat_net = lat_net;
+    pa.q_exact = P == 9 ? c->gr_q_exact.as<double>() : nullptr;
+    pa.q_net = q_net;
+    pa.resid = resid;
+    pa.interp = interp;
+    pa.probes = P;
+    pa.terr = c->gr_terr.as<unsigned>();
+    k_probe_check<<<grid1d(ntiles), 256, 0, c->stream>>>(pa);
     COUNT_LAUNCH(c);
     CUDA_TRY(c, cudaGetLastError());
     CUDA_TRY(c, cudaEventRecord(c->ev2, c->stream));
-    st.exact_points = n_anchor + np;
+    st.exact_points = n_lat + n_q;
   }
   // 3. Decisions, predicted values, exact fallback on the flagged tiles.
   k_flag_tiles<<<grid1d(ntiles), 256, 0, c->stream>>>(fa);
@@ -1757,7 +1799,7 @@ extern "C" int bbkde_eval_grid(bbkde_ctx *c, bbkde_surrogate *sur, const bbkde_k
                               c->stream));
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   TRY(grid_exact(c, r, g, c->gr_list.as<int>(), nsel, cfg->cull_rel, full, out, &st.pairs,
-                 &st.max_bound_ratio));
+                 &st.max_bound_ratio, cfg->pair_form != 0));
   CUDA_TRY(c, cudaEventRecord(c->ev3, c->stream));
   // Points in the flagged tiles (edge tiles may be partial).
   std::vector<int> flags((size_t)ntiles);
@@ -1824,7 +1866,7 @@ extern "C" int bbkde_lsq_numint_cv(bbkde_ctx *c, const bbkde_kernel_desc *k,
   // Square integral over the grid (:62-93).
   const int64_t npts = grid->nx * grid->ny;
   TRY(ensure(c, c->gr_out, (size_t)npts * sizeof(double)));
-  bbkde_grid_config cfg = {BBKDE_GRID_EXACT, 16, 1, 1, 1e-3, 0.0, 1e-7, 1};
+  bbkde_grid_config cfg = {BBKDE_GRID_EXACT, 16, 1, 1, 1e-3, 0.0, 1e-7, 1, 0};
   bbkde_grid_stats st;
   TRY(bbkde_eval_grid(c, nullptr, k, grid, &cfg, c->gr_out.as<double>(), &st));
   const unsigned nb = std::min<unsigned>(grid1d(npts, kRedBlock), 4096u);

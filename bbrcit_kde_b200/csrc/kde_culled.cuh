@@ -12,6 +12,12 @@
 // the Epanechnikov kernels the question is whether any pair lies inside the
 // support.
 //
+// Every run of kGroupTiles consecutive tiles is a "tile group" with the union of
+// their boxes, their widest scales and their summed mass: a group bound is at
+// least the bound of each member tile, so each scan tests the groups first and
+// only opens the members of groups that can matter (two-level scan; a skipped
+// group counts as one skipped unit with its group bound).
+//
 // Gaussian blocks run three scans over the tiles:
 //   1. M = the largest e over the block's box;
 //   2. sum every tile with e >= M - cut (the near field);
@@ -41,7 +47,8 @@
 namespace bbkde {
 
 constexpr int kRefTile = 256;      // references per culling tile
-constexpr int kCullChunk = 1024;   // tiles tested per compaction round
+constexpr int kCullChunk = 1024;   // capacity of the per-round list of needed tiles
+constexpr int kGroupTiles = 16;    // tiles per tile group (two-level scan)
 
 struct RefTile {
   float x0, x1, y0, y1;   // bounding box (y unused in 1-D)
@@ -72,7 +79,9 @@ struct CullArgs {
   const float4 *refs;     // Morton-sorted packed records
   const float *extra;     // second scale column of the product kernels (or null)
   const RefTile *tiles;
+  const RefTile *groups;  // one per kGroupTiles consecutive tiles (bounds of the union)
   int n_tiles;
+  int n_groups;
   int64_t n_ref;
   float cut;              // near-field width in log2 units
   double rel;             // bound of the skipped part relative to the block minimum
@@ -129,6 +138,76 @@ __device__ __forceinline__ bool cull_query(const CullQueries &q, int64_t lq, flo
 // Exponent below which every FP32 kernel value is flushed to zero.
 constexpr float kFlushExp = -128.0f;
 
+// Largest bound(t) over all tiles (block-wide; every thread gets the result).
+// Thread-per-group: a group whose bound does not exceed the thread's running
+// maximum cannot hold a tile that does, so only the others are opened.
+template <int BLOCK, class Bound>
+__device__ __forceinline__ float cull_max(const CullArgs &a, float *s_red, Bound bound) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  float e = -INFINITY;
+  for (int gi = tid; gi < a.n_groups; gi += BLOCK) {
+    if (bound(a.groups[gi]) > e) {
+      const int t1 = min((gi + 1) * kGroupTiles, a.n_tiles);
+      for (int ti = gi * kGroupTiles; ti < t1; ++ti) e = fmaxf(e, bound(a.tiles[ti]));
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) e = fmaxf(e, __shfl_xor_sync(0xffffffffu, e, o));
+  if (lane == 0) s_red[warp] = e;
+  __syncthreads();
+  e = -INFINITY;
+#pragma unroll
+  for (int w = 0; w < BLOCK / 32; ++w) e = fmaxf(e, s_red[w]);
+  __syncthreads();
+  return e;
+}
+
+// One culling pass over the tiles, two levels. Each round, thread tid < GR tests
+// one group (group_needed; it also books the bound of a group it skips); the
+// members of a needed group are tested one by one (tile_needed). The needed tiles
+// of the round are listed in ascending order in s_list[0, total) and handed to
+// sum_list(total), which every thread calls. Returns the number of tiles listed.
+template <int BLOCK, class GroupNeeded, class TileNeeded, class SumList>
+__device__ __forceinline__ int cull_pass(const CullArgs &a, int *s_list, int *s_wc,
+                                         GroupNeeded group_needed, TileNeeded tile_needed,
+                                         SumList sum_list) {
+  constexpr int NW = BLOCK / 32;
+  constexpr int GR = BLOCK < kCullChunk / kGroupTiles ? BLOCK : kCullChunk / kGroupTiles;
+  static_assert(kGroupTiles <= 32, "member mask is 32 bits");
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  int summed = 0;
+  for (int g0 = 0; g0 < a.n_groups; g0 += GR) {
+    const int gi = g0 + tid;
+    unsigned mask = 0;
+    if (tid < GR && gi < a.n_groups && group_needed(a.groups[gi])) {
+      const int t0 = gi * kGroupTiles, t1 = min(t0 + kGroupTiles, a.n_tiles);
+      for (int ti = t0; ti < t1; ++ti)
+        if (tile_needed(a.tiles[ti])) mask |= 1u << (ti - t0);
+    }
+    const int cnt = __popc(mask);
+    int incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    if (lane == 31) s_wc[warp] = incl;
+    __syncthreads();
+    int pos = incl - cnt, total = 0;
+#pragma unroll
+    for (int w = 0; w < NW; ++w) {
+      pos += w < warp ? s_wc[w] : 0;
+      total += s_wc[w];
+    }
+    for (unsigned m = mask; m; m &= m - 1u) s_list[pos++] = gi * kGroupTiles + __ffs(m) - 1;
+    __syncthreads();
+    if (total > 0) sum_list(total);
+    summed += total;
+    __syncthreads();
+  }
+  return summed;
+}
+
 template <int OP, int D, int QPT, int BLOCK, int MINB>
 __global__ void __launch_bounds__(BLOCK, MINB) k_pair_sum_culled(CullArgs a) {
   static_assert(QPT % 2 == 0 && kRefTile % BLOCK == 0 && kCullChunk % BLOCK == 0, "shape");
@@ -151,14 +230,12 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_pair_sum_culled(CullArgs a) {
   float2 qx[NP], qy[NP];
   float sum[QPT], comp[QPT];
   bool valid[QPT];
-  int64_t oidx[QPT];
 #pragma unroll
   for (int k = 0; k < QPT; ++k) {
     float x = 0.f, y = 0.f;
     int64_t o = 0;
     valid[k] = cull_query<D, QPB>(a.q, (int64_t)k * BLOCK + tid, x, y, o);
     if (!valid[k]) { x = 0.f; y = 0.f; }
-    oidx[k] = o;
     float bx0 = valid[k] ? x : 3e38f, bx1 = valid[k] ? x : -3e38f;
     float by0 = valid[k] ? y : 3e38f, by1 = valid[k] ? y : -3e38f;
 #pragma unroll
@@ -197,33 +274,26 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_pair_sum_culled(CullArgs a) {
 
   // Scan 1 (Gaussians): largest tile bound over the block's box.
   float e_max = -INFINITY;
-  if (kGauss) {
-    for (int ti = tid; ti < a.n_tiles; ti += BLOCK) {
-      const RefTile t = a.tiles[ti];
-      e_max = fmaxf(e_max, t.lm + tile_peak<OP, D>(t, qx0, qx1, qy0, qy1));
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) e_max = fmaxf(e_max, __shfl_xor_sync(0xffffffffu, e_max, o));
-    if (lane == 0) s_f[0][0][warp] = e_max;
-    __syncthreads();
-    e_max = -INFINITY;
-#pragma unroll
-    for (int w = 0; w < NW; ++w) e_max = fmaxf(e_max, s_f[0][0][w]);
-    __syncthreads();
-  }
+  if (kGauss)
+    e_max = cull_max<BLOCK>(a, &s_f[0][0][0], [&](const RefTile &t) {
+      return t.lm + tile_peak<OP, D>(t, qx0, qx1, qy0, qy1);
+    });
   const float t_a = e_max - a.cut;
 
   // Skipped bound of slot k relative to its threshold: sum of 2^(e_k - T_k) < 1
-  // per tile (terms below 2^-126 of the threshold flush; they are negligible).
+  // per skipped unit (terms below 2^-126 of the threshold flush; they are
+  // negligible). ex2.approx errs by ~2^-22 relative, inside the 1% mass slack.
   float skipped[QPT];
 #pragma unroll
   for (int k = 0; k < QPT; ++k) skipped[k] = 0.f;
   int summed = 0;
 
-  // Is tile t needed? phase 0: Epanechnikov (support of some slot); phase 1:
-  // Gaussian near field; phase 2: Gaussian far field (per-slot thresholds, and
-  // the per-slot bound of a skipped tile).
-  auto needed = [&](const RefTile &t, int phase) -> bool {
+  // Is tile (or group) t needed? phase 0: Epanechnikov (support of some slot);
+  // phase 1: Gaussian near field; phase 2: Gaussian far field (per-slot
+  // thresholds; a unit that is not needed books its per-slot bound). For a group
+  // the near-field test of phase 2 is left out: a skipped group may hold tiles
+  // summed in phase 1, whose bound is then booked as well (an over-estimate).
+  auto needed = [&](const RefTile &t, int phase, bool group) -> bool {
     if (!kGauss) {
       bool need = false;
 #pragma unroll
@@ -235,7 +305,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_pair_sum_culled(CullArgs a) {
     if (pb < kFlushExp) return false;   // every pair flushes to zero
     const bool near = t.lm + pb >= t_a;
     if (phase == 1) return near;
-    if (near) return false;             // already summed
+    if (near && !group) return false;   // already summed
     bool need = false;
 #pragma unroll
     for (int k = 0; k < QPT; ++k) {
@@ -246,82 +316,69 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_pair_sum_culled(CullArgs a) {
 #pragma unroll
       for (int k = 0; k < QPT; ++k) {
         const float pk = tile_peak<OP, D>(t, s_box[k][0], s_box[k][1], s_box[k][2], s_box[k][3]);
-        if (pk >= kFlushExp) skipped[k] += exp2f(t.lm + pk - s_th[k]);
+        if (pk >= kFlushExp) skipped[k] += ex2_approx(t.lm + pk - s_th[k]);
       }
     }
     return need;
   };
 
-  auto pass = [&](int phase) {
-    for (int c0 = 0; c0 < a.n_tiles; c0 += kCullChunk) {
-      int running = 0;
-      for (int r = 0; r < kCullChunk; r += BLOCK) {
-        const int ti = c0 + r + tid;
-        const bool need = ti < a.n_tiles && needed(a.tiles[ti], phase);
-        const unsigned ballot = __ballot_sync(0xffffffffu, need);
-        if (lane == 0) s_wc[warp] = __popc(ballot);
-        __syncthreads();
-        int base = running, total = 0;
+  // Sum the listed tiles (ascending order).
+  auto sum_list = [&](int running) {
+    for (int li = 0; li < running; ++li) {
+      const int64_t t0 = (int64_t)s_list[li] * kRefTile;
+      const int64_t t1 = min(t0 + kRefTile, a.n_ref);
 #pragma unroll
-        for (int w = 0; w < NW; ++w) {
-          base += w < warp ? s_wc[w] : 0;
-          total += s_wc[w];
-        }
-        if (need) s_list[base + __popc(ballot & ((1u << lane) - 1u))] = ti;
-        running += total;
-        __syncthreads();
-      }
-      summed += running;
-      for (int li = 0; li < running; ++li) {
-        const int64_t t0 = (int64_t)s_list[li] * kRefTile;
-        const int64_t t1 = min(t0 + kRefTile, a.n_ref);
-#pragma unroll
-        for (int i = tid; i < kRefTile; i += BLOCK) {
-          const int64_t rr = t0 + i;
-          const float4 v = rr < t1 ? a.refs[rr] : make_float4(0.f, 0.f, 0.f, 0.f);
-          if (D == 2) {
-            s_r0[i] = make_float4(-v.x, -v.x, -v.y, -v.y);
-            s_r1[i] = make_float4(v.z, v.z, v.w, v.w);
-            if (kExt) {
-              const float e = rr < t1 ? a.extra[rr] : 0.f;
-              s_r2[i] = make_float4(e, e, 0.f, 0.f);
-            }
-          } else {
-            s_r0[i] = make_float4(-v.x, -v.x, 0.f, 0.f);
-            s_r1[i] = make_float4(v.y, v.y, v.z, v.z);
+      for (int i = tid; i < kRefTile; i += BLOCK) {
+        const int64_t rr = t0 + i;
+        const float4 v = rr < t1 ? a.refs[rr] : make_float4(0.f, 0.f, 0.f, 0.f);
+        if (D == 2) {
+          s_r0[i] = make_float4(-v.x, -v.x, -v.y, -v.y);
+          s_r1[i] = make_float4(v.z, v.z, v.w, v.w);
+          if (kExt) {
+            const float e = rr < t1 ? a.extra[rr] : 0.f;
+            s_r2[i] = make_float4(e, e, 0.f, 0.f);
           }
+        } else {
+          s_r0[i] = make_float4(-v.x, -v.x, 0.f, 0.f);
+          s_r1[i] = make_float4(v.y, v.y, v.z, v.z);
         }
-        __syncthreads();
-        for (int j0 = 0; j0 < kRefTile; j0 += kChunk) {
-          float2 acc[NP];
+      }
+      __syncthreads();
+      for (int j0 = 0; j0 < kRefTile; j0 += kChunk) {
+        float2 acc[NP];
 #pragma unroll
-          for (int p = 0; p < NP; ++p) acc[p] = f2(0.0f);
+        for (int p = 0; p < NP; ++p) acc[p] = f2(0.0f);
 #pragma unroll 4
-          for (int j = 0; j < kChunk; ++j) {
-            const float4 r0 = s_r0[j0 + j];
-            const float4 r1 = s_r1[j0 + j];
-            const float4 r2 = kExt ? s_r2[j0 + j] : r1;
-            const float2 m = make_float2(r1.x, r1.y);
+        for (int j = 0; j < kChunk; ++j) {
+          const float4 r0 = s_r0[j0 + j];
+          const float4 r1 = s_r1[j0 + j];
+          const float4 r2 = kExt ? s_r2[j0 + j] : r1;
+          const float2 m = make_float2(r1.x, r1.y);
 #pragma unroll
-            for (int p = 0; p < NP; ++p)
-              acc[p] = __ffma2_rn(m, pair_u2<OP, D>(qx[p], qy[p], r0, r1, r2), acc[p]);
-          }
+          for (int p = 0; p < NP; ++p)
+            acc[p] = __ffma2_rn(m, pair_u2<OP, D>(qx[p], qy[p], r0, r1, r2), acc[p]);
+        }
 #pragma unroll
-          for (int p = 0; p < NP; ++p) {
+        for (int p = 0; p < NP; ++p) {
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
-              const int k = 2 * p + h;
-              const float v = h ? acc[p].y : acc[p].x;
-              const float y = v - comp[k];
-              const float t = sum[k] + y;
-              comp[k] = (t - sum[k]) - y;
-              sum[k] = t;
-            }
+          for (int h = 0; h < 2; ++h) {
+            const int k = 2 * p + h;
+            const float v = h ? acc[p].y : acc[p].x;
+            const float y = v - comp[k];
+            const float t = sum[k] + y;
+            comp[k] = (t - sum[k]) - y;
+            sum[k] = t;
           }
         }
-        __syncthreads();
       }
+      __syncthreads();
     }
+  };
+
+  auto pass = [&](int phase) {
+    summed += cull_pass<BLOCK>(
+        a, s_list, s_wc, [&](const RefTile &g) { return needed(g, phase, true); },
+        [&](const RefTile &t) { return needed(t, phase, false); }, sum_list);
   };
 
   double smin_all = 0.0, ratio = 0.0;
@@ -380,8 +437,12 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_pair_sum_culled(CullArgs a) {
     a.blk_tiles[blockIdx.x] = summed;
   }
 #pragma unroll
-  for (int k = 0; k < QPT; ++k)
-    if (valid[k]) a.q.out[oidx[k]] = a.q.scale * ((double)sum[k] - (double)comp[k]);
+  for (int k = 0; k < QPT; ++k) {
+    float x, y;
+    int64_t o;
+    if (cull_query<D, QPB>(a.q, (int64_t)k * BLOCK + tid, x, y, o))
+      a.q.out[o] = a.q.scale * ((double)sum[k] - (double)comp[k]);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -521,6 +582,29 @@ __global__ void k_ref_tiles(const float4 *rec, const float *ext, int64_t n, int 
     rt.pad = 0.f;
     tiles[t] = rt;
   }
+}
+
+// One thread per group of kGroupTiles consecutive tiles: union of the boxes,
+// widest scales, log2 of the summed (already 1%-padded) masses, rounded up.
+__global__ void k_ref_groups(const RefTile *tiles, int n_tiles, int n_groups,
+                             RefTile *groups) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= n_groups) return;
+  RefTile u;
+  u.x0 = 3e38f; u.x1 = -3e38f; u.y0 = 3e38f; u.y1 = -3e38f;
+  u.sx = -3e38f; u.sy = -3e38f;
+  double m = 0.0;
+  const int t1 = min((g + 1) * kGroupTiles, n_tiles);
+  for (int ti = g * kGroupTiles; ti < t1; ++ti) {
+    const RefTile t = tiles[ti];
+    u.x0 = fminf(u.x0, t.x0); u.x1 = fmaxf(u.x1, t.x1);
+    u.y0 = fminf(u.y0, t.y0); u.y1 = fmaxf(u.y1, t.y1);
+    u.sx = fmaxf(u.sx, t.sx); u.sy = fmaxf(u.sy, t.sy);
+    if (t.lm > -INFINITY) m += exp2((double)t.lm);
+  }
+  u.lm = m > 0.0 ? nextafterf((float)log2(m), INFINITY) : -INFINITY;
+  u.pad = 0.f;
+  groups[g] = u;
 }
 
 // Largest skipped-bound ratio over the blocks, summed tiles.

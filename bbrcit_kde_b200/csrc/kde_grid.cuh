@@ -4,12 +4,19 @@
 // row-major j * gnx + i) is cut into tile x tile blocks, numbered ty * ntx + tx.
 // Per tile the pipeline decides between the surrogate's value and the exact
 // (culled or full) pair sum:
+//   * exact values on the half-pitch lattice: the points (a T/2, b T/2) in grid
+//     index units, 0 <= a <= 2 ntx, 0 <= b <= 2 nty (the last row and column lie
+//     just past the grid's end) -- one regular grid, so one factored culled sum;
 //   * prediction: log-density from the network at every point; in anchored mode
-//     plus the bilinear interpolation of the residual log f - net measured
-//     exactly at the tile corners ("anchors", a (ntx + 1) x (nty + 1) grid offset
-//     by half a point spacing);
-//   * held-out probes: 1, 5 or 9 grid points per tile (centre, edge midpoints,
-//     quarter points), evaluated exactly and compared with the prediction;
+//     plus the interpolation of the residual log f - net measured exactly at the
+//     anchors, the even lattice points (the first point of every tile, a
+//     (ntx + 1) x (nty + 1) lattice of pitch T): bilinear between the tile's
+//     corners or bicubic (Catmull-Rom) over the 4 x 4 anchors around it;
+//   * held-out probes, judged with the tile's own interpolant: the centre
+//     (T/2, T/2), the four edge midpoints (T/2, 0), (0, T/2), (T, T/2), (T/2, T)
+//     -- odd lattice points, the last two shared with the neighbouring tiles --
+//     and, for 9 probes, the quarter points (T/4 + {0, T/2}, T/4 + {0, T/2}) from
+//     a second lattice of pitch T/2;
 //   * a tile goes exact when a probe misses by more than rel_tol, when its
 //     smallest predicted density is below low_frac times the grid's largest,
 //     or when a prediction or anchor is not finite.
@@ -40,14 +47,18 @@ __global__ void k_tile_keys(GridDesc g, unsigned *keys, int *ids) {
 }
 
 // resid = log(exact) - net at the anchors (NaN where the exact density is not
-// a positive finite number); net may be null (a zero network).
-__global__ void k_anchor_residual(const double *exact, const float *net, int64_t n,
+// a positive finite number); net may be null (a zero network). Anchor (A, B),
+// 0 <= A <= ntx, 0 <= B <= nty, is lattice point (2A, 2B) of the half-pitch
+// lattice (row length 2 ntx + 1); resid is (ntx + 1) wide.
+__global__ void k_anchor_residual(const double *exact, const float *net, int ntx, int nty,
                                   float *resid) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const double f = exact[i];
+  const int64_t aw = ntx + 1;
+  if (i >= aw * (nty + 1)) return;
+  const int64_t l = (2 * (i / aw)) * (2 * (int64_t)ntx + 1) + 2 * (i % aw);
+  const double f = exact[l];
   const bool ok = f > 0.0 && f < INFINITY;
-  resid[i] = ok ? (float)(log(f) - (net ? (double)net[i] : 0.0)) : NAN;
+  resid[i] = ok ? (float)(log(f) - (net ? (double)net[l] : 0.0)) : NAN;
 }
 
 // Catmull-Rom weights of the four samples at -1, 0, 1, 2 for a point at t in [0, 1].
@@ -59,9 +70,41 @@ __device__ __forceinline__ void cr_weights(float t, float (&w)[4]) {
   w[3] = 0.5f * (t3 - t2);
 }
 
-// One block per tile: pred += interpolated residual (anchored mode: bilinear
-// between the tile's 4 corner anchors, or bicubic Catmull-Rom over the 4 x 4
-// anchors around the tile, clamped at the grid's edge), tile min / max of pred,
+// Anchor slot (a, c) of tile (tx, ty), 0 <= a, c < 4: bicubic uses the 4 x 4
+// anchors around the tile (clamped at the lattice's edge), bilinear the tile's
+// corners in slots 1 and 2.
+__device__ __forceinline__ int64_t anchor_index(const GridDesc &g, int tx, int ty, int a, int c,
+                                                int interp) {
+  int ax, ay;
+  if (interp == 3) {
+    ax = min(max(tx - 1 + a, 0), g.ntx);
+    ay = min(max(ty - 1 + c, 0), g.nty);
+  } else {
+    ax = tx + (a >= 2 ? 1 : 0);
+    ay = ty + (c >= 2 ? 1 : 0);
+  }
+  return (int64_t)ay * (g.ntx + 1) + ax;
+}
+
+// Residual interpolant of one tile at tile coordinates (u, w) in [0, 1]^2
+// (u = 0 at the tile's first column, u = 1 at the next tile's first column).
+__device__ __forceinline__ float resid_interp(const float (&r)[4][4], float u, float w,
+                                              int interp) {
+  if (interp == 3) {
+    float wu[4], wv[4];
+    cr_weights(u, wu);
+    cr_weights(w, wv);
+    float acc = 0.f;
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+      acc += wv[c] * (wu[0] * r[c][0] + wu[1] * r[c][1] + wu[2] * r[c][2] + wu[3] * r[c][3]);
+    return acc;
+  }
+  return (1.f - w) * ((1.f - u) * r[1][1] + u * r[1][2]) + w * ((1.f - u) * r[2][1] + u * r[2][2]);
+}
+
+// One block per tile: pred += interpolated residual (anchored mode; point
+// (li, lj) of the tile at (u, w) = (li / T, lj / T)), tile min / max of pred,
 // bad flag for non-finite values (a NaN anchor makes its tiles exact).
 __global__ void k_tile_reduce(GridDesc g, float *pred, const float *resid, int interp,
                               float *tmin, float *tmax, int *bad) {
@@ -72,15 +115,7 @@ __global__ void k_tile_reduce(GridDesc g, float *pred, const float *resid, int i
   const int tx = t % g.ntx, ty = t / g.ntx;
   if (resid && threadIdx.x < 16) {
     const int a = threadIdx.x & 3, c = threadIdx.x >> 2;
-    int ax, ay;
-    if (interp == 3) {
-      ax = min(max(tx - 1 + a, 0), g.ntx);
-      ay = min(max(ty - 1 + c, 0), g.nty);
-    } else {   // bilinear: the corners at slots 1 and 2
-      ax = tx + (a >= 2 ? 1 : 0);
-      ay = ty + (c >= 2 ? 1 : 0);
-    }
-    s_r[c][a] = resid[(int64_t)ay * (g.ntx + 1) + ax];
+    s_r[c][a] = resid[anchor_index(g, tx, ty, a, c, interp)];
   }
   __syncthreads();
   float mn = INFINITY, mx = -INFINITY;
@@ -93,21 +128,7 @@ __global__ void k_tile_reduce(GridDesc g, float *pred, const float *resid, int i
     const int64_t p = j * g.nx + i;
     float v = pred[p];
     if (resid) {
-      const float u = (li + 0.5f) / T, w = (lj + 0.5f) / T;
-      if (interp == 3) {
-        float wu[4], wv[4];
-        cr_weights(u, wu);
-        cr_weights(w, wv);
-        float acc = 0.f;
-#pragma unroll
-        for (int c = 0; c < 4; ++c)
-          acc += wv[c] * (wu[0] * s_r[c][0] + wu[1] * s_r[c][1] + wu[2] * s_r[c][2] +
-                          wu[3] * s_r[c][3]);
-        v += acc;
-      } else {
-        v += (1.f - w) * ((1.f - u) * s_r[1][1] + u * s_r[1][2]) +
-             w * ((1.f - u) * s_r[2][1] + u * s_r[2][2]);
-      }
+      v += resid_interp(s_r, (float)li / T, (float)lj / T, interp);
       pred[p] = v;
     }
     if (!(v > -INFINITY && v < INFINITY)) b = 1;   // also catches NaN
@@ -153,47 +174,60 @@ __global__ void k_max_finite(const float *v, int n, float *out) {
   }
 }
 
-// Probe positions in tile coordinates (u, v in [0, 1]): the centre, the edge
-// midpoints, then the quarter points -- where the error of a bilinear
-// interpolation between the corners peaks.
+// Probes of a tile: lattice offsets (da, db) from the tile's first lattice point
+// (2 tx, 2 ty) and tile coordinates (u, w). 0: centre; 1-4: edge midpoints;
+// 5-8: quarter points (on the second lattice, offsets from (2 tx, 2 ty) there).
+__constant__ signed char kProbeDA[9] = {1, 1, 0, 2, 1, 0, 1, 0, 1};
+__constant__ signed char kProbeDB[9] = {1, 0, 1, 1, 2, 0, 0, 1, 1};
 __constant__ float kProbeU[9] = {0.5f, 0.5f, 0.f, 1.f, 0.5f, 0.25f, 0.75f, 0.25f, 0.75f};
-__constant__ float kProbeV[9] = {0.5f, 0.f, 0.5f, 0.5f, 1.f, 0.25f, 0.25f, 0.75f, 0.75f};
+__constant__ float kProbeW[9] = {0.5f, 0.f, 0.5f, 0.5f, 1.f, 0.25f, 0.25f, 0.75f, 0.75f};
 
-// Probe k of the tile at Morton position o -> probe index o * P + k: FP32
-// coordinates and the row-major grid index of the point.
-__global__ void k_make_probes(GridDesc g, const int *order, int P, float *qx, float *qy,
-                              int64_t *gidx) {
-  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int64_t ntiles = (int64_t)g.ntx * g.nty;
-  if (p >= ntiles * P) return;
-  const int t = order[p / P];
-  const int k = (int)(p % P);
-  const int tx = t % g.ntx, ty = t / g.ntx;
-  const int64_t i0 = (int64_t)tx * g.tile, j0 = (int64_t)ty * g.tile;
-  const int64_t wr = g.nx - i0, hr = g.ny - j0;
-  const int w = wr < g.tile ? (int)wr : g.tile, h = hr < g.tile ? (int)hr : g.tile;
-  const int li = min(w - 1, max(0, (int)floorf(kProbeU[k] * w)));
-  const int lj = min(h - 1, max(0, (int)floorf(kProbeV[k] * h)));
-  const int64_t i = i0 + li, j = j0 + lj;
-  qx[p] = (float)(g.x0 + (double)i * g.dx);
-  qy[p] = (float)(g.y0 + (double)j * g.dy);
-  gidx[p] = j * g.nx + i;
-}
+// Inputs of the probe check: the exact values and network values (null: a zero
+// network) on the half-pitch lattice ((2 ntx + 1) x (2 nty + 1)) and, for 9
+// probes, on the quarter lattice (2 ntx x 2 nty); the anchor residuals (null
+// outside anchored mode).
+struct ProbeArgs {
+  GridDesc g;
+  const double *lat_exact;
+  const float *lat_net;
+  const double *q_exact;
+  const float *q_net;
+  const float *resid;
+  int interp;
+  int probes;
+  unsigned *terr;   // per tile: bits of the largest relative error (non-negative float)
+};
 
-// Relative error of the prediction at every probe; per tile the largest, as the
-// ordered bits of a non-negative float (atomicMax is exact and order-free).
-__global__ void k_probe_check(const float *pred, const int64_t *gidx, const double *exact,
-                              const int *order, int P, int64_t n, unsigned *terr) {
-  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= n) return;
-  const double f = exact[p];
-  float err = INFINITY;
-  if (f > 0.0 && f < INFINITY) {
-    const double v = exp((double)pred[gidx[p]]);
-    err = (float)(fabs(v - f) / f);
-    if (!(err >= 0.f)) err = INFINITY;
+// One thread per tile: the largest relative error of the prediction over the
+// tile's probes (+inf where an exact value is not a positive finite number).
+__global__ void k_probe_check(ProbeArgs a) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= a.g.ntx * a.g.nty) return;
+  const int tx = t % a.g.ntx, ty = t / a.g.ntx;
+  float r[4][4];
+  if (a.resid) {
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) r[c][k] = a.resid[anchor_index(a.g, tx, ty, k, c, a.interp)];
   }
-  atomicMax(&terr[order[p / P]], __float_as_uint(err));
+  const int64_t lw = 2 * (int64_t)a.g.ntx + 1, qw = 2 * (int64_t)a.g.ntx;
+  float err = 0.f;
+  for (int k = 0; k < a.probes; ++k) {
+    const bool q = k >= 5;
+    const int64_t l = (2 * (int64_t)ty + kProbeDB[k]) * (q ? qw : lw) + 2 * tx + kProbeDA[k];
+    const double f = q ? a.q_exact[l] : a.lat_exact[l];
+    const float net = q ? (a.q_net ? a.q_net[l] : 0.f) : (a.lat_net ? a.lat_net[l] : 0.f);
+    float v = net;
+    if (a.resid) v += resid_interp(r, kProbeU[k], kProbeW[k], a.interp);
+    float e = INFINITY;
+    if (f > 0.0 && f < INFINITY) {
+      e = (float)(fabs(exp((double)v) - f) / f);
+      if (!(e >= 0.f)) e = INFINITY;
+    }
+    err = fmaxf(err, e);
+  }
+  a.terr[t] = __float_as_uint(err);
 }
 
 struct FlagArgs {

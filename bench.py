@@ -484,9 +484,10 @@ def run_surrogate_grid(a, world, rank, local):
     KDE (pilot h = 0.05, alpha = 0.5), density on an 8192 x 8192 grid over
     [-4, 4]^2. One step = bbkde_eval_grid in anchored mode with the trained network
     (two-term BF16 inference): network value + bicubic residual measured exactly
-    at the tile corners, 5 exact held-out probes per 16 x 16 tile (tolerance
-    5e-4), exact culled fallback on flagged tiles and tiles below 1e-4 of the
-    maximum. Comparators (timed once each): the plain direct sum over all grid
+    at the anchors (every tile's first point), 5 held-out probes per 16 x 16 tile
+    (centre and edge midpoints, tolerance 5e-4; anchors and probes are one
+    1025 x 1025 lattice of pitch 8 evaluated exactly), exact culled fallback on
+    flagged tiles and tiles below 1e-4 of the maximum. Comparators (timed once each): the plain direct sum over all grid
     points, the culled exact sum, the same pipeline without the network, and the
     network alone with probes (no anchors)."""
     import torch
@@ -570,6 +571,9 @@ def run_surrogate_grid(a, world, rank, local):
     # Comparators, each once.
     comp = {}
     for name, kw in [("culled_exact", dict(mode=bk.GRID_EXACT, tile=16)),
+                     ("culled_exact_pair_form", dict(mode=bk.GRID_EXACT, tile=16,
+                                                     pair_form=True)),
+                     ("network_pair_form", dict(main_cfg, pair_form=True)),
                      ("anchored_without_network", dict(main_cfg, surrogate=None)),
                      ("network_bilinear", dict(main_cfg, interp=1)),
                      ("anchored_without_network_bilinear",

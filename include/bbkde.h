@@ -310,14 +310,19 @@ typedef struct {
 enum {
   BBKDE_GRID_EXACT = 0,      /* the exact sum at every point */
   BBKDE_GRID_SURROGATE = 1,  /* network value, held-out probes, exact fallback */
-  BBKDE_GRID_ANCHORED = 2    /* network + residual measured exactly at tile corners */
+  BBKDE_GRID_ANCHORED = 2    /* network + residual measured exactly at the tiles' first
+                                points (anchors), interpolated between them */
 };
 
 typedef struct {
   int mode;          /* BBKDE_GRID_* */
   int tile;          /* decision tile edge in grid points: 16 or 32 */
-  int probes;        /* held-out probes per tile: 1 (centre), 5 (+ edge midpoints)
-                        or 9 (+ quarter points) */
+  int probes;        /* held-out probes per tile, judged with the tile's interpolant:
+                        1 (centre), 5 (+ edge midpoints, shared with the neighbours)
+                        or 9 (+ quarter points). Anchors and the first 5 probes are
+                        the points of one lattice of pitch tile/2 (grid index units)
+                        from the grid's origin, one pitch past its end; the quarter
+                        points a second one: each is one exact grid sum. */
   int exact_culled;  /* 1: exact parts use the culled sum; 0: the full direct sum */
   double rel_tol;    /* a tile keeps the prediction only if every probe is within */
   double low_frac;   /* tiles whose smallest predicted density is below low_frac
@@ -326,24 +331,30 @@ typedef struct {
   int interp;        /* anchored mode: residual between the anchors, 1 = bilinear over
                         the tile's corners, 3 = bicubic (Catmull-Rom) over the 4 x 4
                         anchors around the tile; 0 = 1 */
+  int pair_form;     /* exact sums on grid tiles: 0 = factored over the axes where the
+                        kernel allows it (Gaussians, Epanechnikov product: 2T kernel
+                        factors per reference on a T x T tile instead of T^2 kernel
+                        values); 1 = the pair form everywhere (for comparison) */
 } bbkde_grid_config;
 
 typedef struct {
   int64_t tiles, tiles_low, tiles_flagged, tiles_surrogate;
-  int64_t exact_points;       /* points evaluated by an exact sum (anchors, probes, fallback) */
+  int64_t exact_points;       /* points evaluated by an exact sum (lattices, fallback) */
   double pairs;               /* reference-query pairs of those sums (tile granularity) */
   double max_probe_err;       /* largest held-out error among tiles that are not low */
   double max_bound_ratio;     /* largest culled-sum bound ratio */
-  double ms_total, ms_predict, ms_probe, ms_fallback;   /* device time (CUDA events) */
+  double ms_total, ms_predict, ms_probe, ms_fallback;   /* device time (CUDA events):
+                        predict = network at the grid points; probe = exact lattices,
+                        residual interpolation and probe check; fallback = exact tiles */
 } bbkde_grid_stats;
 
 /* Normalised density of the REFERENCE set (with its current attributes, e.g.
  * after bbkde_adapt_density) on a dense 2-D grid. In the surrogate modes the
  * network `sur` predicts log-density (natural log of the normalised density,
  * the quantity it was trained on); sur may be NULL in BBKDE_GRID_ANCHORED mode
- * (a zero network: bilinear interpolation of the exact log-density between tile
- * corners) and is ignored in BBKDE_GRID_EXACT mode. out_device holds nx * ny
- * doubles in device memory. No reference counterpart. */
+ * (a zero network: interpolation of the exact log-density between the anchors)
+ * and is ignored in BBKDE_GRID_EXACT mode. out_device holds nx * ny doubles in
+ * device memory. No reference counterpart. */
 BBKDE_API int bbkde_eval_grid(bbkde_ctx *ctx, bbkde_surrogate *sur,
                               const bbkde_kernel_desc *kernel, const bbkde_grid *grid,
                               const bbkde_grid_config *cfg, double *out_device,

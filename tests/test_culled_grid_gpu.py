@@ -174,6 +174,29 @@ def test_grid_exact_matches_direct(ctx):
     assert_parity(got32, want, 1e-6 + 1e-7, 1e-8, what="grid exact tile 32")
 
 
+@pytest.mark.parametrize("kind,h", [(W.GAUSS_PROD2D, (0.05, 0.09)), (W.EPAN_PROD2D, (0.2, 0.15)),
+                                    (W.EPAN, (0.2, 0.2))])
+def test_grid_exact_factored_and_pair_forms(ctx, kind, h):
+    """Grid tiles take the factored form u_x * u_y where the kernel factors over
+    the axes (Gaussians, Epanechnikov product) and the pair form otherwise (the
+    isotropic Epanechnikov kernel); both agree with the direct path."""
+    n = 60_000
+    refs = W.config5_refs(n)
+    rng = W.SplitMix64(404)
+    abw = rng.uniform(n, 0.5, 2.0)
+    mass = np.full(n, 1.0 / n) * abw ** -2
+    ctx.upload(bk.REFERENCE, refs, mass=mass, abw=abw)
+    desc = bk.kernel_desc(kind, 2, h)
+    want = _direct_on_grid(ctx, desc, GRID)
+    for tile in (16, 32):
+        for pair_form in (False, True):
+            got, st = _grid_eval(ctx, desc, GRID, mode=bk.GRID_EXACT, tile=tile,
+                                 pair_form=pair_form)
+            assert_parity(got, want, 1e-6 + 1e-7, 1e-8,
+                          what=f"kind {kind} tile {tile} pair_form {pair_form}")
+            assert st.max_bound_ratio <= 1e-7
+
+
 def _tile_ids(grid, tile):
     nx, ny = grid[0], grid[1]
     i = np.arange(nx)[None, :] // tile
@@ -244,6 +267,20 @@ def test_grid_anchored_without_network(ctx):
     assert err3.max() <= 1e-3 and st3.tiles_surrogate > st.tiles // 2, st3.as_dict()
     with pytest.raises(bk.InvalidArgument):
         _grid_eval(ctx, desc, FINE, mode=bk.GRID_ANCHORED, interp=2)
+    # Probes that are grid points of their own tile -- the centre (8, 8), the
+    # first-row and first-column midpoints (8, 0), (0, 8), with 9 probes also the
+    # quarter points -- hold rel_tol in the output: a tile that misses goes exact.
+    # Anchors (0, 0) are exact up to the FP32 log-density.
+    for probes, offs in [(5, [(8, 8), (8, 0), (0, 8)]),
+                         (9, [(8, 8), (8, 0), (0, 8), (4, 4), (12, 4), (4, 12), (12, 12)])]:
+        got_p, st_p = _grid_eval(ctx, desc, FINE, mode=bk.GRID_ANCHORED, tile=16, probes=probes,
+                                 rel_tol=5e-4, low_frac=1e-4, interp=3)
+        e = (np.abs(got_p - want) / want).reshape(FINE[1], FINE[0])
+        for li, lj in offs:
+            assert e[lj::16, li::16].max() <= 5e-4 * (1 + 1e-3), (probes, li, lj)
+        assert e[::16, ::16].max() <= 1e-6, probes
+        assert st_p.exact_points >= (2 * 128 + 1) ** 2 + (256 * 256 if probes == 9 else 0)
+        _check_tiles(st_p, got_p, want, FINE, 16, 5e-4)
     # the low-density rule: tiles below half the maximum go exact
     got, st = _grid_eval(ctx, desc, FINE, mode=bk.GRID_ANCHORED, tile=16, probes=1,
                          rel_tol=5e-4, low_frac=0.5)
@@ -253,7 +290,7 @@ def test_grid_anchored_without_network(ctx):
 
 def test_grid_surrogate_modes_and_network_gain(ctx):
     """The trained network against the same pipeline without it (a zero network:
-    bilinear interpolation of the exact log-density between tile corners)."""
+    bilinear interpolation of the exact log-density between the anchors)."""
     desc, refs = _setup_fine(ctx)
     s = _train(ctx, desc, refs)
     want = _direct_on_grid(ctx, desc, FINE)
