@@ -49,6 +49,8 @@ ENGINE_TCGEN05, ENGINE_MMA_SYNC = 0, 1
 
 # Dense-grid modes (bbkde_grid_config.mode).
 GRID_EXACT, GRID_SURROGATE, GRID_ANCHORED = 0, 1, 2
+# Where the network runs in anchored mode (bbkde_grid_config.net_scope).
+NET_RESCUE, NET_EVERYWHERE = 0, 1
 
 
 class Dataset(C.Structure):
@@ -75,7 +77,8 @@ class Grid(C.Structure):
 class GridConfig(C.Structure):
     _fields_ = [("mode", C.c_int), ("tile", C.c_int), ("probes", C.c_int),
                 ("exact_culled", C.c_int), ("rel_tol", C.c_double), ("low_frac", C.c_double),
-                ("cull_rel", C.c_double), ("interp", C.c_int), ("pair_form", C.c_int)]
+                ("cull_rel", C.c_double), ("interp", C.c_int), ("pair_form", C.c_int),
+                ("net_scope", C.c_int)]
 
 
 class GridStats(C.Structure):
@@ -349,13 +352,14 @@ class Context:
 
     def eval_grid(self, desc: KernelDesc, grid, out_ptr: int, surrogate=None,
                   mode=GRID_EXACT, tile=16, probes=5, exact_culled=True, rel_tol=5e-4,
-                  low_frac=1e-4, cull_rel=1e-7, interp=1, pair_form=False) -> GridStats:
+                  low_frac=1e-4, cull_rel=1e-7, interp=1, pair_form=False,
+                  net_scope=NET_RESCUE) -> GridStats:
         """Density on a dense grid into device memory out_ptr (nx * ny doubles).
 
         grid = (nx, ny, x0, x1, y0, y1). Returns the GridStats."""
         g = Grid(*grid)
         cfg = GridConfig(mode, tile, probes, int(exact_culled), rel_tol, low_frac, cull_rel,
-                         interp, int(pair_form))
+                         interp, int(pair_form), net_scope)
         st = GridStats()
         sh = surrogate.h if surrogate is not None else None
         self._check(self.lib.bbkde_eval_grid(self.h, sh, C.byref(desc), C.byref(g), C.byref(cfg),

@@ -123,7 +123,7 @@ struct bbkde_ctx {
       cb_smin, cb_tiles, cb_stats;
   DevBuf gr_pred, gr_order, gr_tmin, gr_tmax, gr_bad, gr_terr, gr_flag, gr_flag_ord, gr_list,
       gr_nsel, gr_counts, gr_gmax, gr_lat_order, gr_lat_exact, gr_lat_net, gr_q_order, gr_q_exact,
-      gr_q_net, gr_resid, gr_out;
+      gr_q_net, gr_resid, gr_cand_ord, gr_cand_xy, gr_cand_net, gr_out;
   cudaEvent_t ev3 = nullptr;
   std::string err;
 };
@@ -726,7 +726,7 @@ int bbkde_ctx_destroy(bbkde_ctx *c) {
                     &c->gr_terr, &c->gr_flag, &c->gr_flag_ord, &c->gr_list, &c->gr_nsel,
                     &c->gr_counts, &c->gr_gmax, &c->gr_lat_order, &c->gr_lat_exact,
                     &c->gr_lat_net, &c->gr_q_order, &c->gr_q_exact, &c->gr_q_net, &c->gr_resid,
-                    &c->gr_out})
+                    &c->gr_cand_ord, &c->gr_cand_xy, &c->gr_cand_net, &c->gr_out})
     release(*b);
   if (c->cv_graph) cudaGraphExecDestroy(c->cv_graph);
   if (c->ev3) cudaEventDestroy(c->ev3);
@@ -1679,14 +1679,20 @@ extern "C" int bbkde_eval_grid(bbkde_ctx *c, bbkde_surrogate *sur, const bbkde_k
   fa.flag_ord = c->gr_flag_ord.as<int>();
   fa.counts = c->gr_counts.as<unsigned long long>();
 
+  // Rescue mode: the network runs after the probes, on the missed tiles only.
+  const bool rescue =
+      mode == BBKDE_GRID_ANCHORED && sur && cfg->net_scope != BBKDE_NET_EVERYWHERE;
+  const bool net_all = mode != BBKDE_GRID_EXACT && sur && !rescue;
   if (mode == BBKDE_GRID_EXACT) {
     CUDA_TRY(c, cudaEventRecord(c->ev1, c->stream));
     CUDA_TRY(c, cudaEventRecord(c->ev2, c->stream));
+    k_flag_tiles<<<grid1d(ntiles), 256, 0, c->stream>>>(fa);
+    COUNT_LAUNCH(c);
   } else {
-    // 1. Prediction at every point (log-density).
+    // 1. Prediction at every point (log-density): the network, or zero.
     TRY(ensure(c, c->gr_pred, (size_t)npts * sizeof(float)));
     float *pred = c->gr_pred.as<float>();
-    if (sur) {
+    if (net_all) {
       TRY(bbkde::surrogate_infer(sur, c->stream, npts, nullptr, g.nx, g.x0, g.dx, g.y0, g.dy,
                                  pred) == BBKDE_OK
               ? BBKDE_OK
@@ -1695,7 +1701,7 @@ extern "C" int bbkde_eval_grid(bbkde_ctx *c, bbkde_surrogate *sur, const bbkde_k
     } else {
       CUDA_TRY(c, cudaMemsetAsync(pred, 0, (size_t)npts * sizeof(float), c->stream));
     }
-    CUDA_TRY(c, cudaEventRecord(c->ev1, c->stream));
+    if (!rescue) CUDA_TRY(c, cudaEventRecord(c->ev1, c->stream));
     // 2. Exact values on the half-pitch lattice (anchors and probes; one regular
     //    grid of pitch T/2 from the grid's origin, past its end by one pitch) and,
     //    for 9 probes, on the quarter lattice; network values there.
@@ -1708,40 +1714,48 @@ extern "C" int bbkde_eval_grid(bbkde_ctx *c, bbkde_surrogate *sur, const bbkde_k
     TRY(grid_exact(c, r, gl, c->gr_lat_order.as<int>(), (int64_t)gl.ntx * gl.nty,
                    cfg->cull_rel, full, c->gr_lat_exact.as<double>(), &st.pairs,
                    &st.max_bound_ratio, cfg->pair_form != 0));
-    const float *lat_net = nullptr, *q_net = nullptr;
-    if (sur) {
+    auto lattice_net = [&]() -> int {
       TRY(ensure(c, c->gr_lat_net, (size_t)n_lat * sizeof(float)));
       TRY(bbkde::surrogate_infer(sur, c->stream, n_lat, nullptr, gl.nx, gl.x0, gl.dx, gl.y0,
                                  gl.dy, c->gr_lat_net.as<float>()) == BBKDE_OK
               ? BBKDE_OK
               : fail(c, BBKDE_CUDA_ERROR, "grid: surrogate inference failed"));
       COUNT_LAUNCH(c);
+      return BBKDE_OK;
+    };
+    const float *lat_net = nullptr, *q_net = nullptr;
+    if (net_all) {
+      TRY(lattice_net());
       lat_net = c->gr_lat_net.as<float>();
     }
     int64_t n_q = 0;
+    const GridDesc gq = make_grid(2 * (int64_t)g.ntx, 2 * (int64_t)g.nty, g.x0 + (T / 4) * g.dx,
+                                  h * g.dx, g.y0 + (T / 4) * g.dy, h * g.dy, 16);
+    auto quarter_net = [&]() -> int {
+      TRY(ensure(c, c->gr_q_net, (size_t)n_q * sizeof(float)));
+      TRY(bbkde::surrogate_infer(sur, c->stream, n_q, nullptr, gq.nx, gq.x0, gq.dx, gq.y0,
+                                 gq.dy, c->gr_q_net.as<float>()) == BBKDE_OK
+              ? BBKDE_OK
+              : fail(c, BBKDE_CUDA_ERROR, "grid: surrogate inference failed"));
+      COUNT_LAUNCH(c);
+      return BBKDE_OK;
+    };
     if (P == 9) {
-      const GridDesc gq = make_grid(2 * (int64_t)g.ntx, 2 * (int64_t)g.nty, g.x0 + (T / 4) * g.dx,
-                                    h * g.dx, g.y0 + (T / 4) * g.dy, h * g.dy, 16);
       n_q = gq.nx * gq.ny;
       TRY(ensure(c, c->gr_q_exact, (size_t)n_q * sizeof(double)));
       TRY(tile_order(c, gq, c->gr_q_order));
       TRY(grid_exact(c, r, gq, c->gr_q_order.as<int>(), (int64_t)gq.ntx * gq.nty, cfg->cull_rel,
                      full, c->gr_q_exact.as<double>(), &st.pairs, &st.max_bound_ratio,
                      cfg->pair_form != 0));
-      if (sur) {
-        TRY(ensure(c, c->gr_q_net, (size_t)n_q * sizeof(float)));
-        TRY(bbkde::surrogate_infer(sur, c->stream, n_q, nullptr, gq.nx, gq.x0, gq.dx, gq.y0,
-                                   gq.dy, c->gr_q_net.as<float>()) == BBKDE_OK
-                ? BBKDE_OK
-                : fail(c, BBKDE_CUDA_ERROR, "grid: surrogate inference failed"));
-        COUNT_LAUNCH(c);
+      if (net_all) {
+        TRY(quarter_net());
         q_net = c->gr_q_net.as<float>();
       }
     }
     // 3. Anchored mode: residual at the anchors, interpolated onto the grid.
+    const int64_t n_anchor = ((int64_t)g.ntx + 1) * (g.nty + 1);
     const float *resid = nullptr;
     if (mode == BBKDE_GRID_ANCHORED) {
-      const int64_t n_anchor = ((int64_t)g.ntx + 1) * (g.nty + 1);
       TRY(ensure(c, c->gr_resid, (size_t)n_anchor * sizeof(float)));
       k_anchor_residual<<<grid1d(n_anchor), 256, 0, c->stream>>>(
           c->gr_lat_exact.as<double>(), lat_net, g.ntx, g.nty, c->gr_resid.as<float>());
@@ -1759,6 +1773,8 @@ extern "C" int bbkde_eval_grid(bbkde_ctx *c, bbkde_surrogate *sur, const bbkde_k
     // 4. Held-out probes: every tile's interpolant against the exact lattice values.
     ProbeArgs pa;
     pa.g = g;
+    pa.list = nullptr;
+    pa.n_list = 0;
     pa.lat_exact = c->gr_lat_exact.as<double>();
     pa.lat_net = lat_net;
     pa.q_exact = P == 9 ? c->gr_q_exact.as<double>() : nullptr;
@@ -1769,18 +1785,80 @@ extern "C" int bbkde_eval_grid(bbkde_ctx *c, bbkde_surrogate *sur, const bbkde_k
     pa.terr = c->gr_terr.as<unsigned>();
     k_probe_check<<<grid1d(ntiles), 256, 0, c->stream>>>(pa);
     COUNT_LAUNCH(c);
+    k_flag_tiles<<<grid1d(ntiles), 256, 0, c->stream>>>(fa);
+    COUNT_LAUNCH(c);
     CUDA_TRY(c, cudaGetLastError());
-    CUDA_TRY(c, cudaEventRecord(c->ev2, c->stream));
+    CUDA_TRY(c, cudaEventRecord(rescue ? c->ev1 : c->ev2, c->stream));
     st.exact_points = n_lat + n_q;
-  }
-  // 3. Decisions, predicted values, exact fallback on the flagged tiles.
-  k_flag_tiles<<<grid1d(ntiles), 256, 0, c->stream>>>(fa);
-  COUNT_LAUNCH(c);
-  if (mode != BBKDE_GRID_EXACT) {
+
+    // 5. Rescue: the network + its own residual on the tiles whose probes missed;
+    //    a tile keeps that prediction when its probes pass.
+    if (rescue) {
+      TRY(ensure(c, c->gr_cand_ord, (size_t)ntiles * sizeof(int)));
+      k_rescue_mark<<<grid1d(ntiles), 256, 0, c->stream>>>(fa, c->gr_cand_ord.as<int>());
+      COUNT_LAUNCH(c);
+      size_t tmp = 0;
+      CUDA_TRY(c, cub::DeviceSelect::Flagged(nullptr, tmp, c->gr_order.as<int>(),
+                                             c->gr_cand_ord.as<int>(), c->gr_list.as<int>(),
+                                             c->gr_nsel.as<int>(), (int)ntiles, c->stream));
+      TRY(ensure(c, c->ms_tmp, tmp));
+      CUDA_TRY(c, cub::DeviceSelect::Flagged(c->ms_tmp.p, tmp, c->gr_order.as<int>(),
+                                             c->gr_cand_ord.as<int>(), c->gr_list.as<int>(),
+                                             c->gr_nsel.as<int>(), (int)ntiles, c->stream));
+      c->launch_total += 2;
+      int ncand = 0;
+      CUDA_TRY(c, cudaMemcpyAsync(&ncand, c->gr_nsel.p, sizeof(int), cudaMemcpyDeviceToHost,
+                                  c->stream));
+      CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+      if (ncand > 0) {
+        const int *cand = c->gr_list.as<int>();
+        TRY(lattice_net());
+        lat_net = c->gr_lat_net.as<float>();
+        if (P == 9) {
+          TRY(quarter_net());
+          q_net = c->gr_q_net.as<float>();
+        }
+        k_anchor_residual<<<grid1d(n_anchor), 256, 0, c->stream>>>(
+            c->gr_lat_exact.as<double>(), lat_net, g.ntx, g.nty, c->gr_resid.as<float>());
+        COUNT_LAUNCH(c);
+        const int64_t np = (int64_t)ncand * T * T;
+        TRY(ensure(c, c->gr_cand_xy, (size_t)np * sizeof(float2)));
+        TRY(ensure(c, c->gr_cand_net, (size_t)np * sizeof(float)));
+        k_tile_points<<<grid1d(np), 256, 0, c->stream>>>(g, cand, np,
+                                                        c->gr_cand_xy.as<float2>());
+        COUNT_LAUNCH(c);
+        TRY(bbkde::surrogate_infer(sur, c->stream, np, c->gr_cand_xy.as<float2>(), 0, 0.0, 0.0,
+                                   0.0, 0.0, c->gr_cand_net.as<float>()) == BBKDE_OK
+                ? BBKDE_OK
+                : fail(c, BBKDE_CUDA_ERROR, "grid: surrogate inference failed"));
+        COUNT_LAUNCH(c);
+        k_tile_predict_list<<<(unsigned)ncand, 256, 0, c->stream>>>(
+            g, cand, c->gr_cand_net.as<float>(), resid, interp, pred, c->gr_bad.as<int>());
+        COUNT_LAUNCH(c);
+        pa.list = cand;
+        pa.n_list = ncand;
+        pa.lat_net = lat_net;
+        pa.q_net = q_net;
+        k_probe_check<<<grid1d(ncand), 256, 0, c->stream>>>(pa);
+        COUNT_LAUNCH(c);
+        k_rescue_update<<<grid1d(ncand), 256, 0, c->stream>>>(
+            cand, ncand, c->gr_bad.as<int>(), c->gr_terr.as<unsigned>(), (float)cfg->rel_tol,
+            c->gr_flag.as<int>());
+        COUNT_LAUNCH(c);
+        CUDA_TRY(c, cudaMemsetAsync(c->gr_counts.as<unsigned long long>() + 1, 0,
+                                    2 * sizeof(unsigned long long), c->stream));
+        k_flag_recount<<<grid1d(ntiles), 256, 0, c->stream>>>(fa);
+        COUNT_LAUNCH(c);
+        CUDA_TRY(c, cudaGetLastError());
+      }
+      CUDA_TRY(c, cudaEventRecord(c->ev2, c->stream));
+    }
+    // 6. Predicted values on the tiles that keep them.
     const unsigned ab = std::min<unsigned>(grid1d(npts), (unsigned)c->sm_count * 16);
     k_apply<<<ab, 256, 0, c->stream>>>(g, c->gr_pred.as<float>(), c->gr_flag.as<int>(), out);
     COUNT_LAUNCH(c);
   }
+  // 7. Exact fallback on the flagged tiles.
   CUDA_TRY(c, cudaGetLastError());
   size_t tmp = 0;
   CUDA_TRY(c, cub::DeviceSelect::Flagged(nullptr, tmp, c->gr_order.as<int>(),
@@ -1815,10 +1893,11 @@ extern "C" int bbkde_eval_grid(bbkde_ctx *c, bbkde_surrogate *sur, const bbkde_k
   float ms = 0.f;
   CUDA_TRY(c, cudaEventElapsedTime(&ms, c->ev0, c->ev3));
   st.ms_total = ms;
-  CUDA_TRY(c, cudaEventElapsedTime(&ms, c->ev0, c->ev1));
-  st.ms_predict = ms;
-  CUDA_TRY(c, cudaEventElapsedTime(&ms, c->ev1, c->ev2));
-  st.ms_probe = ms;
+  float ms01 = 0.f, ms12 = 0.f;
+  CUDA_TRY(c, cudaEventElapsedTime(&ms01, c->ev0, c->ev1));
+  CUDA_TRY(c, cudaEventElapsedTime(&ms12, c->ev1, c->ev2));
+  st.ms_predict = rescue ? ms12 : ms01;
+  st.ms_probe = rescue ? ms01 : ms12;
   CUDA_TRY(c, cudaEventElapsedTime(&ms, c->ev2, c->ev3));
   st.ms_fallback = ms;
   st.tiles_low = (int64_t)counts[0];
@@ -1866,7 +1945,7 @@ extern "C" int bbkde_lsq_numint_cv(bbkde_ctx *c, const bbkde_kernel_desc *k,
   // Square integral over the grid (:62-93).
   const int64_t npts = grid->nx * grid->ny;
   TRY(ensure(c, c->gr_out, (size_t)npts * sizeof(double)));
-  bbkde_grid_config cfg = {BBKDE_GRID_EXACT, 16, 1, 1, 1e-3, 0.0, 1e-7, 1, 0};
+  bbkde_grid_config cfg = {BBKDE_GRID_EXACT, 16, 1, 1, 1e-3, 0.0, 1e-7, 1, 0, 0};
   bbkde_grid_stats st;
   TRY(bbkde_eval_grid(c, nullptr, k, grid, &cfg, c->gr_out.as<double>(), &st));
   const unsigned nb = std::min<unsigned>(grid1d(npts, kRedBlock), 4096u);

@@ -162,17 +162,26 @@ __device__ __forceinline__ float cull_max(const CullArgs &a, float *s_red, Bound
   return e;
 }
 
+// Groups tested per round of cull_pass and the length of its tile list.
+__host__ __device__ constexpr int cull_groups_per_round(int block) {
+  return block < kCullChunk / kGroupTiles ? block : kCullChunk / kGroupTiles;
+}
+__host__ __device__ constexpr int cull_list_len(int block) {
+  return cull_groups_per_round(block) * kGroupTiles;
+}
+
 // One culling pass over the tiles, two levels. Each round, thread tid < GR tests
 // one group (group_needed; it also books the bound of a group it skips); the
 // members of a needed group are tested one by one (tile_needed). The needed tiles
-// of the round are listed in ascending order in s_list[0, total) and handed to
+// of the round are listed in ascending order in s_list[0, total) (capacity
+// cull_list_len(BLOCK)) and handed to
 // sum_list(total), which every thread calls. Returns the number of tiles listed.
 template <int BLOCK, class GroupNeeded, class TileNeeded, class SumList>
 __device__ __forceinline__ int cull_pass(const CullArgs &a, int *s_list, int *s_wc,
                                          GroupNeeded group_needed, TileNeeded tile_needed,
                                          SumList sum_list) {
   constexpr int NW = BLOCK / 32;
-  constexpr int GR = BLOCK < kCullChunk / kGroupTiles ? BLOCK : kCullChunk / kGroupTiles;
+  constexpr int GR = cull_groups_per_round(BLOCK);
   static_assert(kGroupTiles <= 32, "member mask is 32 bits");
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   int summed = 0;

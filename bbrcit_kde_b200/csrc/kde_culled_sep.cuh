@@ -25,11 +25,16 @@
 // packed f32x2 arithmetic, stored as (even, odd) reference pairs; the points
 // then accumulate two partial sums (even and odd references) with FFMA2.
 //
-// Layout: block = T*T/8 threads, lane (rg, cg) = (tid / (T/4), tid % (T/4)) owns
-// rows 2rg, 2rg + 1 and columns 4cg .. 4cg + 3 of the tile (8 points). Summation:
-// FP32 partial sums of kChunk references (two interleaved halves) folded into
+// Layout: block = T*T/8 threads in two splits of T*T/16 lanes; split sp takes
+// the reference pairs p with p % 2 == sp, and its lane (rg, cg) owns the 4 x 4
+// points of rows {2rg, 2rg + 1, T/2 + 2rg, T/2 + 2rg + 1} and the same columns
+// with cg: per reference pair 4 128-bit loads of factors feed 16 FFMA2 (the
+// shared-memory pipe is the limit of this loop). Factor rows are T + 8 pairs
+// apart so that the splits' loads fall on different banks. Summation: FP32
+// partial sums of kChunk references (two interleaved halves) folded into
 // per-point Kahan accumulators, tiles in ascending sorted order, near field
-// before far field -- deterministic.
+// before far field; the two splits are added in FP64 at the end (split 0 +
+// split 1) -- deterministic.
 #pragma once
 
 #include <cstdint>
@@ -44,37 +49,45 @@ __host__ __device__ constexpr bool op_separable(int op) {
 }
 
 template <int OP, int T>
-__global__ void __launch_bounds__(T *T / 8, T == 32 ? 4 : 16)
+__global__ void __launch_bounds__(T *T / 8, T == 32 ? 3 : 12)
     k_pair_sum_culled_sep(CullArgs a) {
   static_assert(T == 16 || T == 32, "tile edge");
   constexpr int BLOCK = T * T / 8;
   constexpr int NW = BLOCK / 32;
-  constexpr int CG = T / 4;            // column groups (4 columns each)
-  constexpr int RG = T / 2;            // row groups (2 rows each)
+  constexpr int LPS = T * T / 16;      // lanes per split (16 points each)
+  constexpr int CG = T / 4;            // column groups of a split
   constexpr int NS = 8;                // slots: strips of T / 8 rows
-  constexpr int SUB = 64;              // references per factor sub-chunk
+  constexpr int SPR = T / NS;          // rows per slot
+  constexpr int SUB = T == 16 ? 32 : 64;   // references per factor sub-chunk
+  constexpr int FROWS = SUB / 2;       // reference pairs per sub-chunk
+  constexpr int FS = T + 8;            // factor row stride (pairs)
   constexpr int NG = BLOCK / (2 * T);  // factor teams (references split between them)
   constexpr int STG = kRefTile + 4;    // staged column stride (x and y on different banks)
   constexpr bool kGauss = op_gauss(OP);
   constexpr bool kExt = op_has_extra(OP);
-  static_assert(SUB % (2 * NG) == 0 && kRefTile % SUB == 0 && (SUB / 2) % (kChunk / 2) == 0,
-                "shape");
+  static_assert(BLOCK == 2 * LPS, "two splits");
+  static_assert(FROWS % (2 * NG) == 0 || NG == 1, "factor teams");
+  static_assert(kRefTile % SUB == 0 && FROWS % (kChunk / 2) == 0, "shape");
+  static_assert(4 * FROWS * FS >= 2 * T * T, "exchange area");
   __shared__ __align__(16) float s_c[2 * STG];     // -x | -y of the staged references
   __shared__ __align__(16) float s_s[2 * STG];     // x scale | y scale
   __shared__ __align__(16) float s_m[2 * STG];     // 1 | mass
-  __shared__ __align__(16) float2 s_fx[SUB / 2 * T];   // u_x: [pair][column] (even, odd)
-  __shared__ __align__(16) float2 s_fy[SUB / 2 * T];   // m u_y: [pair][row] (even, odd)
+  // u_x rows ([pair][column], (even, odd)) then m u_y rows; reused to hand split
+  // 1's sums to split 0.
+  __shared__ __align__(16) float2 s_fac[2 * FROWS * FS];
   __shared__ float s_qx[T], s_qy[T];
-  __shared__ int s_list[kCullChunk];
+  __shared__ int s_list[cull_list_len(BLOCK)];
   __shared__ int s_wc[NW];
   __shared__ float s_box[NS][4];
   __shared__ float s_th[NS];
   __shared__ unsigned s_min[NS];       // bits of the slot's smallest near-field sum (>= 0)
   __shared__ float s_red[NW];
   __shared__ double s_d[NS][NW];
+  float2 *const s_fx = s_fac;
+  float2 *const s_fy = s_fac + FROWS * FS;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int rg = tid / CG, cg = tid % CG, slot = rg / (RG / NS);
+  const int sp = tid / LPS, rg = (tid % LPS) / CG, cg = (tid % LPS) % CG;
   const CullQueries &q = a.q;
   const int t = q.tile_list[blockIdx.x];
   const int64_t i0 = (int64_t)(t % q.ntx) * T, j0 = (int64_t)(t / q.ntx) * T;
@@ -85,8 +98,8 @@ __global__ void __launch_bounds__(T *T / 8, T == 32 ? 4 : 16)
   for (int i = tid; i < kRefTile; i += BLOCK) s_m[i] = 1.0f;
   if (tid < NS) {
     // slot tid: rows j0 + tid T/8 .. + T/8 - 1 and all columns, inside the grid
-    const int64_t jlo = j0 + (int64_t)tid * (T / NS);
-    const int64_t jhi = (jlo + T / NS < q.gny ? jlo + T / NS : q.gny) - 1;
+    const int64_t jlo = j0 + (int64_t)tid * SPR;
+    const int64_t jhi = (jlo + SPR < q.gny ? jlo + SPR : q.gny) - 1;
     const int64_t ihi = (i0 + T < q.gnx ? i0 + T : q.gnx) - 1;
     if (jlo < q.gny) {
       s_box[tid][0] = grid_coord(q.gx0, q.gdx, i0);
@@ -106,15 +119,11 @@ __global__ void __launch_bounds__(T *T / 8, T == 32 ? 4 : 16)
     qx0 = fminf(qx0, s_box[k][0]); qx1 = fmaxf(qx1, s_box[k][1]);
     qy0 = fminf(qy0, s_box[k][2]); qy1 = fmaxf(qy1, s_box[k][3]);
   }
-  bool valid[8];
+  // The lane's rows and columns: k = 0, 1 -> 2g + k; k = 2, 3 -> T/2 + 2g + k - 2.
+  auto own = [](int g, int k) { return (k < 2 ? 0 : T / 2) + 2 * g + (k & 1); };
+  float sum[16], comp[16];
 #pragma unroll
-  for (int h = 0; h < 2; ++h)
-#pragma unroll
-    for (int k = 0; k < 4; ++k)
-      valid[4 * h + k] = i0 + 4 * cg + k < q.gnx && j0 + 2 * rg + h < q.gny;
-  float sum[8], comp[8];
-#pragma unroll
-  for (int k = 0; k < 8; ++k) { sum[k] = 0.f; comp[k] = 0.f; }
+  for (int k = 0; k < 16; ++k) { sum[k] = 0.f; comp[k] = 0.f; }
 
   // This thread's factor: column w or row w - T of team ft.
   const int fw = tid % (2 * T), ft = tid / (2 * T);
@@ -204,32 +213,31 @@ __global__ void __launch_bounds__(T *T / 8, T == 32 ? 4 : 16)
           u = __ffma2_rn(s2, dd, f2(1.0f));
           u = make_float2(fmaxf(u.x, 0.f), fmaxf(u.y, 0.f));
         }
-        fdst[p * T] = __fmul2_rn(m2, u);
+        fdst[p * FS] = __fmul2_rn(m2, u);
       }
       __syncthreads();
-      for (int pc = 0; pc < SUB / 2; pc += kChunk / 2) {
-        float2 acc[8];
+      for (int pc = 0; pc < FROWS; pc += kChunk / 2) {
+        float2 acc[16];
 #pragma unroll
-        for (int k = 0; k < 8; ++k) acc[k] = f2(0.0f);
-#pragma unroll 8
-        for (int p = pc; p < pc + kChunk / 2; ++p) {
-          const float4 ey = *reinterpret_cast<const float4 *>(&s_fy[p * T + 2 * rg]);
-          const float4 ea = *reinterpret_cast<const float4 *>(&s_fx[p * T + 4 * cg]);
-          const float4 eb = *reinterpret_cast<const float4 *>(&s_fx[p * T + 4 * cg + 2]);
-          const float2 y0 = make_float2(ey.x, ey.y), y1 = make_float2(ey.z, ey.w);
-          const float2 x0 = make_float2(ea.x, ea.y), x1 = make_float2(ea.z, ea.w);
-          const float2 x2 = make_float2(eb.x, eb.y), x3 = make_float2(eb.z, eb.w);
-          acc[0] = __ffma2_rn(y0, x0, acc[0]);
-          acc[1] = __ffma2_rn(y0, x1, acc[1]);
-          acc[2] = __ffma2_rn(y0, x2, acc[2]);
-          acc[3] = __ffma2_rn(y0, x3, acc[3]);
-          acc[4] = __ffma2_rn(y1, x0, acc[4]);
-          acc[5] = __ffma2_rn(y1, x1, acc[5]);
-          acc[6] = __ffma2_rn(y1, x2, acc[6]);
-          acc[7] = __ffma2_rn(y1, x3, acc[7]);
+        for (int k = 0; k < 16; ++k) acc[k] = f2(0.0f);
+#pragma unroll 4
+        for (int p = pc + sp; p < pc + kChunk / 2; p += 2) {
+          const float4 ya = *reinterpret_cast<const float4 *>(&s_fy[p * FS + 2 * rg]);
+          const float4 yb = *reinterpret_cast<const float4 *>(&s_fy[p * FS + T / 2 + 2 * rg]);
+          const float4 xa = *reinterpret_cast<const float4 *>(&s_fx[p * FS + 2 * cg]);
+          const float4 xb = *reinterpret_cast<const float4 *>(&s_fx[p * FS + T / 2 + 2 * cg]);
+          const float2 y[4] = {make_float2(ya.x, ya.y), make_float2(ya.z, ya.w),
+                               make_float2(yb.x, yb.y), make_float2(yb.z, yb.w)};
+          const float2 x[4] = {make_float2(xa.x, xa.y), make_float2(xa.z, xa.w),
+                               make_float2(xb.x, xb.y), make_float2(xb.z, xb.w)};
+#pragma unroll
+          for (int kr = 0; kr < 4; ++kr)
+#pragma unroll
+            for (int kc = 0; kc < 4; ++kc)
+              acc[4 * kr + kc] = __ffma2_rn(y[kr], x[kc], acc[4 * kr + kc]);
         }
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
+        for (int k = 0; k < 16; ++k) {
           const float v = acc[k].x + acc[k].y;
           const float y = v - comp[k];
           const float s2 = sum[k] + y;
@@ -254,14 +262,34 @@ __global__ void __launch_bounds__(T *T / 8, T == 32 ? 4 : 16)
         [&](const RefTile &rt) { return needed(rt, phase, false); }, sum_list);
   };
 
+  // Point k = 4 kr + kc of this lane: row own(rg, kr), column own(cg, kc).
+  auto valid = [&](int k) {
+    return i0 + own(cg, k & 3) < q.gnx && j0 + own(rg, k >> 2) < q.gny;
+  };
+
   double smin_all = 0.0, ratio = 0.0;
   if (kGauss) {
     pass(1);   // near field
-    float m = INFINITY;
+    // Split 1 hands its near-field sums to split 0 (the factor area is free
+    // between passes); split 0 books the smallest per slot.
+    float *const xf = reinterpret_cast<float *>(s_fac);
+    if (sp == 1) {
 #pragma unroll
-    for (int k = 0; k < 8; ++k)
-      if (valid[k]) m = fminf(m, fmaxf(sum[k] - comp[k], 0.f));
-    if (m < INFINITY) atomicMin(&s_min[slot], __float_as_uint(m));
+      for (int k = 0; k < 16; ++k) xf[own(rg, k >> 2) * T + own(cg, k & 3)] = sum[k] - comp[k];
+    }
+    __syncthreads();
+    if (sp == 0) {
+      float m0 = INFINITY, m1 = INFINITY;   // slots of rows k < 2 and k >= 2
+#pragma unroll
+      for (int k = 0; k < 16; ++k) {
+        if (!valid(k)) continue;
+        const float v = fmaxf(sum[k] - comp[k] + xf[own(rg, k >> 2) * T + own(cg, k & 3)], 0.f);
+        if ((k >> 2) < 2) m0 = fminf(m0, v);
+        else m1 = fminf(m1, v);
+      }
+      if (m0 < INFINITY) atomicMin(&s_min[own(rg, 0) / SPR], __float_as_uint(m0));
+      if (m1 < INFINITY) atomicMin(&s_min[own(rg, 2) / SPR], __float_as_uint(m1));
+    }
     __syncthreads();
     if (tid < NS) {
       const double mk = (double)__uint_as_float(s_min[tid]);
@@ -296,13 +324,24 @@ __global__ void __launch_bounds__(T *T / 8, T == 32 ? 4 : 16)
     a.blk_smin[blockIdx.x] = smin_all;
     a.blk_tiles[blockIdx.x] = summed;
   }
+  // Split 1's sums to split 0, which writes split 0 + split 1.
+  double *const xd = reinterpret_cast<double *>(s_fac);
+  __syncthreads();
+  if (sp == 1) {
 #pragma unroll
-  for (int h = 0; h < 2; ++h)
+    for (int k = 0; k < 16; ++k)
+      xd[own(rg, k >> 2) * T + own(cg, k & 3)] = (double)sum[k] - (double)comp[k];
+  }
+  __syncthreads();
+  if (sp == 0) {
 #pragma unroll
-    for (int k = 0; k < 4; ++k)
-      if (valid[4 * h + k])
-        q.out[(j0 + 2 * rg + h) * q.gnx + (i0 + 4 * cg + k)] =
-            q.scale * ((double)sum[4 * h + k] - (double)comp[4 * h + k]);
+    for (int k = 0; k < 16; ++k) {
+      if (!valid(k)) continue;
+      const int row = own(rg, k >> 2), col = own(cg, k & 3);
+      q.out[(j0 + row) * q.gnx + (i0 + col)] =
+          q.scale * (((double)sum[k] - (double)comp[k]) + xd[row * T + col]);
+    }
+  }
 }
 
 }  // namespace bbkde

@@ -188,6 +188,8 @@ __constant__ float kProbeW[9] = {0.5f, 0.f, 0.5f, 0.5f, 1.f, 0.25f, 0.25f, 0.75f
 // outside anchored mode).
 struct ProbeArgs {
   GridDesc g;
+  const int *list;  // tiles to check (null: every tile)
+  int64_t n_list;
   const double *lat_exact;
   const float *lat_net;
   const double *q_exact;
@@ -201,8 +203,9 @@ struct ProbeArgs {
 // One thread per tile: the largest relative error of the prediction over the
 // tile's probes (+inf where an exact value is not a positive finite number).
 __global__ void k_probe_check(ProbeArgs a) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= a.g.ntx * a.g.nty) return;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (a.list ? a.n_list : (int64_t)a.g.ntx * a.g.nty)) return;
+  const int t = a.list ? a.list[i] : (int)i;
   const int tx = t % a.g.ntx, ty = t / a.g.ntx;
   float r[4][4];
   if (a.resid) {
@@ -260,6 +263,80 @@ __global__ void k_flag_tiles(FlagArgs a) {
   if (f) atomicAdd(&a.counts[1], 1ull);
   a.flag[t] = f;
   a.flag_ord[o] = f;
+}
+
+// Rescue candidates: tiles flagged by their probes alone (not low, no
+// non-finite prediction), per Morton position.
+__global__ void k_rescue_mark(FlagArgs a, int *cand_ord) {
+  const int o = blockIdx.x * blockDim.x + threadIdx.x;
+  if (o >= a.g.ntx * a.g.nty) return;
+  const int t = a.order[o];
+  const bool low = !(a.tmin[t] >= *a.gmax + a.log_low);
+  cand_ord[o] = a.flag[t] && !low && !a.bad[t];
+}
+
+// Coordinates of the points of the listed tiles: point l of list entry c is
+// xy[c T^2 + l], (li, lj) = (l % T, l / T) (points past the grid's end included).
+__global__ void k_tile_points(GridDesc g, const int *list, int64_t n, float2 *xy) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int T = g.tile;
+  const int t = list[i / (T * T)];
+  const int l = (int)(i % (T * T));
+  const int64_t gi = (int64_t)(t % g.ntx) * T + l % T, gj = (int64_t)(t / g.ntx) * T + l / T;
+  xy[i] = make_float2((float)(g.x0 + (double)gi * g.dx), (float)(g.y0 + (double)gj * g.dy));
+}
+
+// One block per listed tile: pred = network (net[c T^2 + l]) + interpolated
+// residual on the tile's points; bad flag for non-finite values.
+__global__ void k_tile_predict_list(GridDesc g, const int *list, const float *net,
+                                    const float *resid, int interp, float *pred, int *bad) {
+  __shared__ float s_r[4][4];
+  __shared__ int s_bad;
+  const int c = blockIdx.x, t = list[c];
+  const int tx = t % g.ntx, ty = t / g.ntx;
+  if (threadIdx.x < 16) {
+    const int a = threadIdx.x & 3, r = threadIdx.x >> 2;
+    s_r[r][a] = resid[anchor_index(g, tx, ty, a, r, interp)];
+  }
+  if (threadIdx.x == 0) s_bad = 0;
+  __syncthreads();
+  const int T = g.tile;
+  int b = 0;
+  for (int l = threadIdx.x; l < T * T; l += blockDim.x) {
+    const int li = l % T, lj = l / T;
+    const int64_t i = (int64_t)tx * T + li, j = (int64_t)ty * T + lj;
+    if (i >= g.nx || j >= g.ny) continue;
+    const float v = net[(int64_t)c * T * T + l] + resid_interp(s_r, (float)li / T, (float)lj / T,
+                                                                interp);
+    pred[j * g.nx + i] = v;
+    if (!(v > -INFINITY && v < INFINITY)) b = 1;
+  }
+  if (b) s_bad = 1;
+  __syncthreads();
+  if (threadIdx.x == 0) bad[t] = s_bad;
+}
+
+// A rescued tile keeps the network's prediction when every probe passes.
+__global__ void k_rescue_update(const int *list, int64_t n, const int *bad, const unsigned *terr,
+                                float rel_tol, int *flag) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int t = list[i];
+  flag[t] = bad[t] || !(__uint_as_float(terr[t]) <= rel_tol);
+}
+
+// Flags per Morton position, flagged count and largest probe error over tiles
+// that are not low, from the final per-tile flags and errors (counts[1] and
+// counts[2] start at 0).
+__global__ void k_flag_recount(FlagArgs a) {
+  const int o = blockIdx.x * blockDim.x + threadIdx.x;
+  if (o >= a.g.ntx * a.g.nty) return;
+  const int t = a.order[o];
+  const int f = a.flag[t];
+  a.flag_ord[o] = f;
+  if (f) atomicAdd(&a.counts[1], 1ull);
+  if (a.tmin[t] >= *a.gmax + a.log_low) atomicMax(&a.counts[2], (unsigned long long)a.terr[t]);
 }
 
 // out = exp(pred) on the tiles that keep the prediction.

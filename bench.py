@@ -42,6 +42,7 @@ METRIC = ("2D KDE queries/s (kernel evals/s vs FP32 roofline), direct vs surroga
           "stated rel err")
 UNIT = "kernel evals/s"
 MUFU_EX2_PER_CLK_PER_SM = 16
+FP32_FMA_PER_CLK_PER_SM = 128
 # FP32-pipe poly stride of each pair-sum launch shape (bbkde_launch_variants order):
 # every k-th reference's exponentials on the FP32 pipe, 0 = all on MUFU.
 VARIANT_POLY = [0, 0, 0, 0, 8, 8, 4]
@@ -483,13 +484,15 @@ def run_surrogate_grid(a, world, rank, local):
     """4,000,000 references from the seeded 8-component mixture, adaptive Gaussian
     KDE (pilot h = 0.05, alpha = 0.5), density on an 8192 x 8192 grid over
     [-4, 4]^2. One step = bbkde_eval_grid in anchored mode with the trained network
-    (two-term BF16 inference): network value + bicubic residual measured exactly
-    at the anchors (every tile's first point), 5 held-out probes per 16 x 16 tile
-    (centre and edge midpoints, tolerance 5e-4; anchors and probes are one
-    1025 x 1025 lattice of pitch 8 evaluated exactly), exact culled fallback on
-    flagged tiles and tiles below 1e-4 of the maximum. Comparators (timed once each): the plain direct sum over all grid
-    points, the culled exact sum, the same pipeline without the network, and the
-    network alone with probes (no anchors)."""
+    in rescue mode: bicubic interpolation of the exact log-density between the
+    anchors (every tile's first point), 5 held-out probes per 16 x 16 tile (centre
+    and edge midpoints, tolerance 5e-4; anchors and probes are one 1025 x 1025
+    lattice of pitch 8 evaluated exactly); on the tiles whose probes miss, the
+    network (two-term BF16 inference) + its bicubic residual, kept where its
+    probes pass; exact culled fallback on the rest and on tiles below 1e-4 of the
+    maximum. Comparators (timed once each): the plain direct sum over all grid
+    points, the culled exact sum, the network on every point, the pipeline
+    without the network, and the network alone with probes (no anchors)."""
     import torch
     import bbrcit_kde_b200 as bk
     from bbrcit_kde_b200 import workloads as W
@@ -574,6 +577,7 @@ def run_surrogate_grid(a, world, rank, local):
                      ("culled_exact_pair_form", dict(mode=bk.GRID_EXACT, tile=16,
                                                      pair_form=True)),
                      ("network_pair_form", dict(main_cfg, pair_form=True)),
+                     ("network_everywhere", dict(main_cfg, net_scope=bk.NET_EVERYWHERE)),
                      ("anchored_without_network", dict(main_cfg, surrogate=None)),
                      ("network_bilinear", dict(main_cfg, interp=1)),
                      ("anchored_without_network_bilinear",
@@ -587,10 +591,11 @@ def run_surrogate_grid(a, world, rank, local):
                      ("network_tile32", dict(main_cfg, tile=32)),
                      ("anchored_without_network_tile32",
                       dict(main_cfg, surrogate=None, tile=32))]:
-        l2_flush(torch, flush)
-        torch.cuda.synchronize()
         dst = torch.empty(npts, dtype=torch.float64, device="cuda")
-        st = grid_step(dst, **kw)
+        for _ in range(2):   # the second run is reported (buffers sized, kernels loaded)
+            l2_flush(torch, flush)
+            torch.cuda.synchronize()
+            st = grid_step(dst, **kw)
         comp[name] = (st.as_dict(), dst)
 
     plain = None
@@ -658,17 +663,23 @@ def run_surrogate_grid(a, world, rank, local):
         e2e = {"value": npts * a.steps / (sum(e2e_ms) / 1e3), "unit": GRID_METRIC_UNIT,
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(npts * 8)}
 
-    # Roofline of the culled pair sum (the exact fallback): pairs at tile
-    # granularity of the culled-exact comparator over its device time.
+    # Roofline of the factored culled sum (lattice and fallback kernel): on a
+    # 16 x 16 tile every reference costs 32 kernel factors (MUFU ex2) and 256
+    # multiply-adds, one per pair. The FMA pipe allows 128 pairs/clk/SM and MUFU
+    # 16 ex2/clk/SM = 16 x 256 / 32 = 128 pairs/clk/SM: both bounds coincide.
+    # Pairs at tile granularity of the culled-exact comparator over its device time.
     ce = results["culled_exact"]
     peaks = measured_peaks()
     sm_max = float(peaks.get("sm_max_mhz") or clocks.get("sm_max_mhz") or 1965.0)
-    peak = sm_count * MUFU_EX2_PER_CLK_PER_SM * sm_max * 1e6
+    peak = sm_count * FP32_FMA_PER_CLK_PER_SM * sm_max * 1e6
     ach = ce["pairs"] / (ce["ms_total"] / 1e3)
-    roofline = {"bound": "sfu", "kernel": "k_pair_sum_culled (culled exact grid)",
-                "achieved": ach / 1e9, "peak": peak / 1e9, "unit": "Geval/s",
+    roofline = {"bound": "fp32+sfu", "kernel": "k_pair_sum_culled_sep<GAUSS_ISO,16> "
+                                               "(factored culled exact grid)",
+                "achieved": ach / 1e9, "peak": peak / 1e9, "unit": "Gpair/s",
                 "frac": ach / peak, "traffic": None,
-                "peak_basis": f"{sm_count} SMs x 16 MUFU ex2/clk x {sm_max:.0f} MHz"}
+                "peak_basis": f"{sm_count} SMs x 128 FP32 FMA/clk x {sm_max:.0f} MHz "
+                              "(= 8 pairs per ex2 x 16 ex2/clk: both bounds coincide "
+                              "at tile 16); compute-bound, DRAM traffic negligible"}
     cpu = None
     if rank == 0 and not a.no_cpu_baseline:
         wl = W.Workload("cfg5", W.GAUSS, 2, (0.05, 0.05), refs, w,
@@ -697,8 +708,9 @@ def run_surrogate_grid(a, world, rank, local):
         "config": {"workload": f"surrogate grid: adaptive Gaussian KDE of {n} refs (pilot "
                                f"h=0.05, alpha=0.5) on a {G}x{G} grid over [-4,4]^2",
                    "pipeline": "bbkde_eval_grid anchored mode, bicubic residual, tile 16, "
-                               "5 probes, probe tolerance 5e-4, low_frac 1e-4, two-term BF16 "
-                               "inference on tcgen05",
+                               "5 probes, probe tolerance 5e-4, low_frac 1e-4; network in "
+                               "rescue mode (two-term BF16 inference on tcgen05 on the tiles "
+                               "the interpolated exact anchors miss)",
                    "l2": "flushed between timed steps (256 MB write)"},
         "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
         "gpu_launches": int(launches), "step_stats": stats[-1], "comparators": results,

@@ -335,7 +335,14 @@ typedef struct {
                         kernel allows it (Gaussians, Epanechnikov product: 2T kernel
                         factors per reference on a T x T tile instead of T^2 kernel
                         values); 1 = the pair form everywhere (for comparison) */
+  int net_scope;     /* anchored mode with a network: BBKDE_NET_RESCUE (0) = predict
+                        first without it (interpolated exact log-density) and run the
+                        network only on the tiles whose probes miss, keeping it where
+                        its probes pass; BBKDE_NET_EVERYWHERE (1) = network + residual
+                        on every point */
 } bbkde_grid_config;
+
+enum { BBKDE_NET_RESCUE = 0, BBKDE_NET_EVERYWHERE = 1 };
 
 typedef struct {
   int64_t tiles, tiles_low, tiles_flagged, tiles_surrogate;
@@ -344,8 +351,10 @@ typedef struct {
   double max_probe_err;       /* largest held-out error among tiles that are not low */
   double max_bound_ratio;     /* largest culled-sum bound ratio */
   double ms_total, ms_predict, ms_probe, ms_fallback;   /* device time (CUDA events):
-                        predict = network at the grid points; probe = exact lattices,
-                        residual interpolation and probe check; fallback = exact tiles */
+                        predict = the network (every grid point, or in rescue mode
+                        the lattice and the missed tiles, with their re-check);
+                        probe = exact lattices, residual interpolation and probe
+                        check; fallback = exact tiles */
 } bbkde_grid_stats;
 
 /* Normalised density of the REFERENCE set (with its current attributes, e.g.

@@ -295,21 +295,30 @@ def test_grid_surrogate_modes_and_network_gain(ctx):
     s = _train(ctx, desc, refs)
     want = _direct_on_grid(ctx, desc, FINE)
     res = {}
-    for name, sur, mode, tile in [("surrogate", s, bk.GRID_SURROGATE, 16),
-                                  ("net16", s, bk.GRID_ANCHORED, 16),
-                                  ("zero16", None, bk.GRID_ANCHORED, 16),
-                                  ("net32", s, bk.GRID_ANCHORED, 32),
-                                  ("zero32", None, bk.GRID_ANCHORED, 32)]:
+    for name, sur, mode, tile, scope in [
+            ("surrogate", s, bk.GRID_SURROGATE, 16, bk.NET_RESCUE),
+            ("net16", s, bk.GRID_ANCHORED, 16, bk.NET_RESCUE),
+            ("net16_everywhere", s, bk.GRID_ANCHORED, 16, bk.NET_EVERYWHERE),
+            ("zero16", None, bk.GRID_ANCHORED, 16, bk.NET_RESCUE),
+            ("net32", s, bk.GRID_ANCHORED, 32, bk.NET_RESCUE),
+            ("net32_everywhere", s, bk.GRID_ANCHORED, 32, bk.NET_EVERYWHERE),
+            ("zero32", None, bk.GRID_ANCHORED, 32, bk.NET_RESCUE)]:
         got, st = _grid_eval(ctx, desc, FINE, surrogate=sur, mode=mode, tile=tile, probes=5,
-                             rel_tol=5e-4, low_frac=1e-4)
+                             rel_tol=5e-4, low_frac=1e-4, net_scope=scope)
         err = _check_tiles(st, got, want, FINE, tile, 5e-4)
         res[name] = st
         assert err.max() <= 1e-3, (name, err.max())
     # with the network, more 32-point tiles keep the prediction and fewer points
-    # need an exact sum than without it
-    net, zero = res["net32"], res["zero32"]
-    assert net.tiles_surrogate > zero.tiles_surrogate, (net.as_dict(), zero.as_dict())
-    assert net.exact_points < zero.exact_points
+    # need an exact sum than without it -- the network on every point, and in
+    # rescue mode (the network only where the interpolation alone misses)
+    zero = res["zero32"]
+    for name in ("net32", "net32_everywhere"):
+        net = res[name]
+        assert net.tiles_surrogate > zero.tiles_surrogate, (name, net.as_dict(), zero.as_dict())
+        assert net.exact_points < zero.exact_points, name
+    # rescue mode can only remove tiles from the no-network pipeline's exact set
+    for t in (16, 32):
+        assert res[f"net{t}"].tiles_flagged <= res[f"zero{t}"].tiles_flagged
     # the same with the bicubic residual interpolation (the pipeline's default)
     sts = {}
     for name, sur in [("net", s), ("zero", None)]:
