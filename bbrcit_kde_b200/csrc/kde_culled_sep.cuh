@@ -28,9 +28,14 @@
 // Layout: block = T*T/8 threads in two splits of T*T/16 lanes; split sp takes
 // the reference pairs p with p % 2 == sp, and its lane (rg, cg) owns the 4 x 4
 // points of rows {2rg, 2rg + 1, T/2 + 2rg, T/2 + 2rg + 1} and the same columns
-// with cg: per reference pair 4 128-bit loads of factors feed 16 FFMA2 (the
-// shared-memory pipe is the limit of this loop). Factor rows are T + 8 pairs
-// apart so that the splits' loads fall on different banks. Summation: FP32
+// with cg: per reference pair 4 128-bit loads of factors feed 16 FFMA2. For
+// T = 16 both splits share a warp: odd factor rows are stored with the column
+// index XOR 8, so that the splits' loads fall on different banks.
+//
+// Software pipeline: the factors of sub-chunk s + 1 are computed in the same
+// loop body as the accumulation of sub-chunk s (double-buffered), so that the
+// MUFU/FMA chains of the one and the loads and FFMA2 of the other overlap
+// within every warp. Summation: FP32
 // partial sums of kChunk references (two interleaved halves) folded into
 // per-point Kahan accumulators, tiles in ascending sorted order, near field
 // before far field; the two splits are added in FP64 at the end (split 0 +
@@ -49,7 +54,7 @@ __host__ __device__ constexpr bool op_separable(int op) {
 }
 
 template <int OP, int T>
-__global__ void __launch_bounds__(T *T / 8, T == 32 ? 3 : 12)
+__global__ void __launch_bounds__(T *T / 8, T == 32 ? 4 : 16)
     k_pair_sum_culled_sep(CullArgs a) {
   static_assert(T == 16 || T == 32, "tile edge");
   constexpr int BLOCK = T * T / 8;
@@ -59,22 +64,24 @@ __global__ void __launch_bounds__(T *T / 8, T == 32 ? 3 : 12)
   constexpr int NS = 8;                // slots: strips of T / 8 rows
   constexpr int SPR = T / NS;          // rows per slot
   constexpr int SUB = T == 16 ? 32 : 64;   // references per factor sub-chunk
+  constexpr int NSUB = kRefTile / SUB;
   constexpr int FROWS = SUB / 2;       // reference pairs per sub-chunk
-  constexpr int FS = T + 8;            // factor row stride (pairs)
+  constexpr int FBUF = 2 * FROWS * T;  // factor pairs per buffer (x rows, then y rows)
   constexpr int NG = BLOCK / (2 * T);  // factor teams (references split between them)
+  constexpr int FPB = 2 / NG;          // factor pairs per lane per accumulation step
   constexpr int STG = kRefTile + 4;    // staged column stride (x and y on different banks)
   constexpr bool kGauss = op_gauss(OP);
   constexpr bool kExt = op_has_extra(OP);
   static_assert(BLOCK == 2 * LPS, "two splits");
-  static_assert(FROWS % (2 * NG) == 0 || NG == 1, "factor teams");
+  static_assert(NG * FPB == 2 && kChunk == 32, "one factor step per accumulation step");
   static_assert(kRefTile % SUB == 0 && FROWS % (kChunk / 2) == 0, "shape");
-  static_assert(4 * FROWS * FS >= 2 * T * T, "exchange area");
+  static_assert(2 * FBUF * 2 >= 2 * T * T, "exchange area");
   __shared__ __align__(16) float s_c[2 * STG];     // -x | -y of the staged references
   __shared__ __align__(16) float s_s[2 * STG];     // x scale | y scale
   __shared__ __align__(16) float s_m[2 * STG];     // 1 | mass
-  // u_x rows ([pair][column], (even, odd)) then m u_y rows; reused to hand split
-  // 1's sums to split 0.
-  __shared__ __align__(16) float2 s_fac[2 * FROWS * FS];
+  // Two buffers of u_x rows ([pair][column], (even, odd)) then m u_y rows;
+  // reused to hand split 1's sums to split 0.
+  __shared__ __align__(16) float2 s_fac[2 * FBUF];
   __shared__ float s_qx[T], s_qy[T];
   __shared__ int s_list[cull_list_len(BLOCK)];
   __shared__ int s_wc[NW];
@@ -83,8 +90,6 @@ __global__ void __launch_bounds__(T *T / 8, T == 32 ? 3 : 12)
   __shared__ unsigned s_min[NS];       // bits of the slot's smallest near-field sum (>= 0)
   __shared__ float s_red[NW];
   __shared__ double s_d[NS][NW];
-  float2 *const s_fx = s_fac;
-  float2 *const s_fy = s_fac + FROWS * FS;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int sp = tid / LPS, rg = (tid % LPS) / CG, cg = (tid % LPS) % CG;
@@ -130,7 +135,10 @@ __global__ void __launch_bounds__(T *T / 8, T == 32 ? 3 : 12)
   const bool fx = fw < T;
   const float fq = fx ? s_qx[fw] : s_qy[fw - T];
   const int foff = fx ? 0 : STG;
-  float2 *const fdst = fx ? s_fx + fw : s_fy + (fw - T);
+  const int fcol = fx ? fw : fw - T;
+  float2 *const fbase = s_fac + (fx ? 0 : FROWS * T);
+  // Column swizzle of factor row p (see the layout note).
+  auto swz = [](int p) { return T == 16 ? (p & 1) << 3 : 0; };
 
   // Scan 1 (Gaussians): largest tile bound over the block's box.
   float e_max = -INFINITY;
@@ -196,45 +204,58 @@ __global__ void __launch_bounds__(T *T / 8, T == 32 ? 3 : 12)
       s_m[STG + i] = rec[u].z;
     }
     __syncthreads();
-    for (int sub = 0; sub < kRefTile; sub += SUB) {
-#pragma unroll 4
-      for (int p = ft; p < SUB / 2; p += NG) {
-        const int j = foff + sub + 2 * p;
-        const float2 c2 = *reinterpret_cast<const float2 *>(&s_c[j]);
-        const float2 s2 = *reinterpret_cast<const float2 *>(&s_s[j]);
-        const float2 m2 = *reinterpret_cast<const float2 *>(&s_m[j]);
-        const float2 d = __fadd2_rn(f2(fq), c2);
-        const float2 dd = __fmul2_rn(d, d);
-        float2 u;
-        if (kGauss) {
-          const float2 e = __fmul2_rn(s2, dd);
-          u = make_float2(ex2_approx(e.x), ex2_approx(e.y));
-        } else {
-          u = __ffma2_rn(s2, dd, f2(1.0f));
-          u = make_float2(fmaxf(u.x, 0.f), fmaxf(u.y, 0.f));
-        }
-        fdst[p * FS] = __fmul2_rn(m2, u);
+    // Factor pair p of sub-chunk sub (references sub + 2p, + 1) into buffer b.
+    auto factor = [&](int b, int sub, int p) {
+      const int j = foff + sub + 2 * p;
+      const float2 c2 = *reinterpret_cast<const float2 *>(&s_c[j]);
+      const float2 s2 = *reinterpret_cast<const float2 *>(&s_s[j]);
+      const float2 m2 = *reinterpret_cast<const float2 *>(&s_m[j]);
+      const float2 d = __fadd2_rn(f2(fq), c2);
+      const float2 dd = __fmul2_rn(d, d);
+      float2 u;
+      if (kGauss) {
+        const float2 e = __fmul2_rn(s2, dd);
+        u = make_float2(ex2_approx(e.x), ex2_approx(e.y));
+      } else {
+        u = __ffma2_rn(s2, dd, f2(1.0f));
+        u = make_float2(fmaxf(u.x, 0.f), fmaxf(u.y, 0.f));
       }
-      __syncthreads();
-      for (int pc = 0; pc < FROWS; pc += kChunk / 2) {
+      fbase[b * FBUF + p * T + (fcol ^ swz(p))] = __fmul2_rn(m2, u);
+    };
+    // acc[4 kr + kc] (+)= y[kr] * x[kc] for factor pair p of buffer b.
+    auto step = [&](int b, int p, float2 (&acc)[16], bool first) {
+      const float2 *fx2 = s_fac + b * FBUF + p * T, *fy2 = fx2 + FROWS * T;
+      const int w = swz(p);
+      const float4 ya = *reinterpret_cast<const float4 *>(&fy2[(2 * rg) ^ w]);
+      const float4 yb = *reinterpret_cast<const float4 *>(&fy2[(T / 2 + 2 * rg) ^ w]);
+      const float4 xa = *reinterpret_cast<const float4 *>(&fx2[(2 * cg) ^ w]);
+      const float4 xb = *reinterpret_cast<const float4 *>(&fx2[(T / 2 + 2 * cg) ^ w]);
+      const float2 y[4] = {make_float2(ya.x, ya.y), make_float2(ya.z, ya.w),
+                           make_float2(yb.x, yb.y), make_float2(yb.z, yb.w)};
+      const float2 x[4] = {make_float2(xa.x, xa.y), make_float2(xa.z, xa.w),
+                           make_float2(xb.x, xb.y), make_float2(xb.z, xb.w)};
+#pragma unroll
+      for (int kr = 0; kr < 4; ++kr)
+#pragma unroll
+        for (int kc = 0; kc < 4; ++kc)
+          acc[4 * kr + kc] = first ? __fmul2_rn(y[kr], x[kc])
+                                   : __ffma2_rn(y[kr], x[kc], acc[4 * kr + kc]);
+    };
+    for (int p = ft; p < FROWS; p += NG) factor(0, 0, p);
+    __syncthreads();
+    for (int sb = 0; sb < NSUB; ++sb) {
+      const int cur = sb & 1;
+      const bool more = sb + 1 < NSUB;
+      for (int ch = 0; ch < FROWS / 16; ++ch) {
         float2 acc[16];
 #pragma unroll
-        for (int k = 0; k < 16; ++k) acc[k] = f2(0.0f);
-#pragma unroll 4
-        for (int p = pc + sp; p < pc + kChunk / 2; p += 2) {
-          const float4 ya = *reinterpret_cast<const float4 *>(&s_fy[p * FS + 2 * rg]);
-          const float4 yb = *reinterpret_cast<const float4 *>(&s_fy[p * FS + T / 2 + 2 * rg]);
-          const float4 xa = *reinterpret_cast<const float4 *>(&s_fx[p * FS + 2 * cg]);
-          const float4 xb = *reinterpret_cast<const float4 *>(&s_fx[p * FS + T / 2 + 2 * cg]);
-          const float2 y[4] = {make_float2(ya.x, ya.y), make_float2(ya.z, ya.w),
-                               make_float2(yb.x, yb.y), make_float2(yb.z, yb.w)};
-          const float2 x[4] = {make_float2(xa.x, xa.y), make_float2(xa.z, xa.w),
-                               make_float2(xb.x, xb.y), make_float2(xb.z, xb.w)};
+        for (int i = 0; i < 8; ++i) {
+          if (more) {
 #pragma unroll
-          for (int kr = 0; kr < 4; ++kr)
-#pragma unroll
-            for (int kc = 0; kc < 4; ++kc)
-              acc[4 * kr + kc] = __ffma2_rn(y[kr], x[kc], acc[4 * kr + kc]);
+            for (int f = 0; f < FPB; ++f)
+              factor(cur ^ 1, (sb + 1) * SUB, ft + ((ch * 8 + i) * FPB + f) * NG);
+          }
+          step(cur, ch * 16 + 2 * i + sp, acc, i == 0);
         }
 #pragma unroll
         for (int k = 0; k < 16; ++k) {
