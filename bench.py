@@ -697,7 +697,11 @@ def run_surrogate_grid(a, world, rank, local):
     speedup = {}
     if plain is not None:
         pm = info["plain_direct_ms"]
-        speedup = {"pipeline_vs_plain_direct": pm / (total_ms / a.steps)}
+        speedup = {"pipeline_vs_plain_direct": pm / (total_ms / a.steps),
+                   # one grid including the network's training data and training
+                   "pipeline_with_training_vs_plain_direct":
+                       pm / (total_ms / a.steps + info["train_targets_ms"] +
+                             1e3 * info["train_s"])}
         for name, st in results.items():
             speedup[f"{name}_vs_plain_direct"] = pm / st["ms_total"]
     line = {
