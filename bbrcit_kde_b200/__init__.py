@@ -42,6 +42,7 @@ EXPORTED = [
     "bbkde_surrogate_predict", "bbkde_surrogate_predict_device", "bbkde_surrogate_save",
     "bbkde_surrogate_load", "bbkde_surrogate_set_inference", "bbkde_eval_culled",
     "bbkde_eval_grid", "bbkde_lsq_numint_cv", "bbkde_surrogate_set_engine",
+    "bbkde_adapt_density_tol",
 ]
 
 # Surrogate inference engines (bbkde_surrogate_set_engine).
@@ -158,6 +159,8 @@ def load_library(path: str = LIB_PATH):
     lib.bbkde_eval_range_device.argtypes = [vp, kd, i64, i64, i64, i64, C.c_int, C.c_int, vp,
                                             i64]
     lib.bbkde_adapt_density.argtypes = [vp, kd, C.c_double, C.c_int, _dp, _dp, _dp, _dp]
+    lib.bbkde_adapt_density_tol.argtypes = [vp, kd, C.c_double, C.c_double, _dp, _dp, _dp,
+                                            _dp]
     lib.bbkde_unadapt_density.argtypes = [vp]
     lib.bbkde_likelihood_cv.argtypes = [vp, kd, C.c_int, _dp]
     lib.bbkde_lsq_conv_cv.argtypes = [vp, kd, C.c_int, _dp]
@@ -295,6 +298,19 @@ class Context:
             np.zeros(1)
         self._check(self.lib.bbkde_adapt_density(self.h, C.byref(desc), alpha, precision,
                                                  _p(abw), _p(mass), _p(pilot), _p(g)))
+        return abw[:n], mass[:n], pilot[:n], float(g[0])
+
+    def adapt_density_tol(self, desc: KernelDesc, alpha: float, rel_tol=1e-6, outputs=True):
+        """adapt_density with the pilot to rel_tol (culled self-sum); same returns."""
+        if not outputs:
+            self._check(self.lib.bbkde_adapt_density_tol(self.h, C.byref(desc), alpha, rel_tol,
+                                                         None, None, None, None))
+            return None
+        n = self.size(REFERENCE)
+        abw, mass, pilot, g = np.empty(max(n, 1)), np.empty(max(n, 1)), np.empty(max(n, 1)), \
+            np.zeros(1)
+        self._check(self.lib.bbkde_adapt_density_tol(self.h, C.byref(desc), alpha, rel_tol,
+                                                     _p(abw), _p(mass), _p(pilot), _p(g)))
         return abw[:n], mass[:n], pilot[:n], float(g[0])
 
     def unadapt_density(self):

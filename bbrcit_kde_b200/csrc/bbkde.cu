@@ -1538,6 +1538,89 @@ extern "C" int bbkde_eval_culled(bbkde_ctx *c, const bbkde_kernel_desc *k, int n
   return BBKDE_OK;
 }
 
+// Adaptive densities with the pilot to a relative tolerance
+// (KernelDensity::adapt_density(alpha, rel, abs), KernelDensityImpl.h:291-359,
+// whose pilot the reference evaluates through its tree to rel / abs): the pilot
+// is the culled self-sum of the reference set (every value within rel_tol of
+// the full sum, self term included, FP32-compensated), the rest is
+// bbkde_adapt_density's FP64 epilogue.
+extern "C" int bbkde_adapt_density_tol(bbkde_ctx *c, const bbkde_kernel_desc *k, double alpha,
+                                       double rel_tol, double *abw_out, double *mass_out,
+                                       double *pilot_out, double *g_out) {
+  Resolved r;
+  TRY(self_checks(c, k, BBKDE_FP32C, r));
+  TRY(culled_kernel_ok(c, r));
+  if (!(alpha >= 0 && alpha <= 1))   // KernelDensityImpl.h:301-303
+    return fail(c, BBKDE_INVALID_ARGUMENT, "adapt_density: alpha must be between [0, 1]. ");
+  if (!(rel_tol > 0.0 && rel_tol < 1.0))
+    return fail(c, BBKDE_INVALID_ARGUMENT, "rel_tol must be in (0, 1)");
+  TRY(bbkde_unadapt_density(c));
+  PointSet &s = c->sets[BBKDE_REFERENCE];
+  if (alpha == 0 || s.n == 0) {
+    if (g_out) *g_out = NAN;
+    TRY(download(c, abw_out, s.abw, s.n));
+    TRY(download(c, mass_out, s.mass, s.n));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return BBKDE_OK;
+  }
+  const int64_t n = s.n;
+  TRY(ensure_culled(c, r));
+  const void *qx = nullptr, *qy = nullptr;
+  TRY(ensure_queries(c, BBKDE_REFERENCE, false, &qx, &qy));
+  const float *fx = static_cast<const float *>(qx), *fy = static_cast<const float *>(qy);
+  const int *perm = nullptr;
+  TRY(morton_sort(c, fx, r.dim == 2 ? fy : nullptr, 1, n, &perm));
+  TRY(ensure(c, c->cq_x, (size_t)n * sizeof(float)));
+  TRY(ensure(c, c->cq_y, (size_t)n * sizeof(float)));
+  TRY(ensure(c, c->cq_out, (size_t)std::max<int64_t>(n, kWlogBlocks) * sizeof(double)));
+  TRY(ensure(c, c->out_dev, (size_t)n * sizeof(double)));
+  k_gather_xy<<<grid1d(n), 256, 0, c->stream>>>(fx, r.dim == 2 ? fy : nullptr, perm, n,
+                                                c->cq_x.as<float>(), c->cq_y.as<float>());
+  COUNT_LAUNCH(c);
+  CullQueries q = {};
+  q.mode = 0;
+  q.qx = c->cq_x.as<float>();
+  q.qy = c->cq_y.as<float>();
+  q.count = n;
+  q.out = c->cq_out.as<double>();
+  q.scale = r.norm;
+  double pairs = 0.0, ratio = 0.0;
+  CUDA_TRY(c, cudaEventRecord(c->ev0, c->stream));
+  TRY(launch_culled(c, r, 0, (unsigned)((n + kCullQpb[0] - 1) / kCullQpb[0]), q, rel_tol, false,
+                    &pairs, &ratio));
+  CUDA_TRY(c, cudaEventRecord(c->ev1, c->stream));
+  double *pilot = c->out_dev.as<double>();
+  k_scatter<<<grid1d(n), 256, 0, c->stream>>>(c->cq_out.as<double>(), perm, n, pilot);
+  COUNT_LAUNCH(c);
+  // g = exp(sum_i w_i log pilot_i) in FP64, fixed order (:330-337).
+  k_wlog_partial<<<kWlogBlocks, 256, 0, c->stream>>>(pilot, s.weight.as<double>(), n,
+                                                     c->cq_out.as<double>());
+  COUNT_LAUNCH(c);
+  k_sum_partials<<<1, kWlogBlocks, 0, c->stream>>>(c->cq_out.as<double>(), kWlogBlocks,
+                                                   c->scalars.as<double>());
+  COUNT_LAUNCH(c);
+  k_pilot_finalize<<<grid1d(n), 256, 0, c->stream>>>(
+      pilot, s.weight.as<double>(), c->scalars.as<double>(), alpha, r.dim, n,
+      s.abw.as<double>(), s.mass.as<double>(), c->scalars.as<double>() + 1);
+  COUNT_LAUNCH(c);
+  CUDA_TRY(c, cudaGetLastError());
+  ++s.attr_version;
+  TRY(download(c, pilot_out, c->out_dev, n));
+  TRY(download(c, abw_out, s.abw, n));
+  TRY(download(c, mass_out, s.mass, n));
+  double g = 0;
+  CUDA_TRY(c, cudaMemcpyAsync(&g, c->scalars.as<double>() + 1, sizeof(double),
+                              cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  if (g_out) *g_out = g;
+  float ms = 0.f;
+  CUDA_TRY(c, cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+  c->last_ms = ms;
+  c->last_pairs = pairs;
+  c->last_launches = 6;
+  return BBKDE_OK;
+}
+
 namespace {
 
 // Tile numbers of g in Morton order of their coordinates -> order (ntiles ints).

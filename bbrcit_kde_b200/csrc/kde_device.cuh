@@ -666,6 +666,36 @@ __global__ void k_pilot_finalize(const double *pilot, const double *w, const dou
   mass[i] = w[i] * pow(bw, (double)-dim);
 }
 
+// sum_i w_i log f_i over n values in kWlogBlocks fixed slices: one FP64 partial
+// per block (fixed-order tree within the block) -> part[blockIdx.x].
+constexpr int kWlogBlocks = 256;
+__global__ void k_wlog_partial(const double *f, const double *w, int64_t n, double *part) {
+  __shared__ double s[256];
+  const int64_t per = (n + gridDim.x - 1) / gridDim.x;
+  const int64_t lo = (int64_t)blockIdx.x * per, hi = lo + per < n ? lo + per : n;
+  double acc = 0.0;
+  for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) acc += w[i] * log(f[i]);
+  s[threadIdx.x] = acc;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) s[threadIdx.x] += s[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = s[0];
+}
+
+// out[0] = sum of part[0, m) (m <= 1024 = blockDim.x, a power of two), fixed order.
+__global__ void k_sum_partials(const double *part, int m, double *out) {
+  __shared__ double s[1024];
+  s[threadIdx.x] = (int)threadIdx.x < m ? part[threadIdx.x] : 0.0;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) s[threadIdx.x] += s[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[0] = s[0];
+}
+
 __global__ void k_unadapt(const double *w, int64_t n, double *abw, double *mass) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;

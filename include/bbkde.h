@@ -158,6 +158,16 @@ BBKDE_API int bbkde_adapt_density(bbkde_ctx *ctx, const bbkde_kernel_desc *kerne
                         int precision, double *abw_out, double *mass_out,
                         double *pilot_out, double *g_out);
 
+/* As bbkde_adapt_density, with the pilot to a relative tolerance, as the
+ * reference's adapt_density(alpha, rel, abs) evaluates it through its tree
+ * (KernelDensityImpl.h:291-359): the culled self-sum (see bbkde_eval_culled),
+ * every pilot value within rel_tol (0 < rel_tol < 1) of the full sum plus the
+ * FP32-compensated arithmetic error; g and the attributes in FP64 as above.
+ * The Epanechnikov convolution kernels give UNSUPPORTED. */
+BBKDE_API int bbkde_adapt_density_tol(bbkde_ctx *ctx, const bbkde_kernel_desc *kernel,
+                                      double alpha, double rel_tol, double *abw_out,
+                                      double *mass_out, double *pilot_out, double *g_out);
+
 /* KernelDensity::unadapt_density (KernelDensityImpl.h:254-273): abw = 1, mass = w. */
 BBKDE_API int bbkde_unadapt_density(bbkde_ctx *ctx);
 

@@ -121,6 +121,43 @@ def test_culled_deterministic_and_edge_sizes(ctx, oracle):
     assert got.shape == (0,) and st.pairs == 0
 
 
+@pytest.mark.parametrize("kind,h", [(W.GAUSS_PROD2D, (0.05, 0.05)), (W.EPAN, (0.1, 0.1))])
+def test_adapt_density_tol_matches_exact_pilot(ctx, kind, h):
+    """The pilot to a relative tolerance (culled self-sum) against the exact pilot:
+    every pilot value within rel + 1e-6 (the bound plus both paths' FP32-compensated
+    error), abw within alpha times that, g likewise; far fewer pairs."""
+    refs = W.config5_refs(200_000)
+    rng = W.SplitMix64(8)
+    w = rng.uniform(len(refs), 0.5, 1.5)
+    w /= w.sum()
+    ctx.upload(bk.REFERENCE, refs, mass=w, weight=w)
+    desc = bk.kernel_desc(kind, 2, h)
+    abw0, mass0, pilot0, g0 = ctx.adapt_density(desc, 0.5)
+    for rel in (1e-7, 1e-4):
+        abw, mass, pilot, g = ctx.adapt_density_tol(desc, 0.5, rel_tol=rel)
+        tol = rel + 1e-6
+        np.testing.assert_allclose(pilot, pilot0, rtol=tol, atol=0)
+        np.testing.assert_allclose(abw, abw0, rtol=0.5 * tol, atol=0)
+        np.testing.assert_allclose(mass, mass0, rtol=tol, atol=0)
+        assert g == pytest.approx(g0, rel=tol)
+        _, pairs, _ = ctx.last_launch_stats()
+        assert pairs < 0.5 * len(refs) ** 2
+    # the adapted attributes are the set's: a direct sum now uses them
+    ctx.upload(bk.QUERY, refs[:1000])
+    f_tol = ctx.eval_all(desc)
+    ctx.adapt_density(desc, 0.5)
+    np.testing.assert_allclose(f_tol, ctx.eval_all(desc), rtol=1e-3)
+    abw, _, _, g = ctx.adapt_density_tol(desc, 0.0)
+    assert np.all(abw == 1.0) and np.isnan(g)
+    with pytest.raises(bk.InvalidArgument):
+        ctx.adapt_density_tol(desc, 1.5)
+    with pytest.raises(bk.InvalidArgument):
+        ctx.adapt_density_tol(desc, 0.5, rel_tol=0.0)
+    with pytest.raises(bk.BBKDEError) as e:
+        ctx.adapt_density_tol(bk.kernel_desc(W.EPAN_PROD_CONV2D, 2, (0.1, 0.1)), 0.5)
+    assert e.value.status == bk.UNSUPPORTED
+
+
 def test_culled_rejects_epanechnikov_convolution(ctx):
     refs, q, mass, _ = _problem(3, 1000, 100, 2, False)
     ctx.upload(bk.REFERENCE, refs, mass=mass)
