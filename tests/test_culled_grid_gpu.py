@@ -325,6 +325,44 @@ def test_grid_anchored_without_network(ctx):
     _check_tiles(st, got, want, FINE, 16, 5e-4)
 
 
+def test_grid_ragged_tiles_and_probe_sets(ctx):
+    """Partial edge tiles on both axes (1000 = 62 x 16 + 8, 760 = 47 x 16 + 8):
+    the lattice runs one pitch past the grid's end, every probe set and mode keeps
+    the statistics consistent, flagged tiles are exact, every grid-point probe of
+    a full tile holds rel_tol, and in anchored mode the output stays within 1e-3
+    with the edge probes (5 or 9; measured 1.04e-3 with the centre probe alone at
+    this pitch, which does not guard the tile's edges: bar 2e-3 there). The
+    network alone (surrogate mode, no anchors) is ~2% accurate: a tile whose
+    probes happen to pass keeps that error elsewhere (2.2e-2 measured with one
+    probe), so only the probe points are bounded there."""
+    desc, refs = _setup_fine(ctx)
+    s = _train(ctx, desc, refs, steps=2000)
+    grid = (1000, 760, -3.5, -1.5, 0.5, 2.5)
+    want = _direct_on_grid(ctx, desc, grid)
+    nx, ny = grid[0], grid[1]
+    for name, sur, mode, probes, scope in [
+            ("zero_p1", None, bk.GRID_ANCHORED, 1, bk.NET_RESCUE),
+            ("zero_p9", None, bk.GRID_ANCHORED, 9, bk.NET_RESCUE),
+            ("rescue_p9", s, bk.GRID_ANCHORED, 9, bk.NET_RESCUE),
+            ("everywhere_p5", s, bk.GRID_ANCHORED, 5, bk.NET_EVERYWHERE),
+            ("surrogate_p1", s, bk.GRID_SURROGATE, 1, bk.NET_RESCUE),
+            ("surrogate_p9", s, bk.GRID_SURROGATE, 9, bk.NET_RESCUE)]:
+        got, st = _grid_eval(ctx, desc, grid, surrogate=sur, mode=mode, tile=16, probes=probes,
+                             rel_tol=5e-4, low_frac=1e-4, interp=3, net_scope=scope)
+        assert st.tiles == 63 * 48, name
+        err = _check_tiles(st, got, want, grid, 16, 5e-4)
+        if mode == bk.GRID_ANCHORED:
+            bar = 1e-3 if probes >= 5 else 2e-3
+            assert err.max() <= bar, (name, err.max(), st.as_dict())
+        lattice = 127 * 97 + (126 * 96 if probes == 9 else 0)
+        assert st.exact_points >= lattice, name
+        e = err.reshape(ny, nx)[: 47 * 16, : 62 * 16]   # full tiles only
+        assert e[8::16, 8::16].max() <= 5e-4 * (1 + 1e-3), name   # centre probes
+        if probes >= 5:
+            assert e[::16, 8::16].max() <= 5e-4 * (1 + 1e-3), name
+            assert e[8::16, ::16].max() <= 5e-4 * (1 + 1e-3), name
+
+
 def test_grid_surrogate_modes_and_network_gain(ctx):
     """The trained network against the same pipeline without it (a zero network:
     bilinear interpolation of the exact log-density between the anchors)."""
