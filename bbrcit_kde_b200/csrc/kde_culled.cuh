@@ -170,46 +170,60 @@ __host__ __device__ constexpr int cull_list_len(int block) {
   return cull_groups_per_round(block) * kGroupTiles;
 }
 
+// Block-wide ordered append: the threads with pred write value to dst[rank], rank
+// = the number of such threads before them; returns how many wrote (every thread).
+template <int BLOCK>
+__device__ __forceinline__ int block_append(bool pred, int value, int *dst, int *s_wc) {
+  constexpr int NW = BLOCK / 32;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned b = __ballot_sync(0xffffffffu, pred);
+  const int rank = __popc(b & ((1u << lane) - 1u));
+  if (NW == 1) {
+    if (pred) dst[rank] = value;
+    __syncwarp();
+    return __popc(b);
+  }
+  if (lane == 0) s_wc[warp] = __popc(b);
+  __syncthreads();
+  int base = 0, total = 0;
+#pragma unroll
+  for (int w = 0; w < NW; ++w) {
+    base += w < warp ? s_wc[w] : 0;
+    total += s_wc[w];
+  }
+  if (pred) dst[base + rank] = value;
+  __syncthreads();
+  return total;
+}
+
 // One culling pass over the tiles, two levels. Each round, thread tid < GR tests
 // one group (group_needed; it also books the bound of a group it skips); the
-// members of a needed group are tested one by one (tile_needed). The needed tiles
-// of the round are listed in ascending order in s_list[0, total) (capacity
-// cull_list_len(BLOCK)) and handed to
-// sum_list(total), which every thread calls. Returns the number of tiles listed.
+// needed groups are listed in order (s_glist, GR entries), and the block then
+// tests their members in parallel (tile_needed), BLOCK at a time. The needed
+// tiles of the round are listed in ascending order in s_list[0, total) (capacity
+// cull_list_len(BLOCK)) and handed to sum_list(total), which every thread calls.
+// Returns the number of tiles listed.
 template <int BLOCK, class GroupNeeded, class TileNeeded, class SumList>
-__device__ __forceinline__ int cull_pass(const CullArgs &a, int *s_list, int *s_wc,
+__device__ __forceinline__ int cull_pass(const CullArgs &a, int *s_list, int *s_glist, int *s_wc,
                                          GroupNeeded group_needed, TileNeeded tile_needed,
                                          SumList sum_list) {
-  constexpr int NW = BLOCK / 32;
   constexpr int GR = cull_groups_per_round(BLOCK);
-  static_assert(kGroupTiles <= 32, "member mask is 32 bits");
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int tid = threadIdx.x;
   int summed = 0;
   for (int g0 = 0; g0 < a.n_groups; g0 += GR) {
     const int gi = g0 + tid;
-    unsigned mask = 0;
-    if (tid < GR && gi < a.n_groups && group_needed(a.groups[gi])) {
-      const int t0 = gi * kGroupTiles, t1 = min(t0 + kGroupTiles, a.n_tiles);
-      for (int ti = t0; ti < t1; ++ti)
-        if (tile_needed(a.tiles[ti])) mask |= 1u << (ti - t0);
+    const bool gneed = tid < GR && gi < a.n_groups && group_needed(a.groups[gi]);
+    const int ng = block_append<BLOCK>(gneed, gi, s_glist, s_wc);
+    int total = 0;
+    for (int m0 = 0; m0 < ng * kGroupTiles; m0 += BLOCK) {
+      const int m = m0 + tid;
+      int ti = -1;
+      if (m < ng * kGroupTiles) {
+        ti = s_glist[m / kGroupTiles] * kGroupTiles + m % kGroupTiles;
+        if (ti >= a.n_tiles || !tile_needed(a.tiles[ti])) ti = -1;
+      }
+      total += block_append<BLOCK>(ti >= 0, ti, s_list + total, s_wc);
     }
-    const int cnt = __popc(mask);
-    int incl = cnt;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int v = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= o) incl += v;
-    }
-    if (lane == 31) s_wc[warp] = incl;
-    __syncthreads();
-    int pos = incl - cnt, total = 0;
-#pragma unroll
-    for (int w = 0; w < NW; ++w) {
-      pos += w < warp ? s_wc[w] : 0;
-      total += s_wc[w];
-    }
-    for (unsigned m = mask; m; m &= m - 1u) s_list[pos++] = gi * kGroupTiles + __ffs(m) - 1;
-    __syncthreads();
     if (total > 0) sum_list(total);
     summed += total;
     __syncthreads();
@@ -228,7 +242,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_pair_sum_culled(CullArgs a) {
   __shared__ float4 s_r0[kRefTile];
   __shared__ float4 s_r1[kRefTile];
   __shared__ float4 s_r2[kExt ? kRefTile : 1];
-  __shared__ int s_list[kCullChunk];
+  __shared__ int s_list[cull_list_len(BLOCK)];
+  __shared__ int s_glist[cull_groups_per_round(BLOCK)];
   __shared__ int s_wc[NW];
   __shared__ float s_box[QPT][4];     // slot boxes
   __shared__ float s_th[QPT];         // slot thresholds T_k
@@ -386,7 +401,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_pair_sum_culled(CullArgs a) {
 
   auto pass = [&](int phase) {
     summed += cull_pass<BLOCK>(
-        a, s_list, s_wc, [&](const RefTile &g) { return needed(g, phase, true); },
+        a, s_list, s_glist, s_wc, [&](const RefTile &g) { return needed(g, phase, true); },
         [&](const RefTile &t) { return needed(t, phase, false); }, sum_list);
   };
 

@@ -84,6 +84,7 @@ __global__ void __launch_bounds__(T *T / 8, T == 32 ? 4 : 16)
   __shared__ __align__(16) float2 s_fac[2 * FBUF];
   __shared__ float s_qx[T], s_qy[T];
   __shared__ int s_list[cull_list_len(BLOCK)];
+  __shared__ int s_glist[cull_groups_per_round(BLOCK)];
   __shared__ int s_wc[NW];
   __shared__ float s_box[NS][4];
   __shared__ float s_th[NS];
@@ -126,9 +127,18 @@ __global__ void __launch_bounds__(T *T / 8, T == 32 ? 4 : 16)
   }
   // The lane's rows and columns: k = 0, 1 -> 2g + k; k = 2, 3 -> T/2 + 2g + k - 2.
   auto own = [](int g, int k) { return (k < 2 ? 0 : T / 2) + 2 * g + (k & 1); };
-  float sum[16], comp[16];
+  // Kahan accumulators of the 16 points, two points (k = 2i, 2i + 1: the same
+  // row, adjacent columns) per packed pair.
+  float2 sum[8], comp[8];
 #pragma unroll
-  for (int k = 0; k < 16; ++k) { sum[k] = 0.f; comp[k] = 0.f; }
+  for (int k = 0; k < 8; ++k) { sum[k] = f2(0.f); comp[k] = f2(0.f); }
+  auto point_sum = [&](int k) -> float {
+    return (k & 1) ? sum[k >> 1].y - comp[k >> 1].y : sum[k >> 1].x - comp[k >> 1].x;
+  };
+  auto point_sum_d = [&](int k) -> double {
+    return (k & 1) ? (double)sum[k >> 1].y - (double)comp[k >> 1].y
+                   : (double)sum[k >> 1].x - (double)comp[k >> 1].x;
+  };
 
   // This thread's factor: column w or row w - T of team ft.
   const int fw = tid % (2 * T), ft = tid / (2 * T);
@@ -257,13 +267,17 @@ __global__ void __launch_bounds__(T *T / 8, T == 32 ? 4 : 16)
           }
           step(cur, ch * 16 + 2 * i + sp, acc, i == 0);
         }
+        // Kahan fold, two points per packed op (a - b as fma(b, -1, a): exact
+        // negation, one rounding, as the scalar subtraction).
+        const float2 m1 = f2(-1.0f);
 #pragma unroll
-        for (int k = 0; k < 16; ++k) {
-          const float v = acc[k].x + acc[k].y;
-          const float y = v - comp[k];
-          const float s2 = sum[k] + y;
-          comp[k] = (s2 - sum[k]) - y;
-          sum[k] = s2;
+        for (int k = 0; k < 8; ++k) {
+          const float2 v = make_float2(acc[2 * k].x + acc[2 * k].y,
+                                       acc[2 * k + 1].x + acc[2 * k + 1].y);
+          const float2 y = __ffma2_rn(comp[k], m1, v);
+          const float2 t2 = __fadd2_rn(sum[k], y);
+          comp[k] = __ffma2_rn(y, m1, __ffma2_rn(sum[k], m1, t2));
+          sum[k] = t2;
         }
       }
       __syncthreads();
@@ -279,7 +293,7 @@ __global__ void __launch_bounds__(T *T / 8, T == 32 ? 4 : 16)
 
   auto pass = [&](int phase) {
     summed += cull_pass<BLOCK>(
-        a, s_list, s_wc, [&](const RefTile &g) { return needed(g, phase, true); },
+        a, s_list, s_glist, s_wc, [&](const RefTile &g) { return needed(g, phase, true); },
         [&](const RefTile &rt) { return needed(rt, phase, false); }, sum_list);
   };
 
@@ -296,7 +310,7 @@ __global__ void __launch_bounds__(T *T / 8, T == 32 ? 4 : 16)
     float *const xf = reinterpret_cast<float *>(s_fac);
     if (sp == 1) {
 #pragma unroll
-      for (int k = 0; k < 16; ++k) xf[own(rg, k >> 2) * T + own(cg, k & 3)] = sum[k] - comp[k];
+      for (int k = 0; k < 16; ++k) xf[own(rg, k >> 2) * T + own(cg, k & 3)] = point_sum(k);
     }
     __syncthreads();
     if (sp == 0) {
@@ -304,7 +318,7 @@ __global__ void __launch_bounds__(T *T / 8, T == 32 ? 4 : 16)
 #pragma unroll
       for (int k = 0; k < 16; ++k) {
         if (!valid(k)) continue;
-        const float v = fmaxf(sum[k] - comp[k] + xf[own(rg, k >> 2) * T + own(cg, k & 3)], 0.f);
+        const float v = fmaxf(point_sum(k) + xf[own(rg, k >> 2) * T + own(cg, k & 3)], 0.f);
         if ((k >> 2) < 2) m0 = fminf(m0, v);
         else m1 = fminf(m1, v);
       }
@@ -351,7 +365,7 @@ __global__ void __launch_bounds__(T *T / 8, T == 32 ? 4 : 16)
   if (sp == 1) {
 #pragma unroll
     for (int k = 0; k < 16; ++k)
-      xd[own(rg, k >> 2) * T + own(cg, k & 3)] = (double)sum[k] - (double)comp[k];
+      xd[own(rg, k >> 2) * T + own(cg, k & 3)] = point_sum_d(k);
   }
   __syncthreads();
   if (sp == 0) {
@@ -360,7 +374,7 @@ __global__ void __launch_bounds__(T *T / 8, T == 32 ? 4 : 16)
       if (!valid(k)) continue;
       const int row = own(rg, k >> 2), col = own(cg, k & 3);
       q.out[(j0 + row) * q.gnx + (i0 + col)] =
-          q.scale * (((double)sum[k] - (double)comp[k]) + xd[row * T + col]);
+          q.scale * (point_sum_d(k) + xd[row * T + col]);
     }
   }
 }
