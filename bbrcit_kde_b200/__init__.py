@@ -42,7 +42,7 @@ EXPORTED = [
     "bbkde_surrogate_predict", "bbkde_surrogate_predict_device", "bbkde_surrogate_save",
     "bbkde_surrogate_load", "bbkde_surrogate_set_inference", "bbkde_eval_culled",
     "bbkde_eval_grid", "bbkde_lsq_numint_cv", "bbkde_surrogate_set_engine",
-    "bbkde_adapt_density_tol",
+    "bbkde_adapt_density_tol", "bbkde_likelihood_cv_tol", "bbkde_lsq_conv_cv_tol",
 ]
 
 # Surrogate inference engines (bbkde_surrogate_set_engine).
@@ -161,6 +161,8 @@ def load_library(path: str = LIB_PATH):
     lib.bbkde_adapt_density.argtypes = [vp, kd, C.c_double, C.c_int, _dp, _dp, _dp, _dp]
     lib.bbkde_adapt_density_tol.argtypes = [vp, kd, C.c_double, C.c_double, _dp, _dp, _dp,
                                             _dp]
+    lib.bbkde_likelihood_cv_tol.argtypes = [vp, kd, C.c_double, _dp]
+    lib.bbkde_lsq_conv_cv_tol.argtypes = [vp, kd, C.c_double, _dp]
     lib.bbkde_unadapt_density.argtypes = [vp]
     lib.bbkde_likelihood_cv.argtypes = [vp, kd, C.c_int, _dp]
     lib.bbkde_lsq_conv_cv.argtypes = [vp, kd, C.c_int, _dp]
@@ -319,6 +321,18 @@ class Context:
     def likelihood_cv(self, desc: KernelDesc, precision=FP32C) -> float:
         cv = np.zeros(1)
         self._check(self.lib.bbkde_likelihood_cv(self.h, C.byref(desc), precision, _p(cv)))
+        return float(cv[0])
+
+    def likelihood_cv_tol(self, desc: KernelDesc, rel_tol=1e-6) -> float:
+        """Likelihood CV with the density sums to rel_tol (culled self-sums)."""
+        cv = np.zeros(1)
+        self._check(self.lib.bbkde_likelihood_cv_tol(self.h, C.byref(desc), rel_tol, _p(cv)))
+        return float(cv[0])
+
+    def lsq_conv_cv_tol(self, desc: KernelDesc, rel_tol=1e-6) -> float:
+        """LSQ convolution CV with the density sums to rel_tol (culled self-sums)."""
+        cv = np.zeros(1)
+        self._check(self.lib.bbkde_lsq_conv_cv_tol(self.h, C.byref(desc), rel_tol, _p(cv)))
         return float(cv[0])
 
     def lsq_conv_cv(self, desc: KernelDesc, precision=FP32C) -> float:

@@ -1538,32 +1538,16 @@ extern "C" int bbkde_eval_culled(bbkde_ctx *c, const bbkde_kernel_desc *k, int n
   return BBKDE_OK;
 }
 
-// Adaptive densities with the pilot to a relative tolerance
-// (KernelDensity::adapt_density(alpha, rel, abs), KernelDensityImpl.h:291-359,
-// whose pilot the reference evaluates through its tree to rel / abs): the pilot
-// is the culled self-sum of the reference set (every value within rel_tol of
-// the full sum, self term included, FP32-compensated), the rest is
-// bbkde_adapt_density's FP64 epilogue.
-extern "C" int bbkde_adapt_density_tol(bbkde_ctx *c, const bbkde_kernel_desc *k, double alpha,
-                                       double rel_tol, double *abw_out, double *mass_out,
-                                       double *pilot_out, double *g_out) {
-  Resolved r;
-  TRY(self_checks(c, k, BBKDE_FP32C, r));
-  TRY(culled_kernel_ok(c, r));
-  if (!(alpha >= 0 && alpha <= 1))   // KernelDensityImpl.h:301-303
-    return fail(c, BBKDE_INVALID_ARGUMENT, "adapt_density: alpha must be between [0, 1]. ");
-  if (!(rel_tol > 0.0 && rel_tol < 1.0))
-    return fail(c, BBKDE_INVALID_ARGUMENT, "rel_tol must be in (0, 1)");
-  TRY(bbkde_unadapt_density(c));
-  PointSet &s = c->sets[BBKDE_REFERENCE];
-  if (alpha == 0 || s.n == 0) {
-    if (g_out) *g_out = NAN;
-    TRY(download(c, abw_out, s.abw, s.n));
-    TRY(download(c, mass_out, s.mass, s.n));
-    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
-    return BBKDE_OK;
-  }
-  const int64_t n = s.n;
+namespace {
+
+// Normalised culled self-sum of the REFERENCE set with its current attributes,
+// self term included: out[i] (device, the set's order) within rel of
+// sum_j m_j U(x_i, x_j), FP32-compensated. Queries are the set's own FP32
+// coordinates in Morton order. *pairs gets the pairs at tile granularity and
+// *ms the device time of the culled launch.
+int culled_self_sum(bbkde_ctx *c, const Resolved &r, double rel, double *out, double *pairs,
+                    float *ms) {
+  const int64_t n = c->sets[BBKDE_REFERENCE].n;
   TRY(ensure_culled(c, r));
   const void *qx = nullptr, *qy = nullptr;
   TRY(ensure_queries(c, BBKDE_REFERENCE, false, &qx, &qy));
@@ -1573,7 +1557,6 @@ extern "C" int bbkde_adapt_density_tol(bbkde_ctx *c, const bbkde_kernel_desc *k,
   TRY(ensure(c, c->cq_x, (size_t)n * sizeof(float)));
   TRY(ensure(c, c->cq_y, (size_t)n * sizeof(float)));
   TRY(ensure(c, c->cq_out, (size_t)std::max<int64_t>(n, kWlogBlocks) * sizeof(double)));
-  TRY(ensure(c, c->out_dev, (size_t)n * sizeof(double)));
   k_gather_xy<<<grid1d(n), 256, 0, c->stream>>>(fx, r.dim == 2 ? fy : nullptr, perm, n,
                                                 c->cq_x.as<float>(), c->cq_y.as<float>());
   COUNT_LAUNCH(c);
@@ -1584,21 +1567,75 @@ extern "C" int bbkde_adapt_density_tol(bbkde_ctx *c, const bbkde_kernel_desc *k,
   q.count = n;
   q.out = c->cq_out.as<double>();
   q.scale = r.norm;
-  double pairs = 0.0, ratio = 0.0;
+  double ratio = 0.0;
+  *pairs = 0.0;
   CUDA_TRY(c, cudaEventRecord(c->ev0, c->stream));
-  TRY(launch_culled(c, r, 0, (unsigned)((n + kCullQpb[0] - 1) / kCullQpb[0]), q, rel_tol, false,
-                    &pairs, &ratio));
+  TRY(launch_culled(c, r, 0, (unsigned)((n + kCullQpb[0] - 1) / kCullQpb[0]), q, rel, false,
+                    pairs, &ratio));
   CUDA_TRY(c, cudaEventRecord(c->ev1, c->stream));
+  k_scatter<<<grid1d(n), 256, 0, c->stream>>>(c->cq_out.as<double>(), perm, n, out);
+  COUNT_LAUNCH(c);
+  CUDA_TRY(c, cudaGetLastError());
+  CUDA_TRY(c, cudaEventSynchronize(c->ev1));
+  CUDA_TRY(c, cudaEventElapsedTime(ms, c->ev0, c->ev1));
+  return BBKDE_OK;
+}
+
+// FP64 sum over the set of w_i log(f_i - sub_i C) (mode 0) or w_i (f_i - sub_i C)
+// (mode 1), sub = null for no subtraction, in fixed order -> *dst (device).
+int wsum(bbkde_ctx *c, const double *f, const double *sub, double C, int mode, int64_t n,
+         double *dst) {
+  TRY(ensure(c, c->cq_out, (size_t)std::max<int64_t>(n, kWlogBlocks) * sizeof(double)));
+  k_wsum_partial<<<kWlogBlocks, 256, 0, c->stream>>>(
+      f, sub, C, c->sets[BBKDE_REFERENCE].weight.as<double>(), mode, n, c->cq_out.as<double>());
+  COUNT_LAUNCH(c);
+  k_sum_partials<<<1, kWlogBlocks, 0, c->stream>>>(c->cq_out.as<double>(), kWlogBlocks, dst);
+  COUNT_LAUNCH(c);
+  CUDA_TRY(c, cudaGetLastError());
+  return BBKDE_OK;
+}
+
+// Argument checks of the tolerance forms.
+int tol_checks(bbkde_ctx *c, const bbkde_kernel_desc *k, double rel_tol, Resolved &r) {
+  TRY(self_checks(c, k, BBKDE_FP32C, r));
+  TRY(culled_kernel_ok(c, r));
+  if (!(rel_tol > 0.0 && rel_tol < 1.0))
+    return fail(c, BBKDE_INVALID_ARGUMENT, "rel_tol must be in (0, 1)");
+  return BBKDE_OK;
+}
+
+}  // namespace
+
+// Adaptive densities with the pilot to a relative tolerance
+// (KernelDensity::adapt_density(alpha, rel, abs), KernelDensityImpl.h:291-359,
+// whose pilot the reference evaluates through its tree to rel / abs): the pilot
+// is the culled self-sum of the reference set (every value within rel_tol of
+// the full sum, self term included, FP32-compensated), the rest is
+// bbkde_adapt_density's FP64 epilogue.
+extern "C" int bbkde_adapt_density_tol(bbkde_ctx *c, const bbkde_kernel_desc *k, double alpha,
+                                       double rel_tol, double *abw_out, double *mass_out,
+                                       double *pilot_out, double *g_out) {
+  Resolved r;
+  TRY(tol_checks(c, k, rel_tol, r));
+  if (!(alpha >= 0 && alpha <= 1))   // KernelDensityImpl.h:301-303
+    return fail(c, BBKDE_INVALID_ARGUMENT, "adapt_density: alpha must be between [0, 1]. ");
+  TRY(bbkde_unadapt_density(c));
+  PointSet &s = c->sets[BBKDE_REFERENCE];
+  if (alpha == 0 || s.n == 0) {
+    if (g_out) *g_out = NAN;
+    TRY(download(c, abw_out, s.abw, s.n));
+    TRY(download(c, mass_out, s.mass, s.n));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return BBKDE_OK;
+  }
+  const int64_t n = s.n;
+  TRY(ensure(c, c->out_dev, (size_t)n * sizeof(double)));
   double *pilot = c->out_dev.as<double>();
-  k_scatter<<<grid1d(n), 256, 0, c->stream>>>(c->cq_out.as<double>(), perm, n, pilot);
-  COUNT_LAUNCH(c);
+  double pairs = 0.0;
+  float ms = 0.f;
+  TRY(culled_self_sum(c, r, rel_tol, pilot, &pairs, &ms));
   // g = exp(sum_i w_i log pilot_i) in FP64, fixed order (:330-337).
-  k_wlog_partial<<<kWlogBlocks, 256, 0, c->stream>>>(pilot, s.weight.as<double>(), n,
-                                                     c->cq_out.as<double>());
-  COUNT_LAUNCH(c);
-  k_sum_partials<<<1, kWlogBlocks, 0, c->stream>>>(c->cq_out.as<double>(), kWlogBlocks,
-                                                   c->scalars.as<double>());
-  COUNT_LAUNCH(c);
+  TRY(wsum(c, pilot, nullptr, 0.0, 0, n, c->scalars.as<double>()));
   k_pilot_finalize<<<grid1d(n), 256, 0, c->stream>>>(
       pilot, s.weight.as<double>(), c->scalars.as<double>(), alpha, r.dim, n,
       s.abw.as<double>(), s.mass.as<double>(), c->scalars.as<double>() + 1);
@@ -1613,11 +1650,71 @@ extern "C" int bbkde_adapt_density_tol(bbkde_ctx *c, const bbkde_kernel_desc *k,
                               cudaMemcpyDeviceToHost, c->stream));
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   if (g_out) *g_out = g;
-  float ms = 0.f;
-  CUDA_TRY(c, cudaEventElapsedTime(&ms, c->ev0, c->ev1));
   c->last_ms = ms;
   c->last_pairs = pairs;
   c->last_launches = 6;
+  return BBKDE_OK;
+}
+
+// Cross validation with the density sums to a relative tolerance, as the
+// reference evaluates them through its tree (likelihood_cross_validate,
+// KernelDensityImpl.h:215-252; lsq_convolution_cross_validate, :142-209): the
+// full self-sums are culled sums within rel_tol, and the leave-one-out value is
+// the full sum minus the self term m_i C(h), as the reference computes it.
+extern "C" int bbkde_likelihood_cv_tol(bbkde_ctx *c, const bbkde_kernel_desc *k, double rel_tol,
+                                       double *cv_out) {
+  Resolved r;
+  TRY(tol_checks(c, k, rel_tol, r));
+  if (!cv_out) return fail(c, BBKDE_INVALID_ARGUMENT, "cv_out is NULL");
+  PointSet &s = c->sets[BBKDE_REFERENCE];
+  if (s.n == 0) { *cv_out = 0.0; return BBKDE_OK; }
+  TRY(ensure(c, c->out_dev, (size_t)s.n * sizeof(double)));
+  double pairs = 0.0;
+  float ms = 0.f;
+  TRY(culled_self_sum(c, r, rel_tol, c->out_dev.as<double>(), &pairs, &ms));
+  // sum_i w_i log(f_i - m_i C) (:240-249)
+  TRY(wsum(c, c->out_dev.as<double>(), s.mass.as<double>(), r.norm, 0, s.n,
+           c->scalars.as<double>()));
+  CUDA_TRY(c, cudaMemcpyAsync(cv_out, c->scalars.p, sizeof(double), cudaMemcpyDeviceToHost,
+                              c->stream));
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  c->last_ms = ms;
+  c->last_pairs = pairs;
+  return BBKDE_OK;
+}
+
+extern "C" int bbkde_lsq_conv_cv_tol(bbkde_ctx *c, const bbkde_kernel_desc *k, double rel_tol,
+                                     double *cv_out) {
+  Resolved r;
+  TRY(tol_checks(c, k, rel_tol, r));
+  if (!cv_out) return fail(c, BBKDE_INVALID_ARGUMENT, "cv_out is NULL");
+  const int ck = conv_kind_of(k->kind, k->dim);
+  if (ck < 0)
+    return fail(c, BBKDE_UNSUPPORTED, "no convolution kernel is associated with this kernel");
+  bbkde_kernel_desc kc = *k;
+  kc.kind = ck;
+  Resolved rc;
+  TRY(resolve(c, &kc, rc));
+  TRY(culled_kernel_ok(c, rc));
+  PointSet &s = c->sets[BBKDE_REFERENCE];
+  if (s.n == 0) { *cv_out = 0.0; return BBKDE_OK; }
+  TRY(ensure(c, c->out_dev, (size_t)s.n * sizeof(double)));
+  double pairs = 0.0, pairs2 = 0.0;
+  float ms = 0.f, ms2 = 0.f;
+  double t[2];
+  // Leave-one-out term sum_i w_i (f_i - m_i C) (:162-181).
+  TRY(culled_self_sum(c, r, rel_tol, c->out_dev.as<double>(), &pairs, &ms));
+  TRY(wsum(c, c->out_dev.as<double>(), s.mass.as<double>(), r.norm, 1, s.n,
+           c->scalars.as<double>()));
+  // Square-integral term sum_i w_i f_conv(x_i), self term included (:187-205).
+  TRY(culled_self_sum(c, rc, rel_tol, c->out_dev.as<double>(), &pairs2, &ms2));
+  TRY(wsum(c, c->out_dev.as<double>(), nullptr, 0.0, 1, s.n, c->scalars.as<double>() + 1));
+  CUDA_TRY(c, cudaMemcpyAsync(t, c->scalars.p, 2 * sizeof(double), cudaMemcpyDeviceToHost,
+                              c->stream));
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  *cv_out = t[1] - 2.0 * t[0];   // :207
+  c->last_ms = ms + ms2;
+  c->last_pairs = pairs + pairs2;
   return BBKDE_OK;
 }
 

@@ -666,15 +666,21 @@ __global__ void k_pilot_finalize(const double *pilot, const double *w, const dou
   mass[i] = w[i] * pow(bw, (double)-dim);
 }
 
-// sum_i w_i log f_i over n values in kWlogBlocks fixed slices: one FP64 partial
-// per block (fixed-order tree within the block) -> part[blockIdx.x].
+// sum_i w_i log(v_i) (mode 0) or sum_i w_i v_i (mode 1), v_i = f_i - sub_i C
+// with sub_i rounded to FP32 (the mass the FP32 sums used; sub null: v_i = f_i),
+// over n values in kWlogBlocks fixed slices: one FP64 partial per block
+// (fixed-order tree within the block) -> part[blockIdx.x].
 constexpr int kWlogBlocks = 256;
-__global__ void k_wlog_partial(const double *f, const double *w, int64_t n, double *part) {
+__global__ void k_wsum_partial(const double *f, const double *sub, double C, const double *w,
+                               int mode, int64_t n, double *part) {
   __shared__ double s[256];
   const int64_t per = (n + gridDim.x - 1) / gridDim.x;
   const int64_t lo = (int64_t)blockIdx.x * per, hi = lo + per < n ? lo + per : n;
   double acc = 0.0;
-  for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) acc += w[i] * log(f[i]);
+  for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+    const double v = sub ? f[i] - (double)(float)sub[i] * C : f[i];
+    acc += w[i] * (mode == 0 ? log(v) : v);
+  }
   s[threadIdx.x] = acc;
   __syncthreads();
   for (int o = blockDim.x / 2; o > 0; o >>= 1) {

@@ -3,7 +3,7 @@
 //
 // No reference counterpart: the reference evaluates every query with a density
 // sum. The surrogate is trained on exact densities produced by the pair-sum
-// kernels and is judged against them (bbkde_surrogate_eval_grid).
+// kernels and is judged against them on dense grids (bbkde_eval_grid).
 #include <cuda_runtime.h>
 
 #include <algorithm>

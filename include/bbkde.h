@@ -187,6 +187,20 @@ BBKDE_API int bbkde_likelihood_cv(bbkde_ctx *ctx, const bbkde_kernel_desc *kerne
 BBKDE_API int bbkde_lsq_conv_cv(bbkde_ctx *ctx, const bbkde_kernel_desc *kernel, int precision,
                       double *cv_out);
 
+/* Cross validation with the density sums to a relative tolerance, as the
+ * reference evaluates them through its tree (likelihood_cross_validate,
+ * KernelDensityImpl.h:215-252; lsq_convolution_cross_validate, :142-209): every
+ * full self-sum is a culled sum within rel_tol (0 < rel_tol < 1) of the exact one
+ * (FP32-compensated), and the leave-one-out value is that sum minus the self term
+ * m_i C(h), as the reference computes it (its FP32 mass, so the subtraction
+ * cancels the self term of the sum). FP64 totals in fixed order. Kernels whose
+ * culled sum is unsupported (the Epanechnikov convolution kernels, hence the
+ * Epanechnikov product LSQ) give UNSUPPORTED. */
+BBKDE_API int bbkde_likelihood_cv_tol(bbkde_ctx *ctx, const bbkde_kernel_desc *kernel,
+                                      double rel_tol, double *cv_out);
+BBKDE_API int bbkde_lsq_conv_cv_tol(bbkde_ctx *ctx, const bbkde_kernel_desc *kernel,
+                                    double rel_tol, double *cv_out);
+
 /* ---- batched cross-validation -------------------------------------------- */
 
 typedef struct {
