@@ -15,9 +15,10 @@
 // increasing bandwidths) is one bbkde_cv_batch launch; the numerical-integration
 // form and the adaptive case run bbkde_lsq_numint_cv per bandwidth. Densities on
 // the plotting grid use the culled sum with the configured relative tolerance
-// (bbkde_eval_culled) where the reference uses its tree evaluation with the same
-// tolerance. The Kd-tree leaf sizes and the GPU block size are accepted and not
-// needed.
+// (bbkde_eval_culled) and the adaptive pilots a culled self-sum to that tolerance
+// (bbkde_adapt_density_tol), where the reference uses its tree evaluation with
+// the same tolerance. The Kd-tree leaf sizes and the GPU block size are accepted
+// and not needed.
 #include <chrono>
 #include <cmath>
 #include <cstdint>
@@ -150,6 +151,17 @@ struct Session {
     k.reserved = 0;
     return k;
   }
+  // Adaptive densities as the reference's adapt_density(alpha, rel_tol, abs_tol)
+  // (grid_search.cc:266-268, :508-510): the pilot to rel_tol when it lies in
+  // (0, 1), else the exact pilot.
+  void adapt(const bbkde_kernel_desc &k, double alpha, double rel_tol) {
+    if (rel_tol > 0 && rel_tol < 1)
+      check(bbkde_adapt_density_tol(ctx, &k, alpha, rel_tol, nullptr, nullptr, nullptr, nullptr),
+            ctx);
+    else
+      check(bbkde_adapt_density(ctx, &k, alpha, BBKDE_FP32C, nullptr, nullptr, nullptr, nullptr),
+            ctx);
+  }
   // Density at the grid points (x0..x1 by sx, y0..y1 by sy, ends included).
   std::vector<double> eval_grid(double bx, double by, double x0, double x1, int sx, double y0,
                                 double y1, int sy, double rel_tol) {
@@ -248,9 +260,7 @@ void run(const Options &o) {
     std::cout << "  alpha: " << alpha << "\n\n";
     const bbkde_kernel_desc k = s.kernel(base_bwx, base_bwy);
     t0 = Clock::now();
-    check(bbkde_adapt_density(s.ctx, &k, alpha, BBKDE_FP32C, nullptr, nullptr, nullptr,
-                              nullptr),
-          s.ctx);
+    s.adapt(k, alpha, rel_tol);
     std::cout << "  => running time: " << ms_since(t0) << " ms. \n\n";
   }
 
@@ -369,8 +379,7 @@ void run(const Options &o) {
             << "\n  alpha: " << alpha << "\n\n";
   const bbkde_kernel_desc kb = s.kernel(before_bwx, before_bwy);
   t0 = Clock::now();
-  check(bbkde_adapt_density(s.ctx, &kb, alpha, BBKDE_FP32C, nullptr, nullptr, nullptr, nullptr),
-        s.ctx);
+  s.adapt(kb, alpha, rel_tol);
   std::cout << "  => running time: " << ms_since(t0) << " ms. \n\n";
   double after_bwx = before_bwx, after_bwy = before_bwy;
   if (adaptive_cv) {
