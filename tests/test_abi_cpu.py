@@ -67,3 +67,36 @@ def test_ctx_create_without_device_reports_no_device():
     h = C.c_void_p()
     assert lib.bbkde_ctx_create(0, C.byref(h)) == bk.NO_DEVICE
     assert not h.value
+
+
+# Every ctypes mirror of a C struct of the header, by C name.
+MIRRORS = {"bbkde_kernel_desc": bk.KernelDesc, "bbkde_dataset": bk.Dataset,
+           "bbkde_train_config": bk.TrainConfig, "bbkde_cull_stats": bk.CullStats,
+           "bbkde_grid": bk.Grid, "bbkde_grid_config": bk.GridConfig,
+           "bbkde_grid_stats": bk.GridStats}
+
+
+def test_struct_layouts_match_header(tmp_path):
+    """The Python mirrors have the C structs' sizes and field offsets, as gcc lays
+    them out from include/bbkde.h (a field added on one side only shifts the
+    others and silently corrupts every call that passes the struct)."""
+    lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "bbkde.h"',
+             'int main(void) {']
+    for cname, py in MIRRORS.items():
+        lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for fname, _ in py._fields_:
+            lines.append(f'  printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines += ['  return 0;', '}']
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.check_call(["gcc", "-std=c99", "-I", os.path.join(ROOT, "include"), str(src),
+                           "-o", str(exe)])
+    got = {}
+    for line in subprocess.check_output([str(exe)], text=True).splitlines():
+        cname, key, value = line.split()
+        got[(cname, key)] = int(value)
+    for cname, py in MIRRORS.items():
+        assert got[(cname, "size")] == C.sizeof(py), cname
+        for fname, _ in py._fields_:
+            assert got[(cname, fname)] == getattr(py, fname).offset, (cname, fname)
