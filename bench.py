@@ -237,10 +237,18 @@ def cpu_reference_rate(wl, seconds: float, kind_pref: str = "reference"):
 
 
 def run_reference_arm(a, world, rank):
+    """The reference's own CPU direct_eval (oracle/_ref, all host threads) on the
+    headline workload (config 2, the default) or on plain-small (config 1). The
+    other workloads time their CPU baseline inside their own line."""
+    if a.workload not in ("direct", "plain-small"):
+        print(f"--impl reference times the direct and plain-small workloads; the "
+              f"{a.workload} line carries its own cpu_baseline", file=sys.stderr)
+        return 2
     if rank != 0:
         return 0
     from bbrcit_kde_b200 import workloads as W
-    wl = W.config2(n=a.n, m=a.m)
+    small = a.workload == "plain-small"
+    wl = W.config1() if small else W.config2(n=a.n, m=a.m)
     per_step = max(1.0, a.cpu_seconds / 4)
     rates = []
     base = None
@@ -253,10 +261,13 @@ def run_reference_arm(a, world, rank):
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
         "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
-        "ms_per_step": 2.0 * a.n * a.m / value * 1e3,
+        "ms_per_step": (len(wl.refs) * len(wl.queries) if small else 2.0 * a.n * a.m)
+        / value * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded splitmix64 bimodal mixture)",
-        "config": workload_config(a),
+        "config": ({"workload": "plain 2-D Gaussian, 10k bimodal refs, h=0.1, 100x100 grid "
+                                "on [-3,3)^2 (1e8 evals per call)"}
+                   if small else workload_config(a)),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": base["cores"],
                          "kind": base["kind"], "sample": base["sample"]},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},

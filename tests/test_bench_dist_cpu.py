@@ -55,3 +55,25 @@ def test_single_process_helpers():
     import bench
     assert bench.max_over_ranks(None, 12.5, "cpu") == 12.5
     assert bench.whole_job_rate(1e12, 3, 4, 1000.0) == pytest.approx(1.2e13)
+
+
+def test_reference_arm_line_and_workloads():
+    """--impl reference prints one JSON line with the contract's keys for the
+    workloads it times (the reference's own CPU direct_eval), and refuses, with a
+    message and a non-zero status, the workloads whose line carries its own
+    CPU baseline."""
+    import json
+    import subprocess
+    run = lambda *extra: subprocess.run(   # noqa: E731
+        [sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
+         "--warmup", "1", "--cpu-seconds", "1", *extra], capture_output=True, text=True,
+        timeout=600, cwd=ROOT)
+    r = run("--workload", "plain-small")
+    assert r.returncode == 0, r.stderr
+    line = json.loads([x for x in r.stdout.splitlines() if x.startswith("{")][-1])
+    assert line["impl"] == "reference" and line["value"] > 0
+    assert line["cpu_baseline"]["kind"] in ("reference", "port")
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 and "plain 2-D Gaussian" in \
+        line["config"]["workload"]
+    r = run("--workload", "cv-batch")
+    assert r.returncode == 2 and "own cpu_baseline" in r.stderr
