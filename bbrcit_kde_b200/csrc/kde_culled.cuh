@@ -47,7 +47,7 @@
 namespace bbkde {
 
 constexpr int kRefTile = 256;      // references per culling tile
-constexpr int kCullChunk = 1024;   // capacity of the per-round list of needed tiles
+constexpr int kCullChunk = 1024;   // capacity of the per-batch list of needed tiles
 constexpr int kGroupTiles = 16;    // tiles per tile group (two-level scan)
 
 struct RefTile {
@@ -162,12 +162,12 @@ __device__ __forceinline__ float cull_max(const CullArgs &a, float *s_red, Bound
   return e;
 }
 
-// Groups tested per round of cull_pass and the length of its tile list.
-__host__ __device__ constexpr int cull_groups_per_round(int block) {
+// Groups tested per batch of cull_pass and the length of its tile list.
+__host__ __device__ constexpr int cull_groups_per_batch(int block) {
   return block < kCullChunk / kGroupTiles ? block : kCullChunk / kGroupTiles;
 }
 __host__ __device__ constexpr int cull_list_len(int block) {
-  return cull_groups_per_round(block) * kGroupTiles;
+  return cull_groups_per_batch(block) * kGroupTiles;
 }
 
 // Block-wide ordered append: the threads with pred write value to dst[rank], rank
@@ -196,18 +196,18 @@ __device__ __forceinline__ int block_append(bool pred, int value, int *dst, int 
   return total;
 }
 
-// One culling pass over the tiles, two levels. Each round, thread tid < GR tests
+// One culling pass over the tiles, two levels. Each batch, thread tid < GR tests
 // one group (group_needed; it also books the bound of a group it skips); the
 // needed groups are listed in order (s_glist, GR entries), and the block then
 // tests their members in parallel (tile_needed), BLOCK at a time. The needed
-// tiles of the round are listed in ascending order in s_list[0, total) (capacity
+// tiles of the batch are listed in ascending order in s_list[0, total) (capacity
 // cull_list_len(BLOCK)) and handed to sum_list(total), which every thread calls.
 // Returns the number of tiles listed.
 template <int BLOCK, class GroupNeeded, class TileNeeded, class SumList>
 __device__ __forceinline__ int cull_pass(const CullArgs &a, int *s_list, int *s_glist, int *s_wc,
                                          GroupNeeded group_needed, TileNeeded tile_needed,
                                          SumList sum_list) {
-  constexpr int GR = cull_groups_per_round(BLOCK);
+  constexpr int GR = cull_groups_per_batch(BLOCK);
   const int tid = threadIdx.x;
   int summed = 0;
   for (int g0 = 0; g0 < a.n_groups; g0 += GR) {
@@ -243,7 +243,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_pair_sum_culled(CullArgs a) {
   __shared__ float4 s_r1[kRefTile];
   __shared__ float4 s_r2[kExt ? kRefTile : 1];
   __shared__ int s_list[cull_list_len(BLOCK)];
-  __shared__ int s_glist[cull_groups_per_round(BLOCK)];
+  __shared__ int s_glist[cull_groups_per_batch(BLOCK)];
   __shared__ int s_wc[NW];
   __shared__ float s_box[QPT][4];     // slot boxes
   __shared__ float s_th[QPT];         // slot thresholds T_k

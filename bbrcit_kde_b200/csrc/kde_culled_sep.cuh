@@ -84,7 +84,7 @@ __global__ void __launch_bounds__(T *T / 8, T == 32 ? 4 : 16)
   __shared__ __align__(16) float2 s_fac[2 * FBUF];
   __shared__ float s_qx[T], s_qy[T];
   __shared__ int s_list[cull_list_len(BLOCK)];
-  __shared__ int s_glist[cull_groups_per_round(BLOCK)];
+  __shared__ int s_glist[cull_groups_per_batch(BLOCK)];
   __shared__ int s_wc[NW];
   __shared__ float s_box[NS][4];
   __shared__ float s_th[NS];
