@@ -43,6 +43,7 @@ EXPORTED = [
     "bbkde_surrogate_load", "bbkde_surrogate_set_inference", "bbkde_eval_culled",
     "bbkde_eval_grid", "bbkde_lsq_numint_cv", "bbkde_surrogate_set_engine",
     "bbkde_adapt_density_tol", "bbkde_likelihood_cv_tol", "bbkde_lsq_conv_cv_tol",
+    "bbkde_eval_tol", "bbkde_cv_batch_counts",
 ]
 
 # Surrogate inference engines (bbkde_surrogate_set_engine).
@@ -159,10 +160,10 @@ def load_library(path: str = LIB_PATH):
     lib.bbkde_eval_range_device.argtypes = [vp, kd, i64, i64, i64, i64, C.c_int, C.c_int, vp,
                                             i64]
     lib.bbkde_adapt_density.argtypes = [vp, kd, C.c_double, C.c_int, _dp, _dp, _dp, _dp]
-    lib.bbkde_adapt_density_tol.argtypes = [vp, kd, C.c_double, C.c_double, _dp, _dp, _dp,
-                                            _dp]
-    lib.bbkde_likelihood_cv_tol.argtypes = [vp, kd, C.c_double, _dp]
-    lib.bbkde_lsq_conv_cv_tol.argtypes = [vp, kd, C.c_double, _dp]
+    lib.bbkde_adapt_density_tol.argtypes = [vp, kd, C.c_double, C.c_double, C.c_double, _dp,
+                                            _dp, _dp, _dp]
+    lib.bbkde_likelihood_cv_tol.argtypes = [vp, kd, C.c_double, C.c_double, _dp]
+    lib.bbkde_lsq_conv_cv_tol.argtypes = [vp, kd, C.c_double, C.c_double, _dp]
     lib.bbkde_unadapt_density.argtypes = [vp]
     lib.bbkde_likelihood_cv.argtypes = [vp, kd, C.c_int, _dp]
     lib.bbkde_lsq_conv_cv.argtypes = [vp, kd, C.c_int, _dp]
@@ -194,6 +195,9 @@ def load_library(path: str = LIB_PATH):
     lib.bbkde_surrogate_set_engine.argtypes = [vp, C.c_int]
     lib.bbkde_eval_culled.argtypes = [vp, kd, C.c_int, C.c_double, vp, C.c_int,
                                       C.POINTER(CullStats)]
+    lib.bbkde_cv_batch_counts.argtypes = [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+    lib.bbkde_eval_tol.argtypes = [vp, kd, C.c_int, C.c_double, C.c_double, vp, C.c_int,
+                                   C.POINTER(CullStats)]
     lib.bbkde_eval_grid.argtypes = [vp, vp, kd, C.POINTER(Grid), C.POINTER(GridConfig), vp,
                                     C.POINTER(GridStats)]
     lib.bbkde_lsq_numint_cv.argtypes = [vp, kd, C.POINTER(Grid), C.c_int, _dp]
@@ -302,17 +306,20 @@ class Context:
                                                  _p(abw), _p(mass), _p(pilot), _p(g)))
         return abw[:n], mass[:n], pilot[:n], float(g[0])
 
-    def adapt_density_tol(self, desc: KernelDesc, alpha: float, rel_tol=1e-6, outputs=True):
-        """adapt_density with the pilot to rel_tol (culled self-sum); same returns."""
+    def adapt_density_tol(self, desc: KernelDesc, alpha: float, rel_tol=1e-6, abs_tol=0.0,
+                          outputs=True):
+        """adapt_density with the pilot to max(rel_tol f, abs_tol) (culled self-sum);
+        same returns."""
         if not outputs:
             self._check(self.lib.bbkde_adapt_density_tol(self.h, C.byref(desc), alpha, rel_tol,
-                                                         None, None, None, None))
+                                                         abs_tol, None, None, None, None))
             return None
         n = self.size(REFERENCE)
         abw, mass, pilot, g = np.empty(max(n, 1)), np.empty(max(n, 1)), np.empty(max(n, 1)), \
             np.zeros(1)
         self._check(self.lib.bbkde_adapt_density_tol(self.h, C.byref(desc), alpha, rel_tol,
-                                                     _p(abw), _p(mass), _p(pilot), _p(g)))
+                                                     abs_tol, _p(abw), _p(mass), _p(pilot),
+                                                     _p(g)))
         return abw[:n], mass[:n], pilot[:n], float(g[0])
 
     def unadapt_density(self):
@@ -323,16 +330,18 @@ class Context:
         self._check(self.lib.bbkde_likelihood_cv(self.h, C.byref(desc), precision, _p(cv)))
         return float(cv[0])
 
-    def likelihood_cv_tol(self, desc: KernelDesc, rel_tol=1e-6) -> float:
-        """Likelihood CV with the density sums to rel_tol (culled self-sums)."""
+    def likelihood_cv_tol(self, desc: KernelDesc, rel_tol=1e-6, abs_tol=0.0) -> float:
+        """Likelihood CV with the density sums to max(rel_tol f, abs_tol) (culled)."""
         cv = np.zeros(1)
-        self._check(self.lib.bbkde_likelihood_cv_tol(self.h, C.byref(desc), rel_tol, _p(cv)))
+        self._check(self.lib.bbkde_likelihood_cv_tol(self.h, C.byref(desc), rel_tol, abs_tol,
+                                                     _p(cv)))
         return float(cv[0])
 
-    def lsq_conv_cv_tol(self, desc: KernelDesc, rel_tol=1e-6) -> float:
-        """LSQ convolution CV with the density sums to rel_tol (culled self-sums)."""
+    def lsq_conv_cv_tol(self, desc: KernelDesc, rel_tol=1e-6, abs_tol=0.0) -> float:
+        """LSQ convolution CV with the density sums to max(rel_tol f, abs_tol) (culled)."""
         cv = np.zeros(1)
-        self._check(self.lib.bbkde_lsq_conv_cv_tol(self.h, C.byref(desc), rel_tol, _p(cv)))
+        self._check(self.lib.bbkde_lsq_conv_cv_tol(self.h, C.byref(desc), rel_tol, abs_tol,
+                                                   _p(cv)))
         return float(cv[0])
 
     def lsq_conv_cv(self, desc: KernelDesc, precision=FP32C) -> float:
@@ -371,6 +380,12 @@ class Context:
                                             _p(hy), precision, _p(lik), _p(lsq)))
         return lik[:n], lsq[:n]
 
+    def cv_batch_counts(self):
+        """(likelihood pairs, convolution pairs) in support in the last cv_batch."""
+        a, b = C.c_int64(0), C.c_int64(0)
+        self._check(self.lib.bbkde_cv_batch_counts(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
     def eval_culled(self, desc: KernelDesc, rel_tol=1e-7, normalized=True):
         """Culled direct evaluation of every query; returns (values, CullStats)."""
         n = self.size(QUERY)
@@ -378,6 +393,16 @@ class Context:
         st = CullStats()
         self._check(self.lib.bbkde_eval_culled(self.h, C.byref(desc), int(normalized), rel_tol,
                                                out.ctypes.data, 0, C.byref(st)))
+        return out[:n], st
+
+    def eval_tol(self, desc: KernelDesc, rel_err=1e-6, abs_err=1e-8, normalized=True):
+        """bbkde_eval_tol: every query within max(rel_err f, abs_err) / 2 of the full
+        sum (the reference's eval(queries, rel_err, abs_err)); (values, CullStats)."""
+        n = self.size(QUERY)
+        out = np.empty(max(n, 1))
+        st = CullStats()
+        self._check(self.lib.bbkde_eval_tol(self.h, C.byref(desc), int(normalized), rel_err,
+                                            abs_err, out.ctypes.data, 0, C.byref(st)))
         return out[:n], st
 
     def eval_grid(self, desc: KernelDesc, grid, out_ptr: int, surrogate=None,

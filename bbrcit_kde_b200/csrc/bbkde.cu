@@ -116,6 +116,7 @@ struct bbkde_ctx {
       cv_part, cv_hist, cv_out, cv_parts;
   cudaGraphExec_t cv_graph = nullptr;
   std::vector<uint64_t> cv_graph_key;
+  int64_t cv_counts[2] = {0, 0};   // in-support pairs of the last batched CV launch
   // culled evaluation: sorted references, sort scratch, sorted queries, per-block
   // bounds; dense-grid pipeline buffers
   CullCache cull;
@@ -1226,6 +1227,7 @@ extern "C" int bbkde_cv_batch(bbkde_ctx *c, int kind, int n_sets, const bbkde_da
   a.r_conv = 8;
   a.epan_part = c->cv_part.as<double>();
   a.conv_hist = c->cv_hist.as<double>();
+  a.pairs = reinterpret_cast<unsigned long long *>(c->cv_counter.as<char>() + 16);
   double *lik_dev = c->cv_out.as<double>();
   double *lsq_dev = lik_dev + nout;
   const int *pbeg = c->cv_parts.as<int>();
@@ -1242,7 +1244,7 @@ extern "C" int bbkde_cv_batch(bbkde_ctx *c, int kind, int n_sets, const bbkde_da
       (uint64_t)n_hy, (uint64_t)(uintptr_t)c->stream,
       (uint64_t)(uintptr_t)a.lutx, (uint64_t)basex, (uint64_t)basey, (uint64_t)lut_shift};
   auto enqueue = [&]() -> cudaError_t {
-    cudaError_t e = cudaMemsetAsync(a.counter, 0, sizeof(int), c->stream);
+    cudaError_t e = cudaMemsetAsync(a.counter, 0, 32, c->stream);   // work counter + pairs
     if (e != cudaSuccess) return e;
     e = cudaMemsetAsync(a.conv_hist, 0, (size_t)n_sets * 16 * kCvCells * sizeof(double),
                         c->stream);
@@ -1285,12 +1287,25 @@ extern "C" int bbkde_cv_batch(bbkde_ctx *c, int kind, int n_sets, const bbkde_da
                               c->stream));
   CUDA_TRY(c, cudaMemcpyAsync(lsq_out, lsq_dev, nout * sizeof(double), cudaMemcpyDeviceToHost,
                               c->stream));
+  unsigned long long counts[2] = {0, 0};
+  CUDA_TRY(c, cudaMemcpyAsync(counts, a.pairs, sizeof(counts), cudaMemcpyDeviceToHost,
+                              c->stream));
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   float ms = 0.f;
   CUDA_TRY(c, cudaEventElapsedTime(&ms, c->ev0, c->ev1));
   c->last_ms = ms;
   c->last_pairs = sum_pairs;
   c->last_launches = 2;
+  c->cv_counts[0] = (int64_t)counts[0];
+  c->cv_counts[1] = (int64_t)(counts[1] / 4);   // each x-power group counts every pair
+  return BBKDE_OK;
+}
+
+extern "C" int bbkde_cv_batch_counts(const bbkde_ctx *c, int64_t *lik_pairs,
+                                     int64_t *conv_pairs) {
+  if (!c) return BBKDE_INVALID_ARGUMENT;
+  if (lik_pairs) *lik_pairs = c->cv_counts[0];
+  if (conv_pairs) *conv_pairs = c->cv_counts[1];
   return BBKDE_OK;
 }
 
@@ -1404,9 +1419,12 @@ void launch_cull_sep(int tile, unsigned nblk, cudaStream_t st, const CullArgs &a
 // statistics (pairs at tile granularity, worst bound ratio) to *pairs, *ratio.
 // sep_tile > 0: grid-tile blocks of sep_tile^2 points in the factored form
 // (k_pair_sum_culled_sep); the operator must factor over the axes.
+// abs_n > 0 adds an absolute allowance (unnormalised units): a query's skipped
+// part stays below max(rel * S, abs_n) / 2, and *ratio is then the worst skipped
+// bound over that allowance; with abs_n = 0 it is the worst bound over S.
 int launch_culled(bbkde_ctx *c, const Resolved &r, int shape, unsigned nblk,
                   const CullQueries &q, double rel, bool full, double *pairs, double *ratio,
-                  int sep_tile = 0) {
+                  int sep_tile = 0, double abs_n = 0.0) {
   if (nblk == 0) return BBKDE_OK;
   TRY(ensure(c, c->cb_bound, (size_t)nblk * sizeof(double)));
   TRY(ensure(c, c->cb_smin, (size_t)nblk * sizeof(double)));
@@ -1422,6 +1440,7 @@ int launch_culled(bbkde_ctx *c, const Resolved &r, int shape, unsigned nblk,
   a.n_ref = c->sets[BBKDE_REFERENCE].n;
   a.cut = full ? INFINITY : kCullCut;
   a.rel = rel;
+  a.abs_n = abs_n;
   a.q = q;
   a.blk_bound = c->cb_bound.as<double>();
   a.blk_smin = c->cb_smin.as<double>();
@@ -1456,7 +1475,7 @@ int launch_culled(bbkde_ctx *c, const Resolved &r, int shape, unsigned nblk,
   CUDA_TRY(c, cudaMemcpyAsync(st, c->cb_stats.p, sizeof(st), cudaMemcpyDeviceToHost, c->stream));
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   if (pairs) *pairs += st[1] * kRefTile * kCullQpb[shape];
-  if (ratio) *ratio = std::max(*ratio, st[0]);
+  if (ratio) *ratio = std::max(*ratio, abs_n > 0.0 ? st[0] : st[0] * rel);
   return BBKDE_OK;
 }
 
@@ -1469,16 +1488,17 @@ int culled_kernel_ok(bbkde_ctx *c, const Resolved &r) {
 
 }  // namespace
 
-extern "C" int bbkde_eval_culled(bbkde_ctx *c, const bbkde_kernel_desc *k, int normalized,
-                                 double rel_tol, double *out, int out_on_device,
-                                 bbkde_cull_stats *stats) {
-  TRY(check_ctx(c));
-  if (!out) return fail(c, BBKDE_INVALID_ARGUMENT, "output pointer is NULL");
-  if (!(rel_tol > 0.0 && rel_tol < 1.0))
-    return fail(c, BBKDE_INVALID_ARGUMENT, "rel_tol must be in (0, 1)");
+namespace {
+
+// The culled evaluation of the QUERY set with a relative tolerance rel and an
+// absolute one abs_err (normalised density units, as the reference's abs_err).
+int eval_culled_impl(bbkde_ctx *c, const bbkde_kernel_desc *k, int normalized, double rel_tol,
+                     double abs_err, double *out, int out_on_device, bbkde_cull_stats *stats) {
   Resolved r;
   TRY(resolve(c, k, r));
   TRY(culled_kernel_ok(c, r));
+  // the tree scales abs_err by 1 / C(h) for its unnormalised sums (:723-729)
+  const double abs_n = abs_err > 0.0 ? abs_err / r.norm : 0.0;
   const PointSet &rs = c->sets[BBKDE_REFERENCE], &qs = c->sets[BBKDE_QUERY];
   if ((rs.n > 0 && rs.dim != r.dim) || (qs.n > 0 && qs.dim != r.dim))
     return fail(c, BBKDE_INVALID_ARGUMENT, "point dimension does not match the kernel");
@@ -1517,7 +1537,8 @@ extern "C" int bbkde_eval_culled(bbkde_ctx *c, const bbkde_kernel_desc *k, int n
     q.scale = normalized ? r.norm : 1.0;
     const unsigned nblk = (unsigned)((nq + kCullQpb[0] - 1) / kCullQpb[0]);
     CUDA_TRY(c, cudaEventRecord(c->ev0, c->stream));
-    TRY(launch_culled(c, r, 0, nblk, q, rel_tol, false, &st.pairs, &st.max_bound_ratio));
+    TRY(launch_culled(c, r, 0, nblk, q, rel_tol, false, &st.pairs, &st.max_bound_ratio, 0,
+                      abs_n));
     CUDA_TRY(c, cudaEventRecord(c->ev1, c->stream));
     k_scatter<<<grid1d(nq), 256, 0, c->stream>>>(c->cq_out.as<double>(), perm, nq, dst);
     COUNT_LAUNCH(c);
@@ -1538,15 +1559,39 @@ extern "C" int bbkde_eval_culled(bbkde_ctx *c, const bbkde_kernel_desc *k, int n
   return BBKDE_OK;
 }
 
+}  // namespace
+
+extern "C" int bbkde_eval_culled(bbkde_ctx *c, const bbkde_kernel_desc *k, int normalized,
+                                 double rel_tol, double *out, int out_on_device,
+                                 bbkde_cull_stats *stats) {
+  TRY(check_ctx(c));
+  if (!out) return fail(c, BBKDE_INVALID_ARGUMENT, "output pointer is NULL");
+  if (!(rel_tol > 0.0 && rel_tol < 1.0))
+    return fail(c, BBKDE_INVALID_ARGUMENT, "rel_tol must be in (0, 1)");
+  return eval_culled_impl(c, k, normalized, rel_tol, 0.0, out, out_on_device, stats);
+}
+
+extern "C" int bbkde_eval_tol(bbkde_ctx *c, const bbkde_kernel_desc *k, int normalized,
+                              double rel_err, double abs_err, double *out, int out_on_device,
+                              bbkde_cull_stats *stats) {
+  TRY(check_ctx(c));
+  if (!out) return fail(c, BBKDE_INVALID_ARGUMENT, "output pointer is NULL");
+  if (!(rel_err >= 0.0 && rel_err < 1.0) || !(abs_err >= 0.0) || !std::isfinite(abs_err))
+    return fail(c, BBKDE_INVALID_ARGUMENT,
+                "need 0 <= rel_err < 1 and a finite abs_err >= 0");
+  return eval_culled_impl(c, k, normalized, rel_err, abs_err, out, out_on_device, stats);
+}
+
 namespace {
 
 // Normalised culled self-sum of the REFERENCE set with its current attributes,
-// self term included: out[i] (device, the set's order) within rel of
-// sum_j m_j U(x_i, x_j), FP32-compensated. Queries are the set's own FP32
+// self term included: out[i] (device, the set's order) within max(rel * f_i,
+// abs_err) / 2 of f_i = C sum_j m_j U(x_i, x_j) (abs_err in normalised density
+// units), FP32-compensated. Queries are the set's own FP32
 // coordinates in Morton order. *pairs gets the pairs at tile granularity and
 // *ms the device time of the culled launch.
-int culled_self_sum(bbkde_ctx *c, const Resolved &r, double rel, double *out, double *pairs,
-                    float *ms) {
+int culled_self_sum(bbkde_ctx *c, const Resolved &r, double rel, double abs_err, double *out,
+                    double *pairs, float *ms) {
   const int64_t n = c->sets[BBKDE_REFERENCE].n;
   TRY(ensure_culled(c, r));
   const void *qx = nullptr, *qy = nullptr;
@@ -1571,7 +1616,7 @@ int culled_self_sum(bbkde_ctx *c, const Resolved &r, double rel, double *out, do
   *pairs = 0.0;
   CUDA_TRY(c, cudaEventRecord(c->ev0, c->stream));
   TRY(launch_culled(c, r, 0, (unsigned)((n + kCullQpb[0] - 1) / kCullQpb[0]), q, rel, false,
-                    pairs, &ratio));
+                    pairs, &ratio, 0, abs_err > 0.0 ? abs_err / r.norm : 0.0));
   CUDA_TRY(c, cudaEventRecord(c->ev1, c->stream));
   k_scatter<<<grid1d(n), 256, 0, c->stream>>>(c->cq_out.as<double>(), perm, n, out);
   COUNT_LAUNCH(c);
@@ -1595,28 +1640,31 @@ int wsum(bbkde_ctx *c, const double *f, const double *sub, double C, int mode, i
   return BBKDE_OK;
 }
 
-// Argument checks of the tolerance forms.
-int tol_checks(bbkde_ctx *c, const bbkde_kernel_desc *k, double rel_tol, Resolved &r) {
+// Argument checks of the tolerance forms: 0 <= rel_tol < 1, finite abs_tol >= 0
+// (both 0: every tile that does not flush to zero is summed).
+int tol_checks(bbkde_ctx *c, const bbkde_kernel_desc *k, double rel_tol, double abs_tol,
+               Resolved &r) {
   TRY(self_checks(c, k, BBKDE_FP32C, r));
   TRY(culled_kernel_ok(c, r));
-  if (!(rel_tol > 0.0 && rel_tol < 1.0))
-    return fail(c, BBKDE_INVALID_ARGUMENT, "rel_tol must be in (0, 1)");
+  if (!(rel_tol >= 0.0 && rel_tol < 1.0) || !(abs_tol >= 0.0) || !std::isfinite(abs_tol))
+    return fail(c, BBKDE_INVALID_ARGUMENT,
+                "tolerances: need 0 <= rel_tol < 1 and a finite abs_tol >= 0");
   return BBKDE_OK;
 }
 
 }  // namespace
 
-// Adaptive densities with the pilot to a relative tolerance
-// (KernelDensity::adapt_density(alpha, rel, abs), KernelDensityImpl.h:291-359,
-// whose pilot the reference evaluates through its tree to rel / abs): the pilot
-// is the culled self-sum of the reference set (every value within rel_tol of
-// the full sum, self term included, FP32-compensated), the rest is
+// Adaptive densities with the pilot to a tolerance (KernelDensity::adapt_density
+// (alpha, rel, abs), KernelDensityImpl.h:291-359, whose pilot the reference
+// evaluates through its tree to rel / abs): the pilot is the culled self-sum of
+// the reference set (every value within max(rel_tol f, abs_tol) / 2 of the full
+// sum f, self term included, FP32-compensated), the rest is
 // bbkde_adapt_density's FP64 epilogue.
 extern "C" int bbkde_adapt_density_tol(bbkde_ctx *c, const bbkde_kernel_desc *k, double alpha,
-                                       double rel_tol, double *abw_out, double *mass_out,
-                                       double *pilot_out, double *g_out) {
+                                       double rel_tol, double abs_tol, double *abw_out,
+                                       double *mass_out, double *pilot_out, double *g_out) {
   Resolved r;
-  TRY(tol_checks(c, k, rel_tol, r));
+  TRY(tol_checks(c, k, rel_tol, abs_tol, r));
   if (!(alpha >= 0 && alpha <= 1))   // KernelDensityImpl.h:301-303
     return fail(c, BBKDE_INVALID_ARGUMENT, "adapt_density: alpha must be between [0, 1]. ");
   TRY(bbkde_unadapt_density(c));
@@ -1633,7 +1681,7 @@ extern "C" int bbkde_adapt_density_tol(bbkde_ctx *c, const bbkde_kernel_desc *k,
   double *pilot = c->out_dev.as<double>();
   double pairs = 0.0;
   float ms = 0.f;
-  TRY(culled_self_sum(c, r, rel_tol, pilot, &pairs, &ms));
+  TRY(culled_self_sum(c, r, rel_tol, abs_tol, pilot, &pairs, &ms));
   // g = exp(sum_i w_i log pilot_i) in FP64, fixed order (:330-337).
   TRY(wsum(c, pilot, nullptr, 0.0, 0, n, c->scalars.as<double>()));
   k_pilot_finalize<<<grid1d(n), 256, 0, c->stream>>>(
@@ -1656,22 +1704,23 @@ extern "C" int bbkde_adapt_density_tol(bbkde_ctx *c, const bbkde_kernel_desc *k,
   return BBKDE_OK;
 }
 
-// Cross validation with the density sums to a relative tolerance, as the
-// reference evaluates them through its tree (likelihood_cross_validate,
+// Cross validation with the density sums to a tolerance, as the reference
+// evaluates them through its tree (likelihood_cross_validate,
 // KernelDensityImpl.h:215-252; lsq_convolution_cross_validate, :142-209): the
-// full self-sums are culled sums within rel_tol, and the leave-one-out value is
-// the full sum minus the self term m_i C(h), as the reference computes it.
+// full self-sums are culled sums within max(rel_tol f, abs_tol) / 2, and the
+// leave-one-out value is the full sum minus the self term m_i C(h), as the
+// reference computes it.
 extern "C" int bbkde_likelihood_cv_tol(bbkde_ctx *c, const bbkde_kernel_desc *k, double rel_tol,
-                                       double *cv_out) {
+                                       double abs_tol, double *cv_out) {
   Resolved r;
-  TRY(tol_checks(c, k, rel_tol, r));
+  TRY(tol_checks(c, k, rel_tol, abs_tol, r));
   if (!cv_out) return fail(c, BBKDE_INVALID_ARGUMENT, "cv_out is NULL");
   PointSet &s = c->sets[BBKDE_REFERENCE];
   if (s.n == 0) { *cv_out = 0.0; return BBKDE_OK; }
   TRY(ensure(c, c->out_dev, (size_t)s.n * sizeof(double)));
   double pairs = 0.0;
   float ms = 0.f;
-  TRY(culled_self_sum(c, r, rel_tol, c->out_dev.as<double>(), &pairs, &ms));
+  TRY(culled_self_sum(c, r, rel_tol, abs_tol, c->out_dev.as<double>(), &pairs, &ms));
   // sum_i w_i log(f_i - m_i C) (:240-249)
   TRY(wsum(c, c->out_dev.as<double>(), s.mass.as<double>(), r.norm, 0, s.n,
            c->scalars.as<double>()));
@@ -1684,9 +1733,9 @@ extern "C" int bbkde_likelihood_cv_tol(bbkde_ctx *c, const bbkde_kernel_desc *k,
 }
 
 extern "C" int bbkde_lsq_conv_cv_tol(bbkde_ctx *c, const bbkde_kernel_desc *k, double rel_tol,
-                                     double *cv_out) {
+                                     double abs_tol, double *cv_out) {
   Resolved r;
-  TRY(tol_checks(c, k, rel_tol, r));
+  TRY(tol_checks(c, k, rel_tol, abs_tol, r));
   if (!cv_out) return fail(c, BBKDE_INVALID_ARGUMENT, "cv_out is NULL");
   const int ck = conv_kind_of(k->kind, k->dim);
   if (ck < 0)
@@ -1703,11 +1752,11 @@ extern "C" int bbkde_lsq_conv_cv_tol(bbkde_ctx *c, const bbkde_kernel_desc *k, d
   float ms = 0.f, ms2 = 0.f;
   double t[2];
   // Leave-one-out term sum_i w_i (f_i - m_i C) (:162-181).
-  TRY(culled_self_sum(c, r, rel_tol, c->out_dev.as<double>(), &pairs, &ms));
+  TRY(culled_self_sum(c, r, rel_tol, abs_tol, c->out_dev.as<double>(), &pairs, &ms));
   TRY(wsum(c, c->out_dev.as<double>(), s.mass.as<double>(), r.norm, 1, s.n,
            c->scalars.as<double>()));
   // Square-integral term sum_i w_i f_conv(x_i), self term included (:187-205).
-  TRY(culled_self_sum(c, rc, rel_tol, c->out_dev.as<double>(), &pairs2, &ms2));
+  TRY(culled_self_sum(c, rc, rel_tol, abs_tol, c->out_dev.as<double>(), &pairs2, &ms2));
   TRY(wsum(c, c->out_dev.as<double>(), nullptr, 0.0, 1, s.n, c->scalars.as<double>() + 1));
   CUDA_TRY(c, cudaMemcpyAsync(t, c->scalars.p, 2 * sizeof(double), cudaMemcpyDeviceToHost,
                               c->stream));
@@ -2171,10 +2220,6 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratch
 
 namespace {
 
-constexpr int kNoAllocMaxDevices = 64;
-std::mutex g_noalloc_mu;
-void *g_noalloc_addr[kNoAllocMaxDevices] = {};
-
 void noalloc_msg(char *buf, int64_t len, const char *fmt, ...) {
   if (!buf || len <= 0) return;
   va_list ap;
@@ -2185,25 +2230,20 @@ void noalloc_msg(char *buf, int64_t len, const char *fmt, ...) {
 
 inline size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
 
-// Device address of g_noalloc_scratch on `device` (which must be current),
-// resolved on the first call for that device and cached afterwards.
-int noalloc_scratch(int device, void **out, char *err, int64_t errlen) {
-  if (device < 0 || device >= kNoAllocMaxDevices) {
-    noalloc_msg(err, errlen, "device ordinal %d not supported", device);
-    return BBKDE_INVALID_ARGUMENT;
+// Device address of g_noalloc_scratch in the current context. Resolved on every
+// call (a lookup once the module is loaded), so a device reset or a different
+// current context never leaves a stale pointer behind. The first resolution on a
+// device loads the library's module there (CUDA loads modules lazily), which
+// places the array in that device's memory.
+int noalloc_scratch(void **out, char *err, int64_t errlen) {
+  void *p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess || !p) {
+    noalloc_msg(err, errlen, "cudaGetSymbolAddress(scratch): %s", cudaGetErrorString(e));
+    cudaGetLastError();
+    return BBKDE_CUDA_ERROR;
   }
-  std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_addr[device]) {
-    void *p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || !p) {
-      noalloc_msg(err, errlen, "cudaGetSymbolAddress(scratch): %s", cudaGetErrorString(e));
-      cudaGetLastError();
-      return BBKDE_CUDA_ERROR;
-    }
-    g_noalloc_addr[device] = p;
-  }
-  *out = g_noalloc_addr[device];
+  *out = p;
   return BBKDE_OK;
 }
 
@@ -2226,10 +2266,30 @@ extern "C" int bbkde_eval_noalloc(const bbkde_kernel_desc *kernel, int64_t n_ref
     noalloc_msg(errbuf, errbuf_len, "need n_ref >= 1 and n_query >= 0");
     return BBKDE_INVALID_ARGUMENT;
   }
+  // Resolve the scratch before anything else, so that a call with no queries loads
+  // the array on this device (a cheap warm-up before capture or memory pressure).
+  int device = 0;
+  cudaError_t e = cudaGetDevice(&device);
+  if (e != cudaSuccess) {
+    noalloc_msg(errbuf, errbuf_len, "cudaGetDevice: %s", cudaGetErrorString(e));
+    return BBKDE_CUDA_ERROR;
+  }
+  void *base = nullptr;
+  int rc = noalloc_scratch(&base, errbuf, errbuf_len);
+  if (rc != BBKDE_OK) return rc;
   if (n_query == 0) return BBKDE_OK;
   if (!ref_x || !ref_mass || !query_x || !out || (dim == 2 && (!ref_y || !query_y))) {
     noalloc_msg(errbuf, errbuf_len, "a required device pointer is NULL");
     return BBKDE_INVALID_ARGUMENT;
+  }
+  // Bound the counts before any byte arithmetic, so that no product can wrap.
+  if (n_ref > (int64_t)(kNoAllocScratchBytes / 16) ||
+      n_query > (int64_t)(kNoAllocScratchBytes / 12)) {
+    noalloc_msg(errbuf, errbuf_len,
+                "n_ref = %lld or n_query = %lld exceeds the %zu bytes of scratch of the "
+                "allocation-free entry point; use bbkde_eval_range for larger problems",
+                (long long)n_ref, (long long)n_query, kNoAllocScratchBytes);
+    return BBKDE_OUT_OF_RANGE;
   }
   // Scratch layout: records | extra column | query x | query y | partials.
   const bool ext = op_has_extra(r.op);
@@ -2248,15 +2308,6 @@ extern "C" int bbkde_eval_noalloc(const bbkde_kernel_desc *kernel, int64_t n_ref
                 kNoAllocScratchBytes);
     return BBKDE_OUT_OF_RANGE;
   }
-  int device = 0;
-  cudaError_t e = cudaGetDevice(&device);
-  if (e != cudaSuccess) {
-    noalloc_msg(errbuf, errbuf_len, "cudaGetDevice: %s", cudaGetErrorString(e));
-    return BBKDE_CUDA_ERROR;
-  }
-  void *base = nullptr;
-  int rc = noalloc_scratch(device, &base, errbuf, errbuf_len);
-  if (rc != BBKDE_OK) return rc;
   unsigned char *sb = static_cast<unsigned char *>(base);
   float4 *rec = reinterpret_cast<float4 *>(sb);
   float *extc = ext ? reinterpret_cast<float *>(sb + off_ext) : nullptr;
@@ -2283,8 +2334,14 @@ extern "C" int bbkde_eval_noalloc(const bbkde_kernel_desc *kernel, int64_t n_ref
   if (dim == 2) k_to_f32<<<grid1d(n_query), 256, 0, st>>>(query_y, qy, n_query);
 
   // Segment the reference range as the context path does, within the scratch.
-  int sm_count = 148;
-  cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, device);
+  int sm_count = 0;
+  e = cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, device);
+  if (e != cudaSuccess || sm_count < 1) {
+    noalloc_msg(errbuf, errbuf_len, "cudaDeviceGetAttribute(SM count): %s",
+                cudaGetErrorString(e));
+    cudaGetLastError();
+    return BBKDE_CUDA_ERROR;
+  }
   const int variant = kDefaultVariant;
   const int qpb = queries_per_block(variant, false);
   const int64_t qtiles = (n_query + qpb - 1) / qpb;

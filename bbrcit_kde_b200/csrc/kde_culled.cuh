@@ -21,13 +21,16 @@
 // Gaussian blocks run three scans over the tiles:
 //   1. M = the largest e over the block's box;
 //   2. sum every tile with e >= M - cut (the near field);
-//   3. with S_k = the smallest near-field sum in slot k and
-//      T_k = log2(rel * S_k / n_tiles) - 1, also sum every remaining tile that
-//      reaches e_k >= T_k for some slot k.
-// A tile left out has 2^e_k < rel S_k / (2 n_tiles) for every slot, so the skipped
-// part of every query of slot k is below rel * S_k / 2 <= rel * S_q / 2: every
-// culled sum is within rel of the full sum (plus the FP32 arithmetic error of
-// the full sum). Tiles whose largest pair exponent s_max d_min^2 is below -128
+//   3. with S_k = the smallest near-field sum in slot k, the allowance
+//      A_k = max(rel * S_k, abs) and T_k = log2(A_k / n_tiles) - 1, also sum
+//      every remaining tile that reaches e_k >= T_k for some slot k.
+// A tile left out has 2^e_k < A_k / (2 n_tiles) for every slot, so the skipped
+// part of every query q of slot k is below A_k / 2 <= max(rel * S_q, abs) / 2:
+// every culled sum is within rel of the full sum, or within abs of it, whichever
+// is larger (plus the FP32 arithmetic error of the full sum). abs = 0 gives the
+// purely relative bound. This is the reference's combined criterion: its tree
+// stops refining a query once the bounds are within rel_err relative or
+// abs_err absolute (KernelDensityImpl.h:1071-1095). Tiles whose largest pair exponent s_max d_min^2 is below -128
 // are skipped without a bound: ex2.approx.ftz flushes every such kernel value
 // to zero, so they add exactly nothing to the FP32 sum either. The per-block
 // worst ratio (skipped bound / S_k) is written for the host to verify.
@@ -85,8 +88,9 @@ struct CullArgs {
   int64_t n_ref;
   float cut;              // near-field width in log2 units
   double rel;             // bound of the skipped part relative to the block minimum
+  double abs_n;           // absolute allowance of the skipped part (unnormalised units)
   CullQueries q;
-  double *blk_bound;      // per block: worst (skipped bound / slot minimum sum)
+  double *blk_bound;      // per block: worst (skipped bound / slot allowance A_k)
   double *blk_smin;       // per block: smallest unnormalised sum of its queries
   int *blk_tiles;         // per block: reference tiles summed
 };
@@ -421,20 +425,25 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_pair_sum_culled(CullArgs a) {
       double m = INFINITY;
 #pragma unroll
       for (int w = 0; w < NW; ++w) m = fmin(m, s_d[tid][w]);
-      // m = +inf: an empty slot needs nothing; m <= 0: the slot needs every tile
-      // that does not flush to zero.
-      s_th[tid] = m > 0.0 ? (float)(log2(a.rel * m) - log2((double)a.n_tiles)) - 1.0f
-                          : -INFINITY;
+      // m = +inf: an empty slot needs nothing; allowance 0 (m <= 0 and no abs):
+      // the slot needs every tile that does not flush to zero.
+      const double allow = fmax(a.rel * m, a.abs_n);
+      s_th[tid] = allow > 0.0 ? (float)(log2(allow) - log2((double)a.n_tiles)) - 1.0f
+                              : -INFINITY;
       s_d[tid][0] = m;
+      s_d[tid][1] = allow;
     }
     __syncthreads();
-    double smk[QPT];
+    double smk[QPT], alk[QPT];
 #pragma unroll
-    for (int k = 0; k < QPT; ++k) smk[k] = s_d[k][0];
+    for (int k = 0; k < QPT; ++k) {
+      smk[k] = s_d[k][0];
+      alk[k] = s_d[k][1];
+    }
     __syncthreads();
     pass(2);   // scan 3: far field, bound of the rest
-    // Per-slot bound of the skipped part (fixed-order reduction), worst ratio:
-    // bound_k = skipped_k 2^T_k and 2^T_k = rel S_k / (2 n_tiles).
+    // Per-slot bound of the skipped part (fixed-order reduction), worst ratio to
+    // the allowance: bound_k = skipped_k 2^T_k and 2^T_k = A_k / (2 n_tiles).
 #pragma unroll
     for (int k = 0; k < QPT; ++k) {
       double sk = skipped[k];
@@ -450,7 +459,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_pair_sum_culled(CullArgs a) {
 #pragma unroll
       for (int w = 0; w < NW; ++w) b += s_d[k][w];
       smin_all = fmin(smin_all, smk[k]);
-      if (b > 0.0) ratio = fmax(ratio, b * exp2((double)s_th[k]) / smk[k]);
+      if (b > 0.0) ratio = fmax(ratio, b * exp2((double)s_th[k]) / alk[k]);
     }
   } else {
     pass(0);

@@ -328,8 +328,9 @@ __global__ void __launch_bounds__(T *T / 8, T == 32 ? 4 : 16)
     __syncthreads();
     if (tid < NS) {
       const double mk = (double)__uint_as_float(s_min[tid]);
-      s_th[tid] = mk > 0.0 ? (float)(log2(a.rel * mk) - log2((double)a.n_tiles)) - 1.0f
-                           : -INFINITY;
+      const double allow = fmax(a.rel * mk, a.abs_n);   // the pair form's allowance
+      s_th[tid] = allow > 0.0 ? (float)(log2(allow) - log2((double)a.n_tiles)) - 1.0f
+                              : -INFINITY;
     }
     __syncthreads();
     pass(2);   // far field, bound of the rest
@@ -349,7 +350,7 @@ __global__ void __launch_bounds__(T *T / 8, T == 32 ? 4 : 16)
       for (int w = 0; w < NW; ++w) b += s_d[k][w];
       const double mk = (double)__uint_as_float(s_min[k]);
       smin_all = fmin(smin_all, mk);
-      if (b > 0.0) ratio = fmax(ratio, b * exp2((double)s_th[k]) / mk);
+      if (b > 0.0) ratio = fmax(ratio, b * exp2((double)s_th[k]) / fmax(a.rel * mk, a.abs_n));
     }
   } else {
     pass(0);

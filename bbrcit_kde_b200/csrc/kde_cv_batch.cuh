@@ -72,6 +72,8 @@ struct CvArgs {
   int r_epan, r_conv;               // candidate half-widths in grid cells
   double *epan_part;                // [part][2][kCvCells]: sum w log f, sum w f
   double *conv_hist;                // [set][16][kCvCells]
+  unsigned long long *pairs;        // [0] likelihood pairs in support (4 atomics each),
+                                    // [1] convolution pairs in support (4 per x-group)
 };
 
 // #{h[a] <= v} for v >= 0. The key (the double's bits shifted right: exponent
@@ -191,6 +193,7 @@ __global__ void __launch_bounds__(1024, 1) k_cv_batch(CvArgs a) {
     sluty[i] = a.luty[i];
   }
   const double hxmax = a.hx[a.nhx - 1], hymax = a.hy[a.nhy - 1];
+  unsigned long long n_lik = 0, n_conv = 0;   // in-support pairs of this thread
   __syncthreads();
 
   for (;;) {
@@ -246,6 +249,7 @@ __global__ void __launch_bounds__(1024, 1) k_cv_batch(CvArgs a) {
             const double dx = qx - xs[u], dy = qy - ys[u];
             const double ax = fabs(dx), ay = fabs(dy);
             if (ax >= hxmax || ay >= hymax || js[u] == i) continue;
+            ++n_lik;
             const int p = cv_cell(ax, shx, a.nhx, slutx, a.lut_basex, a.lut_shift);
             const int q = cv_cell(ay, shy, a.nhy, sluty, a.lut_basey, a.lut_shift);
             const int c = p * kCvRow + q;
@@ -344,6 +348,7 @@ __global__ void __launch_bounds__(1024, 1) k_cv_batch(CvArgs a) {
           const double v0 = bqw[t] * mj;
           if (++t == lim) t = 0;
           if (ax >= hx2 || ay >= hy2) continue;
+          ++n_conv;
           const double hax = 0.5 * ax, hay = 0.5 * ay;
           const int p = cv_cell(hax, shx, a.nhx, slutx, a.lut_basex, a.lut_shift);
           const int q = cv_cell(hay, shy, a.nhy, sluty, a.lut_basey, a.lut_shift);
@@ -371,6 +376,17 @@ __global__ void __launch_bounds__(1024, 1) k_cv_batch(CvArgs a) {
         if (v != 0ull) atomicAdd(&dst[e], v);
       }
       __syncthreads();
+    }
+  }
+  if (a.pairs) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      n_lik += __shfl_xor_sync(0xffffffffu, n_lik, o);
+      n_conv += __shfl_xor_sync(0xffffffffu, n_conv, o);
+    }
+    if (lane == 0) {
+      atomicAdd(&a.pairs[0], n_lik);
+      atomicAdd(&a.pairs[1], n_conv);
     }
   }
 }

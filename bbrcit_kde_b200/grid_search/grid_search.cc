@@ -152,11 +152,12 @@ struct Session {
     return k;
   }
   // Adaptive densities as the reference's adapt_density(alpha, rel_tol, abs_tol)
-  // (grid_search.cc:266-268, :508-510): the pilot to rel_tol when it lies in
-  // (0, 1), else the exact pilot.
-  void adapt(const bbkde_kernel_desc &k, double alpha, double rel_tol) {
-    if (rel_tol > 0 && rel_tol < 1)
-      check(bbkde_adapt_density_tol(ctx, &k, alpha, rel_tol, nullptr, nullptr, nullptr, nullptr),
+  // (grid_search.cc:266-268, :508-510): the pilot to max(rel_tol f, abs_tol) when
+  // rel_tol lies in [0, 1) and a tolerance is set, else the exact pilot.
+  void adapt(const bbkde_kernel_desc &k, double alpha, double rel_tol, double abs_tol) {
+    if (rel_tol >= 0 && rel_tol < 1 && abs_tol >= 0 && (rel_tol > 0 || abs_tol > 0))
+      check(bbkde_adapt_density_tol(ctx, &k, alpha, rel_tol, abs_tol, nullptr, nullptr, nullptr,
+                                    nullptr),
             ctx);
     else
       check(bbkde_adapt_density(ctx, &k, alpha, BBKDE_FP32C, nullptr, nullptr, nullptr, nullptr),
@@ -164,7 +165,7 @@ struct Session {
   }
   // Density at the grid points (x0..x1 by sx, y0..y1 by sy, ends included).
   std::vector<double> eval_grid(double bx, double by, double x0, double x1, int sx, double y0,
-                                double y1, int sy, double rel_tol) {
+                                double y1, int sy, double rel_tol, double abs_tol) {
     auto g = grid_points(x0, x1, sx, y0, y1, sy);
     std::vector<double> q(2 * g.size()), out(g.size());
     for (size_t i = 0; i < g.size(); ++i) {
@@ -175,8 +176,8 @@ struct Session {
                        nullptr),
           ctx);
     const bbkde_kernel_desc k = kernel(bx, by);
-    if (rel_tol > 0 && rel_tol < 1) {
-      check(bbkde_eval_culled(ctx, &k, 1, rel_tol, out.data(), 0, nullptr), ctx);
+    if (rel_tol >= 0 && rel_tol < 1 && abs_tol >= 0 && (rel_tol > 0 || abs_tol > 0)) {
+      check(bbkde_eval_tol(ctx, &k, 1, rel_tol, abs_tol, out.data(), 0, nullptr), ctx);
     } else {
       const int64_t n = bbkde_size(ctx, BBKDE_REFERENCE);
       check(bbkde_eval_range(ctx, &k, 0, n - 1, 0, (int64_t)g.size() - 1, 1, BBKDE_FP32C,
@@ -260,7 +261,7 @@ void run(const Options &o) {
     std::cout << "  alpha: " << alpha << "\n\n";
     const bbkde_kernel_desc k = s.kernel(base_bwx, base_bwy);
     t0 = Clock::now();
-    s.adapt(k, alpha, rel_tol);
+    s.adapt(k, alpha, rel_tol, abs_tol);
     std::cout << "  => running time: " << ms_since(t0) << " ms. \n\n";
   }
 
@@ -363,7 +364,7 @@ void run(const Options &o) {
   std::cout << "  grid dimensions: " << nqx << "x" << nqy << "\n  x bandwidth: " << bx
             << "\n  y bandwidth: " << by << "\n\n";
   t0 = Clock::now();
-  std::vector<double> dens = s.eval_grid(bx, by, sqx, eqx, nqx, sqy, eqy, nqy, rel_tol);
+  std::vector<double> dens = s.eval_grid(bx, by, sqx, eqx, nqx, sqy, eqy, nqy, rel_tol, abs_tol);
   std::cout << "  => running time: " << ms_since(t0) << " ms. \n\n";
   {
     const std::string out = o.str("output_eval_fname");
@@ -379,7 +380,7 @@ void run(const Options &o) {
             << "\n  alpha: " << alpha << "\n\n";
   const bbkde_kernel_desc kb = s.kernel(before_bwx, before_bwy);
   t0 = Clock::now();
-  s.adapt(kb, alpha, rel_tol);
+  s.adapt(kb, alpha, rel_tol, abs_tol);
   std::cout << "  => running time: " << ms_since(t0) << " ms. \n\n";
   double after_bwx = before_bwx, after_bwy = before_bwy;
   if (adaptive_cv) {
@@ -390,7 +391,7 @@ void run(const Options &o) {
   std::cout << "  final bandwidth x: " << after_bwx << "\n  final bandwidth y: " << after_bwy
             << "\n\n";
   t0 = Clock::now();
-  dens = s.eval_grid(after_bwx, after_bwy, sqx, eqx, nqx, sqy, eqy, nqy, rel_tol);
+  dens = s.eval_grid(after_bwx, after_bwy, sqx, eqx, nqx, sqy, eqy, nqy, rel_tol, abs_tol);
   std::cout << "  => running time: " << ms_since(t0) << " ms. \n\n";
   const std::string out = o.str("output_adaptive_eval_fname");
   write_grid_values(out, dens, sqx, eqx, nqx, sqy, eqy, nqy);

@@ -203,16 +203,17 @@ def cpu_reference_rate(wl, seconds: float, kind_pref: str = "reference"):
     from oracle.pyoracle import Oracle, Reference, nthreads_default
     threads = nthreads_default()
     n = len(wl.refs)
+    dim = wl.dim
     if kind_pref == "reference" and Reference.available():
         ref = Reference()
-        handle = ref.create(wl.kind, 2, wl.h, wl.refs, wl.weights)
+        handle = ref.create(wl.kind, dim, wl.h, wl.refs, wl.weights)
         run = lambda q: ref.direct(handle, q, nthreads=threads)  # noqa: E731
         kind = "reference"
         cleanup = lambda: ref.destroy(handle)  # noqa: E731
     else:
         orc = Oracle()
         wn = wl.weights / wl.weights.sum()
-        run = lambda q: orc.direct(wl.kind, 2, wl.h, wl.refs, wn, q, nthreads=threads)  # noqa
+        run = lambda q: orc.direct(wl.kind, dim, wl.h, wl.refs, wn, q, nthreads=threads)  # noqa
         kind = "port"
         cleanup = lambda: None  # noqa: E731
     # size the sample from a probe of at least ~0.5 s
@@ -230,10 +231,11 @@ def cpu_reference_rate(wl, seconds: float, kind_pref: str = "reference"):
     run(wl.queries[:m])
     dt = time.perf_counter() - t0
     cleanup()
+    kname = {0: f"GaussianKernel<{dim},double>", 2: "GaussianProductKernel2d<double>"}.get(
+        wl.kind, f"kind {wl.kind}")
     return {"value": m * n / dt, "unit": UNIT, "cores": threads, "kind": kind,
-            "sample": f"direct_eval of {m} queries x {n} refs "
-                      f"(GaussianProductKernel2d<double>, same per-pair code as the pilot "
-                      f"pass), {threads} host threads, {dt:.1f} s"}
+            "sample": f"direct_eval of {m} queries x {n} refs ({kname}), {threads} host "
+                      f"threads, {dt:.1f} s"}
 
 
 def run_reference_arm(a, world, rank):
@@ -399,17 +401,25 @@ def main():
     sl = slice(m // 2, m // 2 + 4096)
     ctx.adapt_density(desc, wl.alpha, bk.FP32C, outputs=False)
     f32 = ctx.eval_range(desc, 0, n - 1, sl.start, sl.stop - 1, True, bk.FP32C)
-    abw64, mass64, _, _ = ctx.adapt_density(desc, wl.alpha, bk.FP64)
+    abw64, mass64, pilot64, _ = ctx.adapt_density(desc, wl.alpha, bk.FP64)
     f64 = ctx.eval_range(desc, 0, n - 1, sl.start, sl.stop - 1, True, bk.FP64)
     err = error_stats(f32, f64)
     err_def = ("vs FP64 device path (pilot + eval in FP64) on 4096 queries; pass = "
                "approximately_equal(rel 1e-6, abs 1e-8) as FloatUtils.h:49-61")
     oracle_check = None
     if rank == 0:
+        # The FP64 device path against the CPU oracle at full size: 1,024 of the
+        # error-check queries (with the FP64 attributes) and 1,024 pilot rows.
         from oracle.pyoracle import Oracle
         orc = Oracle()
-        want = orc.direct(wl.kind, 2, wl.h, wl.refs, mass64, wl.queries[sl][:64], abw=abw64)
-        oracle_check = error_stats(f64[:64], want, 1e-10, 0.0)["pass_rate"]
+        want = orc.direct(wl.kind, 2, wl.h, wl.refs, mass64, wl.queries[sl][:1024], abw=abw64)
+        rows = np.linspace(0, n - 1, 1024).astype(np.int64)
+        pilot_want = orc.direct(wl.kind, 2, wl.h, wl.refs, wn, wl.refs[rows])
+        oracle_check = {
+            "queries": 1024, "eval": error_stats(f64[:1024], want, 1e-10, 0.0),
+            "pilot_rows": 1024, "pilot": error_stats(pilot64[rows], pilot_want, 1e-10, 0.0)}
+        oracle_check["pass_rate"] = min(oracle_check["eval"]["pass_rate"],
+                                        oracle_check["pilot"]["pass_rate"])
 
     # ---- end to end through the C ABI with host buffers -----------------
     e2e = None
@@ -468,7 +478,7 @@ def main():
         "clocks": clocks,
         "gpu_launches": int(launches),
         "error_vs_fp64": {**err, "definition": err_def,
-                          "fp64_vs_cpu_oracle_pass_rate": oracle_check},
+                          "fp64_vs_cpu_oracle": oracle_check},
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -800,11 +810,21 @@ def run_plain_small(a, world, rank, local):
     ctx.upload(bk.REFERENCE, wl.refs, mass=w, weight=w)
     ctx.upload(bk.QUERY, wl.queries)
     out = torch.empty(m, dtype=torch.float64, device="cuda")
+    sm_count, _ = ctx.device_info()
+    kernel_ms = []
+
+    def step():
+        ctx.eval_range_device(desc, 0, n - 1, 0, m - 1, out.data_ptr())
+        kernel_ms.append(ctx.last_launch_stats()[0])
+
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     launches0 = ctx.launch_count()
-    ms = _timed(torch, stream,
-                lambda: ctx.eval_range_device(desc, 0, n - 1, 0, m - 1, out.data_ptr()),
-                a.steps, a.warmup)
+    sampler = ClockSampler(local)
+    sampler.start()
+    ms = _timed(torch, stream, step, a.steps, a.warmup, flush)
+    clocks = sampler.stop()
     launches = (ctx.launch_count() - launches0) * a.steps // (a.steps + a.warmup)
+    _, variant = ctx.launch_variants()
     pin = lambda arr: torch.from_numpy(np.ascontiguousarray(arr)).pin_memory().numpy()  # noqa
     h_q, h_out = pin(wl.queries), pin(np.empty(m))
 
@@ -812,7 +832,7 @@ def run_plain_small(a, world, rank, local):
         ctx.upload(bk.QUERY, h_q)
         ctx.eval_range(desc, 0, n - 1, 0, m - 1, True, bk.FP32C, out=h_out)
 
-    e2e_ms = _timed(torch, stream, e2e_step, a.steps, a.warmup)
+    e2e_ms = _timed(torch, stream, e2e_step, a.steps, a.warmup, flush)
     got = ctx.eval_all(desc)
     f64 = ctx.eval_all(desc, precision=bk.FP64)
     from oracle.pyoracle import Oracle
@@ -820,9 +840,22 @@ def run_plain_small(a, world, rank, local):
     cpu = cpu_reference_rate(wl, min(a.cpu_seconds, 4.0)) if not a.no_cpu_baseline else None
     ctx.close()
     pairs = float(n) * m
+    peaks = measured_peaks()
+    sm_max = float(peaks.get("sm_max_mhz") or clocks.get("sm_max_mhz") or 1965.0)
+    poly = VARIANT_POLY[variant] if 0 <= variant < len(VARIANT_POLY) else 0
+    per_clk, bound = pair_sum_bound_per_clk_per_sm(poly)
+    peak = sm_count * per_clk * sm_max * 1e6
+    kms = float(np.mean(kernel_ms[-a.steps:]))
     _line(a, world, UNIT, pairs * world / (np.mean(ms) / 1e3), ms,
           {"workload": "plain 2-D Gaussian, 10k bimodal refs, h=0.1, 100x100 grid on "
-                       "[-3,3)^2 (1e8 evals per call)"}, "f32",
+                       "[-3,3)^2 (1e8 evals per call)",
+           "l2": "flushed between timed steps (256 MB write)"}, "f32",
+          clocks=clocks,
+          roofline={"bound": bound, "achieved": pairs / (kms / 1e3) / 1e9,
+                    "peak": peak / 1e9, "unit": "Geval/s",
+                    "frac": pairs / (kms / 1e3) / peak, "traffic": None,
+                    "kernel_ms_per_launch": kms, "launch_shape": variant,
+                    "note": "1e8 pairs fill the 148 SMs for ~20 us: launch and tail bound"},
           latency_us={"device": float(np.median(ms) * 1e3),
                       "e2e_c_abi": float(np.median(e2e_ms) * 1e3)},
           e2e={"value": pairs * world / (np.mean(e2e_ms) / 1e3), "unit": UNIT,
@@ -834,11 +867,49 @@ def run_plain_small(a, world, rank, local):
     return 0
 
 
+def _cv_cpu_baseline(bk, W, sets, hb, seconds):
+    """The reference's likelihood_cross_validate + lsq_convolution_cross_validate
+    (rel = abs = 0: its dual tree then sums every pair exactly), one bandwidth per
+    call as grid_search does, on all host cores (one (hx, hy) per thread), on a
+    bounded sample: the first dataset of at least 10,000 points cut to 10,000."""
+    from concurrent.futures import ThreadPoolExecutor
+    from oracle.pyoracle import Reference, nthreads_default
+    if not Reference.available():
+        return None
+    ref = Reference()
+    s1 = next(s for s in sets if len(s) >= 10_000)[:10_000]
+    ones = np.ones(len(s1))
+    threads = nthreads_default()
+    rng = np.random.default_rng(11)
+    grid = [(hb[i], hb[j]) for i, j in zip(rng.integers(0, len(hb), 4096),
+                                           rng.integers(0, len(hb), 4096))]
+
+    def one(h):
+        ref.likelihood_cv(bk.EPANECHNIKOV_PRODUCT_2D, 2, h, s1, ones)
+        ref.lsq_conv_cv(bk.EPANECHNIKOV_PRODUCT_2D, 2, h, s1, ones)
+
+    done, t0 = 0, time.perf_counter()
+    with ThreadPoolExecutor(threads) as ex:
+        while time.perf_counter() - t0 < seconds and done < len(grid):
+            batch = grid[done: done + threads]
+            list(ex.map(one, batch))
+            done += len(batch)
+    dt = time.perf_counter() - t0
+    return {"value": float(len(s1)) ** 2 * 2 * done / dt,
+            "unit": "(pair, bandwidth, kernel) items/s", "cores": threads, "kind": "reference",
+            "sample": f"likelihood_cross_validate + lsq_convolution_cross_validate (rel = abs "
+                      f"= 0) of one 10,000-point dataset at {done} random (hx, hy) of the "
+                      f"64 x 64 grid, one bandwidth per call on {threads} threads, {dt:.1f} s"}
+
+
 def run_cv_batch(a, world, rank, local):
     """Batched cross-validation: 16 datasets (log-uniform sizes in [1e4, 5e5], 3-component
     mixtures), Epanechnikov product kernel, 64 x 64 log-spaced (hx, hy) over [0.01, 1]^2:
     LOO likelihood and LSQ-convolution scores for every (dataset, hx, hy) in one
-    persistent graph-captured launch. One step = one bbkde_cv_batch call."""
+    persistent graph-captured launch. One step = one bbkde_cv_batch call: host
+    datasets in, both score tables out. `value` is the device time of the launch
+    (CUDA events around the graph), `e2e` the whole call (binning on the host,
+    uploads, launch, downloads)."""
     torch, bk, stream, ctx = _device_setup(local)
     from bbrcit_kde_b200 import workloads as W
     sizes = [a.cv_size] * a.cv_sets if a.cv_size else None
@@ -848,15 +919,21 @@ def run_cv_batch(a, world, rank, local):
                 for s in sets]
     hb = W.config3_bandwidths()
     ds = [(s, None) for s in sets]
-    res = {}
+    sm_count, _ = ctx.device_info()
+    res, dev_ms = {}, []
     launches0 = ctx.launch_count()
 
     def step():
         res["out"] = ctx.cv_batch(bk.EPANECHNIKOV_PRODUCT_2D, ds, hb, hb)
+        dev_ms.append(ctx.last_launch_stats()[0])
 
+    sampler = ClockSampler(local)
+    sampler.start()
     ms = _timed(torch, stream, step, a.steps, a.warmup)
+    clocks = sampler.stop()
     launches = (ctx.launch_count() - launches0) // (a.steps + a.warmup)
     _, pairs, _ = ctx.last_launch_stats()
+    lik_pairs, conv_pairs = ctx.cv_batch_counts()
     lik, lsq = res["out"]
     # Exactness: a few (dataset, hx, hy) against the per-bandwidth FP64 pair sums.
     small = int(np.argmin([len(s) for s in sets]))
@@ -875,29 +952,40 @@ def run_cv_batch(a, world, rank, local):
                        "lsq_rel": abs(qg - q64) / abs(q64)})
     cpu = None
     if rank == 0 and not a.no_cpu_baseline:
-        from oracle.pyoracle import Reference
-        if Reference.available():
-            ref = Reference()
-            s1 = s0[:10_000]
-            d = (hb[41], hb[49])
-            t0 = time.perf_counter()
-            ref.likelihood_cv(bk.EPANECHNIKOV_PRODUCT_2D, 2, d, s1, np.ones(len(s1)))
-            ref.lsq_conv_cv(bk.EPANECHNIKOV_PRODUCT_2D, 2, d, s1, np.ones(len(s1)))
-            dt = time.perf_counter() - t0
-            cpu = {"value": float(len(s1)) ** 2 * 2 / dt, "unit": "(pair, bandwidth, kernel) "
-                   "items/s", "cores": 1, "kind": "reference",
-                   "sample": f"likelihood_cross_validate + lsq_convolution_cross_validate of "
-                             f"one 10k-point dataset at one (hx, hy) = {d} (rel = abs = 0, "
-                             f"single-threaded dual tree), {dt:.1f} s"}
+        cpu = _cv_cpu_baseline(bk, W, sets, hb, a.cpu_seconds)
     ctx.close()
     items = pairs * hb.size * hb.size * 2
-    _line(a, world, "(pair, bandwidth, kernel) items/s", items * world / (np.mean(ms) / 1e3),
-          ms, {"workload": f"batched CV: {len(sets)} datasets (sizes {min(map(len, sets))}.."
-                           f"{max(map(len, sets))}), Epanechnikov product, 64x64 (hx,hy) "
-                           f"log-spaced on [0.01,1]^2, likelihood + LSQ-conv",
-               "pairs": pairs, "bandwidths": int(hb.size ** 2)}, "fixed-point int64 + f64",
+    kms = float(np.mean(dev_ms[-a.steps:]))
+    # Roofline: the histograms are built by 64-bit shared-memory atomic adds, 4 per
+    # in-support likelihood pair and 16 per in-support convolution pair. The shared
+    # pipe moves one 128-byte wavefront per clock per SM; a warp's 64-bit atomic
+    # without bank conflicts is two wavefronts, i.e. 16 atomics per clock per SM.
+    atomics = 4.0 * lik_pairs + 16.0 * conv_pairs
+    peaks = measured_peaks()
+    sm_max = float(peaks.get("sm_max_mhz") or clocks.get("sm_max_mhz") or 1965.0)
+    peak = sm_count * 16 * sm_max * 1e6
+    h2d = sum(s.nbytes for s in sets)
+    nout = len(sets) * hb.size * hb.size
+    _line(a, world, "(pair, bandwidth, kernel) items/s", items * world / (kms / 1e3), ms,
+          {"workload": f"batched CV: {len(sets)} datasets (sizes {min(map(len, sets))}.."
+                       f"{max(map(len, sets))}), Epanechnikov product, 64x64 (hx,hy) "
+                       f"log-spaced on [0.01,1]^2, likelihood + LSQ-conv",
+           "pairs": pairs, "bandwidths": int(hb.size ** 2),
+           "l2": "inputs (the datasets, up to 8 MB each) are re-uploaded by every call; "
+                 "the launch runs for seconds, so L2 state between steps is immaterial"},
+          "fixed-point int64 + f64",
+          clocks=clocks,
+          e2e={"value": items * world / (np.mean(ms) / 1e3),
+               "unit": "(pair, bandwidth, kernel) items/s", "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(2 * nout * 8)},
+          roofline={"bound": "shared-memory pipe (64-bit atomic adds of the moment "
+                             "histograms; 16 per clk per SM without bank conflicts)",
+                    "achieved": atomics / (kms / 1e3) / 1e9, "peak": peak / 1e9,
+                    "unit": "G atomics/s", "frac": atomics / (kms / 1e3) / peak,
+                    "traffic": None, "lik_pairs_in_support": lik_pairs,
+                    "conv_pairs_in_support": conv_pairs, "kernel_ms_per_launch": kms},
           gpu_launches=int(launches), exactness_vs_fp64_per_bandwidth=checks, cpu_baseline=cpu,
-          pairs_per_s=pairs * world / (np.mean(ms) / 1e3))
+          pairs_per_s=pairs * world / (kms / 1e3))
     return 0
 
 
@@ -926,15 +1014,34 @@ def run_direct1d(a, world, rank, local):
         ctx.eval_range_device(desc, 0, n - 1, 0, m - 1, out.data_ptr())
         kernel_ms.append(ctx.last_launch_stats()[0])
 
+    launches0 = ctx.launch_count()
     sampler.start()
     ms = _timed(torch, stream, step, a.steps, a.warmup, flush)
     clocks = sampler.stop()
+    launches = (ctx.launch_count() - launches0) * a.steps // (a.steps + a.warmup)
     pairs = float(n) * m
     # error vs FP64 on 4096 queries
     q0 = m // 2
     _, variant = ctx.launch_variants()
     f32 = ctx.eval_range(desc, 0, n - 1, q0, q0 + 4095)
     f64 = ctx.eval_range(desc, 0, n - 1, q0, q0 + 4095, True, bk.FP64)
+    # end to end through the C ABI: queries in from pinned host memory, densities
+    # out to pinned host memory, every step
+    e2e = None
+    if not a.no_e2e:
+        pin = lambda arr: torch.from_numpy(np.ascontiguousarray(arr)).pin_memory().numpy()  # noqa
+        h_q, h_out = pin(wl.queries), pin(np.empty(m))
+
+        def e2e_step():
+            ctx.upload(bk.QUERY, h_q)
+            ctx.eval_range(desc, 0, n - 1, 0, m - 1, True, bk.FP32C, out=h_out)
+
+        e2e_ms = _timed(torch, stream, e2e_step, a.steps, a.warmup, flush)
+        e2e = {"value": pairs * world / (np.mean(e2e_ms) / 1e3), "unit": UNIT,
+               "h2d_bytes_per_step": int(h_q.nbytes), "d2h_bytes_per_step": int(h_out.nbytes)}
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        cpu = cpu_reference_rate(wl, a.cpu_seconds)
     ctx.close()
     peaks = measured_peaks()
     sm_max = float(peaks.get("sm_max_mhz") or clocks.get("sm_max_mhz") or 1965.0)
@@ -945,7 +1052,7 @@ def run_direct1d(a, world, rank, local):
     _line(a, world, UNIT, pairs * world / (np.mean(ms) / 1e3), ms,
           {"workload": f"1-D Gaussian, h=0.02, {n} refs (5-component mixture), {m} uniform "
                        f"queries on [-6,6] per rank", "l2": "flushed between timed steps"},
-          "f32", clocks=clocks,
+          "f32", clocks=clocks, e2e=e2e, cpu_baseline=cpu, gpu_launches=int(launches),
           roofline={"bound": bound, "achieved": pairs / (kms / 1e3) / 1e9, "peak": peak / 1e9,
                     "unit": "Geval/s", "frac": pairs / (kms / 1e3) / peak, "traffic": None,
                     "launch_shape": variant,

@@ -24,7 +24,7 @@
 extern "C" {
 #endif
 
-#define BBKDE_ABI_VERSION 1
+#define BBKDE_ABI_VERSION 2
 
 #if defined(__GNUC__)
 #define BBKDE_API __attribute__((visibility("default")))
@@ -158,15 +158,18 @@ BBKDE_API int bbkde_adapt_density(bbkde_ctx *ctx, const bbkde_kernel_desc *kerne
                         int precision, double *abw_out, double *mass_out,
                         double *pilot_out, double *g_out);
 
-/* As bbkde_adapt_density, with the pilot to a relative tolerance, as the
- * reference's adapt_density(alpha, rel, abs) evaluates it through its tree
- * (KernelDensityImpl.h:291-359): the culled self-sum (see bbkde_eval_culled),
- * every pilot value within rel_tol (0 < rel_tol < 1) of the full sum plus the
- * FP32-compensated arithmetic error; g and the attributes in FP64 as above.
- * The Epanechnikov convolution kernels give UNSUPPORTED. */
+/* As bbkde_adapt_density, with the pilot to a tolerance, as the reference's
+ * adapt_density(alpha, rel_err, abs_err) evaluates it through its tree
+ * (KernelDensityImpl.h:291-359): the culled self-sum (see bbkde_eval_tol),
+ * every pilot value f within max(rel_tol f, abs_tol) / 2 of the full sum plus
+ * the FP32-compensated arithmetic error (0 <= rel_tol < 1, abs_tol >= 0 in
+ * density units; both 0 sum every pair that does not flush to zero in FP32);
+ * g and the attributes in FP64 as above. The Epanechnikov convolution kernels
+ * give UNSUPPORTED. */
 BBKDE_API int bbkde_adapt_density_tol(bbkde_ctx *ctx, const bbkde_kernel_desc *kernel,
-                                      double alpha, double rel_tol, double *abw_out,
-                                      double *mass_out, double *pilot_out, double *g_out);
+                                      double alpha, double rel_tol, double abs_tol,
+                                      double *abw_out, double *mass_out, double *pilot_out,
+                                      double *g_out);
 
 /* KernelDensity::unadapt_density (KernelDensityImpl.h:254-273): abw = 1, mass = w. */
 BBKDE_API int bbkde_unadapt_density(bbkde_ctx *ctx);
@@ -187,19 +190,20 @@ BBKDE_API int bbkde_likelihood_cv(bbkde_ctx *ctx, const bbkde_kernel_desc *kerne
 BBKDE_API int bbkde_lsq_conv_cv(bbkde_ctx *ctx, const bbkde_kernel_desc *kernel, int precision,
                       double *cv_out);
 
-/* Cross validation with the density sums to a relative tolerance, as the
- * reference evaluates them through its tree (likelihood_cross_validate,
+/* Cross validation with the density sums to a tolerance, as the reference
+ * evaluates them through its tree (likelihood_cross_validate(rel_err, abs_err),
  * KernelDensityImpl.h:215-252; lsq_convolution_cross_validate, :142-209): every
- * full self-sum is a culled sum within rel_tol (0 < rel_tol < 1) of the exact one
- * (FP32-compensated), and the leave-one-out value is that sum minus the self term
+ * full self-sum f is a culled sum within max(rel_tol f, abs_tol) / 2 of the exact
+ * one (0 <= rel_tol < 1, abs_tol >= 0; FP32-compensated), and the leave-one-out
+ * value is that sum minus the self term
  * m_i C(h), as the reference computes it (its FP32 mass, so the subtraction
  * cancels the self term of the sum). FP64 totals in fixed order. Kernels whose
  * culled sum is unsupported (the Epanechnikov convolution kernels, hence the
  * Epanechnikov product LSQ) give UNSUPPORTED. */
 BBKDE_API int bbkde_likelihood_cv_tol(bbkde_ctx *ctx, const bbkde_kernel_desc *kernel,
-                                      double rel_tol, double *cv_out);
+                                      double rel_tol, double abs_tol, double *cv_out);
 BBKDE_API int bbkde_lsq_conv_cv_tol(bbkde_ctx *ctx, const bbkde_kernel_desc *kernel,
-                                    double rel_tol, double *cv_out);
+                                    double rel_tol, double abs_tol, double *cv_out);
 
 /* ---- batched cross-validation -------------------------------------------- */
 
@@ -227,6 +231,14 @@ typedef struct {
 BBKDE_API int bbkde_cv_batch(bbkde_ctx *ctx, int kind, int n_sets, const bbkde_dataset *sets,
                              int n_hx, const double *hx, int n_hy, const double *hy,
                              int precision, double *lik_out, double *lsq_out);
+
+/* In-support pair counts of the last bbkde_cv_batch launch on this context (the
+ * units of its shared-memory bound): lik_pairs ordered pairs with |dx| < hx_max
+ * and |dy| < hy_max (4 64-bit shared-memory atomic adds each), conv_pairs
+ * unordered pairs with |dx| < 2 hx_max and |dy| < 2 hy_max (16 each, 4 per
+ * x-power group). No reference counterpart. */
+BBKDE_API int bbkde_cv_batch_counts(const bbkde_ctx *ctx, int64_t *lik_pairs,
+                                    int64_t *conv_pairs);
 
 /* ---- learned log-density surrogate ---------------------------------------- */
 
@@ -321,6 +333,24 @@ typedef struct {
 BBKDE_API int bbkde_eval_culled(bbkde_ctx *ctx, const bbkde_kernel_desc *kernel, int normalized,
                                 double rel_tol, double *out, int out_on_device,
                                 bbkde_cull_stats *stats);
+
+/* KernelDensity::eval(queries, rel_err, abs_err[, leaf_nmax, block_size])
+ * (KernelDensityImpl.h:624-737, pruning rule :1071-1095): the QUERY set against
+ * the REFERENCE set with the reference's combined tolerance. The reference's tree
+ * stops refining once a query's bounds are within rel_err relative or abs_err
+ * absolute; here the culled sum skips reference tiles whose total bound stays
+ * below max(rel_err S, abs_err) / 2, S the smallest near-field density of the
+ * query block, so every value f satisfies |out - f| <= max(rel_err f, abs_err) / 2
+ * plus the FP32-compensated arithmetic error. abs_err is in normalised density
+ * units (the reference divides it by C(h) for its unnormalised sums) and applies
+ * as given when normalized = 0 too. 0 <= rel_err < 1, abs_err >= 0 (both 0: every
+ * tile that does not flush to zero is summed). Query order is preserved (the
+ * reference returns its queries in Kd-tree order). stats->max_bound_ratio is the
+ * worst skipped bound over the allowance max(rel_err S, abs_err) (at most 1/2).
+ * Kernels as bbkde_eval_culled. */
+BBKDE_API int bbkde_eval_tol(bbkde_ctx *ctx, const bbkde_kernel_desc *kernel, int normalized,
+                             double rel_err, double abs_err, double *out, int out_on_device,
+                             bbkde_cull_stats *stats);
 
 /* A regular 2-D grid: point (i, j), 0 <= i < nx, 0 <= j < ny, at
  * (x0 + i (x1 - x0) / nx, y0 + j (y1 - y0) / ny) (end points excluded, the
@@ -434,24 +464,30 @@ BBKDE_API int bbkde_launch_variants(const bbkde_ctx *ctx, int *n_variants, int *
  * already exhausted. The caller passes device pointers for all inputs (FP64
  * columns ref_x / ref_y / ref_mass / ref_abw, query_x / query_y; ref_abw may be
  * NULL, the y columns are ignored for dim 1) and for the output out[n_query]
- * (normalized = 1 multiplies by C(h)). The result equals bbkde_eval_range with
- * BBKDE_FP32C over all references and queries.
+ * (normalized = 1 multiplies by C(h)). The result matches bbkde_eval_range with
+ * BBKDE_FP32C over all references and queries to the FP32C tolerance (the
+ * reference range may be cut into fewer segments here, so the last FP32 bits of
+ * the summation order can differ).
  *
  * Scratch is one fixed 64 MiB array in the library's device image (held by every
  * device that loads the library until the process exits). Problems that do not
  * fit -- 16 B per reference (20 B for product and convolution kernels), 4 B per
  * query coordinate and at least 8 B per query -- are rejected with
- * BBKDE_OUT_OF_RANGE and a message in errbuf (may be NULL). Up to 1,000,000
- * references with 1,000,000 2-D queries fit.
+ * BBKDE_OUT_OF_RANGE and a message in errbuf (may be NULL), before any work is
+ * enqueued. Up to 1,000,000 references with 1,000,000 2-D queries fit.
  *
  * The work is enqueued on `stream` (a cudaStream_t, NULL = legacy default
  * stream) and the call returns without waiting for it. All calls share the one
  * scratch array, so calls whose GPU work can overlap (different streams, or
  * different host threads without ordering) race and corrupt each other's
- * results; order them on one stream. The first call on each device resolves the
- * array's device address (cudaGetSymbolAddress) for that device, with the device
- * current; make that first call before any stream capture. Every scratch entry a
- * call reads is written earlier in the same call, so nothing is cleared. */
+ * results; order them on one stream. Every call resolves the array's device
+ * address in the current context (cudaGetSymbolAddress). CUDA loads a library's
+ * device code lazily, so the first call on a device is the one that places the
+ * 64 MiB array in that device's memory; that first call must come before any
+ * stream capture and before device memory runs out. A call with n_query = 0 does
+ * only this (no work is enqueued), so make one such call per device at set-up,
+ * with that device current. Every scratch entry a call reads is written earlier
+ * in the same call, so nothing is cleared. */
 BBKDE_API int bbkde_eval_noalloc(const bbkde_kernel_desc *kernel, int64_t n_ref,
                                  const double *ref_x, const double *ref_y,
                                  const double *ref_mass, const double *ref_abw,

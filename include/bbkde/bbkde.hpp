@@ -18,9 +18,10 @@
 //     reference's Kd-tree merges duplicates too, Kdtree.h:365-390, but stores
 //     points in Kd-tree order).
 //   * eval(...) with rel/abs tolerances runs the culled direct sum
-//     (bbkde_eval_culled: every value within rel_err of the full sum, a
-//     deterministic bound instead of the reference's tree bounds) for FP32
-//     kernels with rel_err in (0, 1), and the exact direct sum otherwise; query
+//     (bbkde_eval_tol: every value within max(rel_err f, abs_err) / 2 of the full
+//     sum f, a deterministic bound instead of the reference's tree bounds) for
+//     FP32 kernels, and the exact direct sum otherwise; adapt_density and the CV
+//     scores take the same tolerances for their density sums; query
 //     order is preserved (the reference's vector overload returns queries in
 //     Kd-tree order, KernelDensityImpl.h:642-651).
 //   * Kernel float type selects the device arithmetic: float kernels run the
@@ -270,10 +271,22 @@ class EpanechnikovKernel {
   template <typename P> T unnormalized_eval(const P &p, const P &q, T a = T(1)) const {
     return T(std::max(1.0 - bbkde_detail::sqdist(p, q, D) / (double(h_) * h_ * a * a), 0.0));
   }
+  // 1-D: the reference's three-uniform draw (EpanechnikovKernel.h:162-180). The
+  // reference has no 2-D sampler; here a 2-D draw is radial: the density
+  // (2 / pi)(1 - r^2) on the unit disk gives s = r^2 the density 2 (1 - s), so
+  // s = 1 - sqrt(1 - U) by inversion, with a uniform angle.
   template <typename RNG> void simulate(RNG &e, std::vector<T> &p, T a = T(1)) const {
-    std::uniform_real_distribution<T> d(-1, 1);
     p.resize(D);
-    for (int i = 0; i < D; ++i) p[i] = a * h_ * bbkde_detail::epanechnikov_draw(d(e), d(e), d(e));
+    if (D == 1) {
+      std::uniform_real_distribution<T> d(-1, 1);
+      p[0] = a * h_ * bbkde_detail::epanechnikov_draw(d(e), d(e), d(e));
+      return;
+    }
+    std::uniform_real_distribution<double> u(0, 1);
+    const double r = std::sqrt(1.0 - std::sqrt(1.0 - u(e)));
+    const double t = 6.283185307179586477 * u(e);
+    p[0] = T(a * h_ * r * std::cos(t));
+    p[1] = T(a * h_ * r * std::sin(t));
   }
   T bandwidth() const { return h_; }
   void set_bandwidth(T h) { h_ = h; }
@@ -505,6 +518,7 @@ class Kdtree {
   std::vector<DataPointType> &points() { return points_; }
   size_t size() const { return points_.size(); }
   bool empty() const { return points_.empty(); }
+  int leaf_nmax() const { return leaf_nmax_; }
 
  private:
   void merge_duplicates() {
@@ -638,9 +652,10 @@ class KernelDensity {
     direct_eval(queries, kernel_, block_size);
   }
 
-  // Tolerance-driven evaluation (KernelDensityImpl.h:473-680): the culled sum
-  // within rel_err of the full sum (FP32 kernels), else the exact direct sum;
-  // either meets the reference's rel_err / abs_err contract.
+  // Tolerance-driven evaluation (KernelDensityImpl.h:473-737): for FP32 kernels
+  // the culled sum (bbkde_eval_tol), every value within max(rel_err f, abs_err) / 2
+  // of the full sum f -- the reference's combined rel/abs criterion -- else the
+  // exact direct sum; either meets the reference's contract.
   FloatT eval(DataPointType &p, FloatType rel_err, FloatType abs_err) const {
     std::vector<DataPointType> q(1, p);
     eval(q, rel_err, abs_err);
@@ -650,19 +665,22 @@ class KernelDensity {
   }
   void eval(std::vector<DataPointType> &queries, FloatType rel_err, FloatType abs_err,
             int leaf_nmax = 2, size_t block_size = 128) const {
-    (void)abs_err; (void)leaf_nmax;
-    tolerance_eval(queries, rel_err, block_size);
+    (void)leaf_nmax;
+    tolerance_eval(queries, rel_err, abs_err, block_size);
   }
   void eval(KdtreeType &query_tree, FloatType rel_err, FloatType abs_err,
             size_t block_size = 128) const {
-    (void)abs_err;
-    tolerance_eval(query_tree.points(), rel_err, block_size);
+    tolerance_eval(query_tree.points(), rel_err, abs_err, block_size);
   }
 
-  // adapt_density / unadapt_density (KernelDensityImpl.h:254-359)
+  // adapt_density / unadapt_density (KernelDensityImpl.h:254-359). The pilot is
+  // evaluated to the reference's tolerance: for FP32 kernels each pilot value f
+  // within max(rel_err f, abs_err) / 2 (bbkde_adapt_density_tol); rel_err =
+  // abs_err = 0, FP64 kernels and the Epanechnikov convolution kernels use the
+  // exact pilot.
   void adapt_density(FloatType alpha, FloatType rel_err = 1e-6, FloatType abs_err = 1e-6,
                      size_t block_size = 128) {
-    (void)rel_err; (void)abs_err; (void)block_size;
+    (void)block_size;
     if (alpha < 0 || alpha > 1)
       throw std::invalid_argument("adapt_density: alpha must be between [0, 1]. ");
     unadapt_density();
@@ -671,9 +689,15 @@ class KernelDensity {
     const size_t n = size();
     std::vector<double> abw(n), mass(n);
     bbkde_kernel_desc k = kernel_.bbkde_desc();
-    bbkde_detail::check(bbkde_adapt_density(c, &k, double(alpha), precision_, abw.data(),
-                                            mass.data(), nullptr, nullptr),
-                        c);
+    if (use_tolerance(k, rel_err, abs_err))
+      bbkde_detail::check(bbkde_adapt_density_tol(c, &k, double(alpha), double(rel_err),
+                                                  double(abs_err), abw.data(), mass.data(),
+                                                  nullptr, nullptr),
+                          c);
+    else
+      bbkde_detail::check(bbkde_adapt_density(c, &k, double(alpha), precision_, abw.data(),
+                                              mass.data(), nullptr, nullptr),
+                          c);
     auto &pts = data_tree_.points();
     for (size_t i = 0; i < n; ++i) {
       pts[i].attributes().set_lower_abw(FloatT(abw[i]));
@@ -691,23 +715,35 @@ class KernelDensity {
     refs_fresh_ = false;
   }
 
-  // Cross validation (KernelDensityImpl.h:142-252)
+  // Cross validation (KernelDensityImpl.h:142-252), the density sums to the
+  // reference's tolerance as adapt_density's pilot (exact where that has no
+  // tolerance form: FP64 kernels, rel_err = abs_err = 0, and the LSQ score of
+  // the Epanechnikov kernels, whose convolution kernel has no culled sum).
   FloatType likelihood_cross_validate(FloatType rel_err = 1e-6, FloatType abs_err = 1e-6,
                                       size_t block_size = 128) const {
-    (void)rel_err; (void)abs_err; (void)block_size;
+    (void)block_size;
     bbkde_ctx *c = refs_uploaded();
     bbkde_kernel_desc k = kernel_.bbkde_desc();
     double cv = 0;
-    bbkde_detail::check(bbkde_likelihood_cv(c, &k, precision_, &cv), c);
+    if (use_tolerance(k, rel_err, abs_err))
+      bbkde_detail::check(
+          bbkde_likelihood_cv_tol(c, &k, double(rel_err), double(abs_err), &cv), c);
+    else
+      bbkde_detail::check(bbkde_likelihood_cv(c, &k, precision_, &cv), c);
     return FloatType(cv);
   }
   FloatType lsq_convolution_cross_validate(FloatType rel_err = 1e-6, FloatType abs_err = 1e-6,
                                            size_t block_size = 128) const {
-    (void)rel_err; (void)abs_err; (void)block_size;
+    (void)block_size;
     bbkde_ctx *c = refs_uploaded();
     bbkde_kernel_desc k = kernel_.bbkde_desc();
     double cv = 0;
-    bbkde_detail::check(bbkde_lsq_conv_cv(c, &k, precision_, &cv), c);
+    const bool epan = k.kind == BBKDE_EPANECHNIKOV || k.kind == BBKDE_EPANECHNIKOV_PRODUCT_2D;
+    if (!epan && use_tolerance(k, rel_err, abs_err))
+      bbkde_detail::check(
+          bbkde_lsq_conv_cv_tol(c, &k, double(rel_err), double(abs_err), &cv), c);
+    else
+      bbkde_detail::check(bbkde_lsq_conv_cv(c, &k, precision_, &cv), c);
     return FloatType(cv);
   }
 
@@ -769,20 +805,27 @@ class KernelDensity {
   }
 
  private:
+  // Whether a call with these tolerances has a culled (tolerance) form: FP32
+  // kernels that the culled sum supports, 0 <= rel_err < 1, abs_err >= 0, and
+  // a tolerance that is not zero.
+  bool use_tolerance(const bbkde_kernel_desc &k, FloatType rel_err, FloatType abs_err) const {
+    return precision_ == BBKDE_FP32C && rel_err >= 0 && rel_err < 1 && abs_err >= 0 &&
+           std::isfinite(double(abs_err)) && (rel_err > 0 || abs_err > 0) &&
+           k.kind != BBKDE_EPANECHNIKOV_PRODUCT_CONV_2D && k.kind != BBKDE_EPANECHNIKOV_CONV_1D &&
+           size() > 0;
+  }
   void tolerance_eval(std::vector<DataPointType> &queries, FloatType rel_err,
-                      size_t block_size) const {
+                      FloatType abs_err, size_t block_size) const {
     bbkde_kernel_desc k = kernel_.bbkde_desc();
-    const bool culled = precision_ == BBKDE_FP32C && rel_err > 0 && rel_err < 1 &&
-                        k.kind != BBKDE_EPANECHNIKOV_PRODUCT_CONV_2D &&
-                        k.kind != BBKDE_EPANECHNIKOV_CONV_1D && size() > 0;
-    if (!culled || queries.empty()) {
+    if (!use_tolerance(k, rel_err, abs_err) || queries.empty()) {
       direct_eval(queries, kernel_, block_size);
       return;
     }
     bbkde_ctx *c = refs_uploaded();
     bbkde_detail::upload_points<D>(c, BBKDE_QUERY, queries, false);
     std::vector<double> out(queries.size());
-    bbkde_detail::check(bbkde_eval_culled(c, &k, 1, double(rel_err), out.data(), 0, nullptr),
+    bbkde_detail::check(bbkde_eval_tol(c, &k, 1, double(rel_err), double(abs_err), out.data(),
+                                       0, nullptr),
                         c);
     for (size_t i = 0; i < queries.size(); ++i) {
       queries[i].attributes().set_lower(FloatT(out[i]));
@@ -861,6 +904,78 @@ FT lsq_numint_cross_validate(const KernelDensity<2, KT, FT, AT> &kde, FT start_x
   }
   return sq - 2 * llo;
 }
+
+// ---------------------------------------------------------------------------
+// Marginal densities (MarginalDensityAssociator.h:22-128): the 1-D density of
+// one coordinate of a 2-D product-kernel density. Each data point keeps its
+// weight and adaptive bandwidth; its mass becomes weight / abw (abw^-1 in one
+// dimension), and the marginal kernel is the 1-D kernel of the same family with
+// that axis' bandwidth. The 1-D density evaluates on the device like any other.
+// ---------------------------------------------------------------------------
+template <typename FloatT, typename AttrT>
+DecoratedPoint<1, AttrT, FloatT> marginalize_decorated_point2d(
+    const DecoratedPoint<2, AttrT, FloatT> &pt2d, size_t dim_idx) {
+  DecoratedPoint<1, AttrT, FloatT> pt1d;
+  pt1d[0] = pt2d[dim_idx];
+  AttrT &a = pt1d.attributes();
+  a.set_weight(pt2d.attributes().weight());
+  a.set_lower_abw(pt2d.attributes().lower_abw());
+  a.set_upper_abw(pt2d.attributes().upper_abw());
+  a.set_mass(a.weight() / a.abw());
+  return pt1d;
+}
+
+template <typename K> class MarginalKernelAssociator {};
+template <typename T> class MarginalKernelAssociator<EpanechnikovProductKernel2d<T>> {
+ public:
+  using KernelType = EpanechnikovProductKernel2d<T>;
+  using MarginalKernelType = EpanechnikovKernel<1, T>;
+  static MarginalKernelType marginal_kernel(const KernelType &k, size_t dim_idx) {
+    return MarginalKernelType(dim_idx == 0 ? k.hx() : k.hy());
+  }
+};
+template <typename T> class MarginalKernelAssociator<GaussianProductKernel2d<T>> {
+ public:
+  using KernelType = GaussianProductKernel2d<T>;
+  using MarginalKernelType = GaussianKernel<1, T>;
+  static MarginalKernelType marginal_kernel(const KernelType &k, size_t dim_idx) {
+    return MarginalKernelType(dim_idx == 0 ? k.hx() : k.hy());
+  }
+};
+
+template <typename KdeT, typename KernelT = typename KdeT::KernelType,
+          typename FloatT = typename KdeT::FloatType,
+          typename AttrT = typename KdeT::AttributeType>
+class MarginalDensityAssociator {};
+
+template <typename KernelT, typename FloatT, typename AttrT>
+class MarginalDensityAssociator<KernelDensity<2, KernelT, FloatT, AttrT>, KernelT, FloatT,
+                                AttrT> {
+ public:
+  using KernelDensityType = KernelDensity<2, KernelT, FloatT, AttrT>;
+  using MarginalKernelType = typename MarginalKernelAssociator<KernelT>::MarginalKernelType;
+  using MarginalDensityType = KernelDensity<1, MarginalKernelType, FloatT, AttrT>;
+  using Point1d = typename MarginalDensityType::DataPointType;
+
+  // The marginal density of coordinate dim_idx (0: x, 1: y). Its constructor
+  // normalises the weights and sets mass = weight * abw^-1, which is the mass
+  // marginalize_decorated_point2d gives; exact duplicates of the 1-D coordinate
+  // merge as in any density's constructor.
+  static MarginalDensityType marginal_density(const KernelDensityType &kde, size_t dim_idx) {
+    std::vector<Point1d> pts;
+    pts.reserve(kde.points().size());
+    for (const auto &p : kde.points()) pts.push_back(marginalize_decorated_point2d(p, dim_idx));
+    MarginalDensityType m(std::move(pts), kde.data_tree().leaf_nmax());
+    m.kernel() = MarginalKernelAssociator<KernelT>::marginal_kernel(kde.kernel(), dim_idx);
+    return m;
+  }
+  static MarginalDensityType marginal_density_x(const KernelDensityType &kde) {
+    return marginal_density(kde, 0);
+  }
+  static MarginalDensityType marginal_density_y(const KernelDensityType &kde) {
+    return marginal_density(kde, 1);
+  }
+};
 
 }  // namespace bbrcit
 

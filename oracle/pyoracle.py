@@ -176,6 +176,12 @@ class Reference:
         lib.ref_kde_create.argtypes = [C.c_int, C.c_int, _dp, C.c_int64, _dp, _dp]
         lib.ref_kde_direct.argtypes = [C.c_void_p, C.c_int64, _dp, _dp, C.c_int]
         lib.ref_kde_destroy.argtypes = [C.c_void_p]
+        lib.ref_kde_tree_eval.argtypes = [C.c_int, C.c_int, _dp, C.c_int64, _dp, _dp,
+                                          C.c_double, C.c_double, C.c_double, C.c_int64, _dp,
+                                          _dp, _dp, _i64p, _dp, _dp, _dp, _dp, _i64p]
+        lib.ref_kde_marginal_direct.argtypes = [C.c_int, _dp, C.c_int64, _dp, _dp, C.c_double,
+                                                C.c_double, C.c_double, C.c_int, C.c_int64,
+                                                _dp, _dp, _dp, _dp, _dp, _dp, _i64p, C.c_int]
         self.lib = lib
 
     def create(self, kind, dim, h, refs, w):
@@ -258,3 +264,43 @@ class Reference:
                                             alpha, x0, x1, sx, y0, y1, sy, rel, abs_, _p(cv))
         assert rc == 0, rc
         return float(cv[0])
+
+    def tree_eval(self, kind, dim, h, refs, w, queries, rel, abs_, alpha=-1.0):
+        """The reference's dual-tree eval(queries, rel, abs) after an exact
+        adapt_density(alpha) when alpha >= 0. Returns (query coordinates as the
+        tree returns them, their values, tree-ordered (xy, w, mass, abw))."""
+        refs, w, queries = _c(refs), _c(w), _c(queries)
+        n, m = refs.shape[0], queries.shape[0]
+        hh = Oracle._h(h)
+        oq, out = np.empty(m * dim), np.empty(m)
+        mo = np.zeros(1, dtype=np.int64)
+        txy, tw, tm, ta = np.empty(n * dim), np.empty(n), np.empty(n), np.empty(n)
+        nt = np.zeros(1, dtype=np.int64)
+        rc = self.lib.ref_kde_tree_eval(kind, dim, _p(hh), n, _p(refs), _p(w), alpha, rel, abs_,
+                                        m, _p(queries), _p(oq), _p(out),
+                                        mo.ctypes.data_as(_i64p), _p(txy), _p(tw), _p(tm),
+                                        _p(ta), nt.ctypes.data_as(_i64p))
+        assert rc == 0, rc
+        k, t = int(mo[0]), int(nt[0])
+        return (oq[: k * dim].reshape(k, dim), out[:k],
+                (txy[: t * dim].reshape(t, dim), tw[:t], tm[:t], ta[:t]))
+
+    def marginal_direct(self, kind, h, refs, w, dim_idx, queries, alpha=-1.0, rel=0.0,
+                        abs_=0.0, nthreads=None):
+        """The reference's MarginalDensityAssociator marginal of a 2-D product-kernel
+        density (after adapt_density(alpha, rel, abs) when alpha >= 0), evaluated by
+        direct_eval at 1-D queries. Returns (values, marginal points (x, w, mass,
+        abw) in its tree order)."""
+        refs, w, queries = _c(refs), _c(w), _c(queries).reshape(-1)
+        n, m = refs.shape[0], queries.shape[0]
+        hh = Oracle._h(h)
+        out = np.empty(m)
+        tx, tw, tm, ta = np.empty(n), np.empty(n), np.empty(n), np.empty(n)
+        nt = np.zeros(1, dtype=np.int64)
+        rc = self.lib.ref_kde_marginal_direct(kind, _p(hh), n, _p(refs), _p(w), alpha, rel,
+                                              abs_, dim_idx, m, _p(queries), _p(out), _p(tx),
+                                              _p(tw), _p(tm), _p(ta), nt.ctypes.data_as(_i64p),
+                                              nthreads or nthreads_default())
+        assert rc == 0, rc
+        t = int(nt[0])
+        return out, (tx[:t], tw[:t], tm[:t], ta[:t])

@@ -24,11 +24,13 @@
 #include <cstdint>
 #include <random>  // the reference headers use std:: distributions without including it
 #include <cstring>
+#include <iostream>
 #include <stdexcept>
 #include <thread>
 #include <vector>
 
 #include <KernelDensity.h>
+#include <MarginalDensityAssociator.h>
 #include <Kernels/EpanechnikovKernel.h>
 #include <Kernels/EpanechnikovProductKernel2d.h>
 #include <Kernels/EpanechnikovProductConvKernel2d.h>
@@ -208,6 +210,86 @@ int dispatch_lsq(const Req &r) {
   return 5;
 }
 
+// KernelDensity::eval(std::vector<DataPointType>&, rel_err, abs_err, leaf_nmax)
+// (KernelDensityImpl.h:624-651): the reference's dual-tree evaluation. The query
+// tree reorders the queries and merges exact duplicates, so the returned
+// coordinates go to out_q (m_out rows of D) beside their values in out. The
+// data points (after an exact adapt_density when alpha >= 0) are exported
+// through the tree_* outputs, so that a comparison can evaluate with identical
+// attributes.
+// The reference reports every bound wider than the requested tolerance on
+// std::cerr (KernelDensityImpl.h:1113-1143), at rel = abs = 0 for nearly every
+// point; this mutes it for the duration of one call.
+struct MuteCerr {
+  std::streambuf *old;
+  MuteCerr() : old(std::cerr.rdbuf(nullptr)) {}
+  ~MuteCerr() {
+    std::cerr.rdbuf(old);
+    std::cerr.clear();
+  }
+};
+
+template <int D, typename K>
+int run_tree_eval(const Req &r, double *out_q, int64_t *m_out) {
+  using P = typename KdeT<D, K>::DataPointType;
+  MuteCerr mute;
+  KdeT<D, K> kde(make_points<D, K>(r.n, r.xy, r.w), 2);
+  set_bw(kde.kernel(), r.h);
+  if (r.alpha >= 0) kde.adapt_density(r.alpha, 0.0, 0.0);
+  std::vector<P> q;
+  q.reserve(r.m);
+  for (int64_t i = 0; i < r.m; ++i) {
+    P p;
+    for (int d = 0; d < D; ++d) p[d] = r.q[i * D + d];
+    q.push_back(p);
+  }
+  kde.eval(q, r.rel, r.abs, 32);
+  for (size_t i = 0; i < q.size(); ++i) {
+    for (int d = 0; d < D; ++d) out_q[i * D + d] = q[i][d];
+    r.out[i] = q[i].attributes().value();
+  }
+  *m_out = (int64_t)q.size();
+  export_tree(kde, r.tree_xy, r.tree_w, r.tree_mass, r.tree_abw, r.n_tree);
+  return 0;
+}
+
+int dispatch_tree_eval(const Req &r, double *out_q, int64_t *m_out) {
+  if (r.dim == 1) {
+    switch (r.kind) {
+      case GAUSS: return run_tree_eval<1, GaussianKernel<1, double>>(r, out_q, m_out);
+      case EPAN: return run_tree_eval<1, EpanechnikovKernel<1, double>>(r, out_q, m_out);
+    }
+  } else if (r.dim == 2) {
+    switch (r.kind) {
+      case GAUSS: return run_tree_eval<2, GaussianKernel<2, double>>(r, out_q, m_out);
+      case EPAN: return run_tree_eval<2, EpanechnikovKernel<2, double>>(r, out_q, m_out);
+      case GAUSS_PROD2D:
+        return run_tree_eval<2, GaussianProductKernel2d<double>>(r, out_q, m_out);
+      case EPAN_PROD2D:
+        return run_tree_eval<2, EpanechnikovProductKernel2d<double>>(r, out_q, m_out);
+    }
+  }
+  return 5;
+}
+
+// MarginalDensityAssociator<KernelDensity<2, K, double>>::marginal_density(kde,
+// dim_idx) (MarginalDensityAssociator.h:95-118) of the (optionally adapted)
+// 2-D density, then direct_eval of the 1-D marginal at m queries. The marginal's
+// own points (its Kd-tree order, duplicates merged) are exported through the
+// tree_* outputs (coordinate, weight, mass, abw).
+template <typename K>
+int run_marginal(const Req &r, int dim_idx) {
+  using Assoc = MarginalDensityAssociator<KdeT<2, K>>;
+  MuteCerr mute;
+  KdeT<2, K> kde(make_points<2, K>(r.n, r.xy, r.w), 2);
+  set_bw(kde.kernel(), r.h);
+  if (r.alpha >= 0) kde.adapt_density(r.alpha, r.rel, r.abs);
+  typename Assoc::MarginalDensityType m = Assoc::marginal_density(kde, (size_t)dim_idx);
+  if (r.m > 0 && r.q && r.out) threaded_direct_eval(m, r.m, r.q, r.out, r.nthreads);
+  export_tree(m, r.tree_xy, r.tree_w, r.tree_mass, r.tree_abw, r.n_tree);
+  return 0;
+}
+
 // A KernelDensity kept alive across calls, for timing repeated direct_eval
 // batches without rebuilding the Kd-tree (bench.py's CPU baseline).
 struct Handle {
@@ -308,6 +390,41 @@ int ref_kde_lsq_numint_cv(int kind, const double *h, int64_t n, const double *xy
           nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, cv, 1};
     NumintReq g{x0, x1, y0, y1, sx, sy};
     return dispatch_numint(r, g);
+  } catch (const std::invalid_argument &) { return 2; }
+  catch (...) { return 9; }
+}
+
+// KernelDensity::eval(queries, rel_err, abs_err) (see run_tree_eval), after an
+// exact adapt_density(alpha, 0, 0) when alpha >= 0. Exports the data points in
+// tree order like ref_kde_eval. Returns 2 on invalid arguments, 5 unsupported.
+int ref_kde_tree_eval(int kind, int dim, const double *h, int64_t n, const double *xy,
+                      const double *w, double alpha, double rel, double abs, int64_t m,
+                      const double *q, double *out_q, double *out, int64_t *m_out,
+                      double *tree_xy, double *tree_w, double *tree_mass, double *tree_abw,
+                      int64_t *n_tree) {
+  try {
+    Req r{kind, dim, h, n, xy, w, alpha, rel, abs, m, q, out,
+          tree_xy, tree_w, tree_mass, tree_abw, n_tree, nullptr, nullptr, 1};
+    return dispatch_tree_eval(r, out_q, m_out);
+  } catch (const std::invalid_argument &) { return 2; }
+  catch (...) { return 9; }
+}
+
+// The 1-D marginal density of a 2-D product-kernel density (see run_marginal):
+// kind GAUSS_PROD2D or EPAN_PROD2D; adapt_density(alpha, rel, abs) first when
+// alpha >= 0; direct_eval at m 1-D queries.
+int ref_kde_marginal_direct(int kind, const double *h, int64_t n, const double *xy,
+                            const double *w, double alpha, double rel, double abs, int dim_idx,
+                            int64_t m, const double *q, double *out, double *tree_x,
+                            double *tree_w, double *tree_mass, double *tree_abw,
+                            int64_t *n_tree, int nthreads) {
+  try {
+    Req r{kind, 2, h, n, xy, w, alpha, rel, abs, m, q, out,
+          tree_x, tree_w, tree_mass, tree_abw, n_tree, nullptr, nullptr, nthreads};
+    if (dim_idx != 0 && dim_idx != 1) return 2;
+    if (kind == GAUSS_PROD2D) return run_marginal<GaussianProductKernel2d<double>>(r, dim_idx);
+    if (kind == EPAN_PROD2D) return run_marginal<EpanechnikovProductKernel2d<double>>(r, dim_idx);
+    return 5;
   } catch (const std::invalid_argument &) { return 2; }
   catch (...) { return 9; }
 }

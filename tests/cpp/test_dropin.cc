@@ -150,7 +150,7 @@ void test_kernel_density() {
   // adapt_density (KernelDensityImpl.h:291-359): check the local bandwidths
   // against an FP64 CPU pilot pass.
   kde.kernel().set_bandwidths(0.05f, 0.05f);
-  kde.adapt_density(0.5);
+  kde.adapt_density(0.5, 0.0, 0.0);   // rel_err = abs_err = 0: the exact pilot
   const auto &pts = kde.points();
   GaussianProductKernel2d<double> kp(0.05f, 0.05f);
   double logg = 0;
@@ -172,6 +172,23 @@ void test_kernel_density() {
     if (!ok) why = "i=" + std::to_string(i);
   }
   report("KernelDensity::adapt_density", ok, ok ? "" : why);
+
+  // The reference's default tolerances (rel 1e-6, abs 1e-6): every pilot value
+  // within max(1e-6 f, 1e-6) / 2 of the exact one (plus FP32 rounding), so the
+  // bandwidth factor (f / g)^-1/2 moves by at most half that relative change
+  // and half the relative change of g.
+  std::vector<double> abw_exact(pts.size());
+  for (size_t i = 0; i < pts.size(); ++i) abw_exact[i] = double(pts[i].attributes().abw());
+  kde.adapt_density(0.5);
+  ok = true;
+  for (size_t i = 0; i < pts.size() && ok; ++i) {
+    const double rel_pilot = 0.5e-6 * std::max(1.0, 1.0 / pilot[i]) + 2e-7;
+    ok = approximately_equal(abw_exact[i], double(pts[i].attributes().abw()),
+                             rel_pilot + 1e-6, 0.0);
+    if (!ok) why = "i=" + std::to_string(i);
+  }
+  report("KernelDensity::adapt_density (rel 1e-6, abs 1e-6)", ok, ok ? "" : why);
+  kde.adapt_density(0.5, 0.0, 0.0);
 
   // adaptive direct_eval uses the adapted attributes
   kde.direct_eval(queries);
@@ -242,9 +259,22 @@ void test_gaussian_likelihood() {
       if (j != i) f += pts[j].attributes().mass() * k.unnormalized_eval(pts[i].point(), pts[j].point());
     lik += pts[i].attributes().weight() * std::log(f * k.normalization());
   }
-  double gl = kde.likelihood_cross_validate();
+  double gl = kde.likelihood_cross_validate(0.0, 0.0);   // exact sums
   report("likelihood_cross_validate (Gaussian, FP32C)", approximately_equal(gl, lik, 1e-6, 0.0),
          std::to_string(gl) + " vs " + std::to_string(lik));
+  // Default tolerances (rel 1e-6, abs 1e-6): each leave-one-out density within
+  // max(1e-6 f, 1e-6) / 2, so each log term within that over f.
+  double bound = 0;
+  for (size_t i = 0; i < pts.size(); ++i) {
+    double f = 0;
+    for (size_t j = 0; j < pts.size(); ++j)
+      if (j != i) f += pts[j].attributes().mass() * k.unnormalized_eval(pts[i].point(), pts[j].point());
+    f *= k.normalization();
+    bound += pts[i].attributes().weight() * (0.5e-6 * std::max(f, 1.0) + 2e-7 * f) / f;
+  }
+  double gt = kde.likelihood_cross_validate();
+  report("likelihood_cross_validate (rel 1e-6, abs 1e-6)", std::fabs(gt - lik) <= bound,
+         std::to_string(gt) + " vs " + std::to_string(lik) + " bound " + std::to_string(bound));
 }
 
 void test_one_dimensional() {

@@ -41,7 +41,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_abi_version_and_status_strings():
     lib = bk.load_library()
-    assert lib.bbkde_abi_version() == 1
+    assert lib.bbkde_abi_version() == 2
     assert lib.bbkde_status_string(bk.OUT_OF_RANGE) == b"out of range"
     assert lib.bbkde_status_string(bk.INVALID_ARGUMENT) == b"invalid argument"
     assert lib.bbkde_status_string(99) == b"unknown status"

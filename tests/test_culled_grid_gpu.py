@@ -152,7 +152,16 @@ def test_adapt_density_tol_matches_exact_pilot(ctx, kind, h):
     with pytest.raises(bk.InvalidArgument):
         ctx.adapt_density_tol(desc, 1.5)
     with pytest.raises(bk.InvalidArgument):
-        ctx.adapt_density_tol(desc, 0.5, rel_tol=0.0)
+        ctx.adapt_density_tol(desc, 0.5, rel_tol=-1e-3)
+    with pytest.raises(bk.InvalidArgument):
+        ctx.adapt_density_tol(desc, 0.5, rel_tol=1e-6, abs_tol=-1.0)
+    # rel = abs = 0: every tile that does not flush to zero is summed
+    abw, _, pilot, _ = ctx.adapt_density_tol(desc, 0.5, rel_tol=0.0, abs_tol=0.0)
+    np.testing.assert_allclose(pilot, pilot0, rtol=1e-6, atol=0)
+    # an absolute tolerance alone: every pilot value within abs / 2 plus FP32C error
+    abs_tol = 1e-3 * float(pilot0.min())
+    abw, _, pilot, _ = ctx.adapt_density_tol(desc, 0.5, rel_tol=0.0, abs_tol=abs_tol)
+    assert np.all(np.abs(pilot - pilot0) <= 0.5 * abs_tol + 1e-6 * pilot0)
     with pytest.raises(bk.BBKDEError) as e:
         ctx.adapt_density_tol(bk.kernel_desc(W.EPAN_PROD_CONV2D, 2, (0.1, 0.1)), 0.5)
     assert e.value.status == bk.UNSUPPORTED
