@@ -43,7 +43,7 @@ EXPORTED = [
     "bbkde_surrogate_load", "bbkde_surrogate_set_inference", "bbkde_eval_culled",
     "bbkde_eval_grid", "bbkde_lsq_numint_cv", "bbkde_surrogate_set_engine",
     "bbkde_adapt_density_tol", "bbkde_likelihood_cv_tol", "bbkde_lsq_conv_cv_tol",
-    "bbkde_eval_tol", "bbkde_cv_batch_counts",
+    "bbkde_eval_tol", "bbkde_cv_batch_info", "bbkde_ctx_set_cv_plan",
 ]
 
 # Surrogate inference engines (bbkde_surrogate_set_engine).
@@ -195,7 +195,9 @@ def load_library(path: str = LIB_PATH):
     lib.bbkde_surrogate_set_engine.argtypes = [vp, C.c_int]
     lib.bbkde_eval_culled.argtypes = [vp, kd, C.c_int, C.c_double, vp, C.c_int,
                                       C.POINTER(CullStats)]
-    lib.bbkde_cv_batch_counts.argtypes = [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+    lib.bbkde_cv_batch_info.argtypes = [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64),
+                                        C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    lib.bbkde_ctx_set_cv_plan.argtypes = [vp, C.c_int]
     lib.bbkde_eval_tol.argtypes = [vp, kd, C.c_int, C.c_double, C.c_double, vp, C.c_int,
                                    C.POINTER(CullStats)]
     lib.bbkde_eval_grid.argtypes = [vp, vp, kd, C.POINTER(Grid), C.POINTER(GridConfig), vp,
@@ -380,11 +382,17 @@ class Context:
                                             _p(hy), precision, _p(lik), _p(lsq)))
         return lik[:n], lsq[:n]
 
-    def cv_batch_counts(self):
-        """(likelihood pairs, convolution pairs) in support in the last cv_batch."""
-        a, b = C.c_int64(0), C.c_int64(0)
-        self._check(self.lib.bbkde_cv_batch_counts(self.h, C.byref(a), C.byref(b)))
-        return a.value, b.value
+    def cv_batch_info(self):
+        """(likelihood pairs, convolution pairs in support, plan, number of plans) of
+        the last cv_batch."""
+        a, b, p, n = C.c_int64(0), C.c_int64(0), C.c_int(0), C.c_int(0)
+        self._check(self.lib.bbkde_cv_batch_info(self.h, C.byref(a), C.byref(b), C.byref(p),
+                                                 C.byref(n)))
+        return a.value, b.value, p.value, n.value
+
+    def set_cv_plan(self, plan: int):
+        """Force a batched-CV work-item plan (-1: autotune)."""
+        self._check(self.lib.bbkde_ctx_set_cv_plan(self.h, plan))
 
     def eval_culled(self, desc: KernelDesc, rel_tol=1e-7, normalized=True):
         """Culled direct evaluation of every query; returns (values, CullStats)."""

@@ -117,6 +117,10 @@ struct bbkde_ctx {
   cudaGraphExec_t cv_graph = nullptr;
   std::vector<uint64_t> cv_graph_key;
   int64_t cv_counts[2] = {0, 0};   // in-support pairs of the last batched CV launch
+  int cv_forced_plan = -1;         // -1: autotune the batched CV work-item plan
+  int cv_last_plan = -1;
+  // per problem class: device ms of each plan tried so far (< 0: not yet tried)
+  std::map<std::tuple<int, int, int, int, int>, std::vector<double>> cv_tuned;
   // culled evaluation: sorted references, sort scratch, sorted queries, per-block
   // bounds; dense-grid pipeline buffers
   CullCache cull;
@@ -966,8 +970,17 @@ int bbkde_device_info(const bbkde_ctx *c, int *sm_count, int *device) {
 // ===========================================================================
 namespace {
 
-constexpr int kCvChunk = 4096;     // queries per likelihood work item
 constexpr int kCvBlock = 1024;
+
+// Work-item plans of the batched CV launch: likelihood items of `chunk` queries
+// of one set, convolution items of at most `qblock` (<= kCvQBlock) queries of one
+// grid cell. Smaller items balance the 148 persistent blocks better at the end of
+// the launch; larger ones pay the per-item histogram set-up and flush less often.
+struct CvPlan {
+  int chunk, qblock;
+};
+constexpr CvPlan kCvPlans[] = {{4096, 256}, {1024, 256}, {2048, 128}};
+constexpr int kCvNumPlans = 3;
 
 size_t cv_smem_bytes() {
   return sizeof(double) * (4 * kCvHist + 6 * kCvMaxH + 3 * kCvQBlock) +
@@ -1125,8 +1138,34 @@ extern "C" int bbkde_cv_batch(bbkde_ctx *c, int kind, int n_sets, const bbkde_da
     s.diag_wm = diag;
     sum_pairs += (double)n * (double)n;
   }
+  // Work-item plan: forced, or tuned per problem class on the real calls -- the
+  // first calls of a class each run an untried plan (every call returns complete
+  // results whatever its plan; the likelihood sums' FP64 grouping follows the
+  // plan), then the fastest measured plan is kept.
+  const std::tuple<int, int, int, int, int> tkey{
+      n_sets, (int)std::floor(std::log2((double)total)), n_hx, n_hy,
+      (int)std::floor(std::log2(std::max(1.0, sum_pairs)))};
+  int plan_id = 0;
+  std::vector<double> *trials = nullptr;
+  if (c->cv_forced_plan >= 0) {
+    plan_id = c->cv_forced_plan;
+  } else {
+    trials = &c->cv_tuned[tkey];
+    if (trials->empty()) trials->assign(kCvNumPlans, -1.0);
+    int untried = -1;
+    for (int i = 0; i < kCvNumPlans && untried < 0; ++i)
+      if ((*trials)[i] < 0) untried = i;
+    if (untried >= 0) {
+      plan_id = untried;
+    } else {
+      for (int i = 1; i < kCvNumPlans; ++i)
+        if ((*trials)[i] < (*trials)[plan_id]) plan_id = i;
+      trials = nullptr;   // tuned: nothing more to record
+    }
+  }
+  const CvPlan plan = kCvPlans[plan_id];
   // Work items: likelihood items (set, chunk of queries) and convolution items
-  // (set, grid cell, block of <= kCvQBlock queries, x-power group), ordered by
+  // (set, grid cell, block of <= plan.qblock queries, x-power group), ordered by
   // estimated cost so the largest start first.
   std::vector<CvItem> items;
   std::vector<double> cost;
@@ -1135,10 +1174,10 @@ extern "C" int bbkde_cv_batch(bbkde_ctx *c, int kind, int n_sets, const bbkde_da
   for (int sidx = 0; sidx < n_sets; ++sidx) {
     const CvSet &st = hs[sidx];
     part_begin[sidx] = parts;
-    part_count[sidx] = (int)((st.n + kCvChunk - 1) / kCvChunk);
+    part_count[sidx] = (int)((st.n + plan.chunk - 1) / plan.chunk);
     for (int ch = 0; ch < part_count[sidx]; ++ch) {
-      const int64_t q0 = (int64_t)ch * kCvChunk;
-      const int64_t q1 = std::min<int64_t>(st.n, q0 + kCvChunk);
+      const int64_t q0 = (int64_t)ch * plan.chunk;
+      const int64_t q1 = std::min<int64_t>(st.n, q0 + plan.chunk);
       items.push_back({sidx, 0, parts + ch, 0, 0, 0, q0, q1});
       cost.push_back((double)(q1 - q0) * st.n);
     }
@@ -1147,8 +1186,8 @@ extern "C" int bbkde_cv_batch(bbkde_ctx *c, int kind, int n_sets, const bbkde_da
     for (int cy = 0; cy < st.gy; ++cy)
       for (int cx = 0; cx < st.gx; ++cx) {
         const int64_t cb = cst[(int64_t)cy * st.gx + cx], ce = cst[(int64_t)cy * st.gx + cx + 1];
-        for (int64_t q0 = cb; q0 < ce; q0 += kCvQBlock) {
-          const int64_t q1 = std::min<int64_t>(ce, q0 + kCvQBlock);
+        for (int64_t q0 = cb; q0 < ce; q0 += plan.qblock) {
+          const int64_t q1 = std::min<int64_t>(ce, q0 + plan.qblock);
           for (int g = 0; g < 4; ++g) {
             items.push_back({sidx, 1 + g, 0, cx, cy, 0, q0, q1});
             cost.push_back(0.5 * (double)(q1 - q0) * st.n);
@@ -1298,14 +1337,26 @@ extern "C" int bbkde_cv_batch(bbkde_ctx *c, int kind, int n_sets, const bbkde_da
   c->last_launches = 2;
   c->cv_counts[0] = (int64_t)counts[0];
   c->cv_counts[1] = (int64_t)(counts[1] / 4);   // each x-power group counts every pair
+  c->cv_last_plan = plan_id;
+  if (trials) (*trials)[plan_id] = ms;
   return BBKDE_OK;
 }
 
-extern "C" int bbkde_cv_batch_counts(const bbkde_ctx *c, int64_t *lik_pairs,
-                                     int64_t *conv_pairs) {
+extern "C" int bbkde_cv_batch_info(const bbkde_ctx *c, int64_t *lik_pairs, int64_t *conv_pairs,
+                                   int *plan, int *n_plans) {
   if (!c) return BBKDE_INVALID_ARGUMENT;
   if (lik_pairs) *lik_pairs = c->cv_counts[0];
   if (conv_pairs) *conv_pairs = c->cv_counts[1];
+  if (plan) *plan = c->cv_last_plan;
+  if (n_plans) *n_plans = kCvNumPlans;
+  return BBKDE_OK;
+}
+
+extern "C" int bbkde_ctx_set_cv_plan(bbkde_ctx *c, int plan) {
+  TRY(check_ctx(c));
+  if (plan < -1 || plan >= kCvNumPlans)
+    return fail(c, BBKDE_INVALID_ARGUMENT, "cv plan out of range");
+  c->cv_forced_plan = plan;
   return BBKDE_OK;
 }
 

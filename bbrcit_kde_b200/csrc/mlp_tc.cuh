@@ -70,21 +70,48 @@ __device__ __forceinline__ uint64_t tc_desc(uint32_t saddr) {
          ((uint64_t)(128u >> 4) << 32) | (1ull << 46);
 }
 
+// The same stored matrix read transposed, as an MN-major operand: a matrix
+// stored at tc_off(r, k) has its second index k contiguous in 16-byte runs, so
+// read with k as the M (or N) dimension and r as K it is the canonical MN-major
+// layout without swizzle, whose K-direction core-matrix stride goes in the
+// leading byte offset (128 B between groups of 8 r) and the M/N-direction stride
+// in the stride byte offset (2048 B between groups of 8 k). One K = 16 step of
+// such an operand advances 2 x 128 B (a K-major one 2 x 2048 B).
+__device__ __forceinline__ uint64_t tc_desc_mn(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128u >> 4) << 16) |
+         ((uint64_t)(2048u >> 4) << 32) | (1ull << 46);
+}
+constexpr uint32_t kTcAMajorMN = 1u << 15;   // instruction descriptor: A is MN-major
+constexpr uint32_t kTcBMajorMN = 1u << 16;   // B is MN-major
+
 __device__ __forceinline__ void tc_mma(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
-                                       uint32_t accumulate) {
+                                       uint32_t accumulate, uint32_t idesc = kTcIdesc) {
   const uint32_t zero = 0;
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}\n"
       :
-      : "r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(kTcIdesc), "r"(accumulate), "r"(zero));
+      : "r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(zero));
 }
 
 __device__ __forceinline__ void tc_commit(uint32_t mbar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
                ::"r"(mbar)
                : "memory");
+}
+
+// D (+)= A x B over K = 128 (8 instructions of K = 16), M = N = 128. A and B are
+// stored 128 x 128 BF16 matrices at tc_off; a_mn / b_mn read them transposed.
+__device__ __forceinline__ void tc_gemm128(uint32_t tmem_d, uint32_t a, bool a_mn, uint32_t b,
+                                           bool b_mn, bool accumulate) {
+  const uint32_t idesc = kTcIdesc | (a_mn ? kTcAMajorMN : 0u) | (b_mn ? kTcBMajorMN : 0u);
+#pragma unroll
+  for (int s = 0; s < kH / 16; ++s) {
+    const uint64_t ad = a_mn ? tc_desc_mn(a + s * 256) : tc_desc(a + s * 4096);
+    const uint64_t bd = b_mn ? tc_desc_mn(b + s * 256) : tc_desc(b + s * 4096);
+    tc_mma(tmem_d, ad, bd, (accumulate || s > 0) ? 1u : 0u, idesc);
+  }
 }
 
 // Bounded wait for the mbarrier phase `parity` to complete; false on expiry.
@@ -289,6 +316,296 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_mlp_infer_tc(TcArgs ta) {
   if (warp == 0)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
                  "r"(kTcTmemCols));
+}
+
+
+// ===========================================================================
+// Training step on tcgen05: forward and backward of 128 points per CTA.
+//
+// One warpgroup, thread t = point t = TMEM lane t. The four 128 x 128 x 128
+// products of a step run on the tensor cores from the same stored BF16
+// matrices (canonical K-major at tc_off), reading them transposed (MN-major)
+// where the product needs it:
+//   forward   Z2 = A1 W2^T, Z3 = A2 W3^T                 (A, B K-major)
+//   input     dA2 = dZ3 W3, dA1 = dZ2 W2                  (A K-major, B MN-major)
+//   weights   dW3 = dZ3^T A2, dW2 = dZ2^T A1 (K = points) (A, B MN-major)
+// TMEM (512 columns): [0, 128) Z2, kept for silu'(z2); [128, 256) Z3, then dA2,
+// then dA1; [256, 384) dW3, then dW2. The 2 -> 128 and 128 -> 1 layers and every
+// per-feature sum over the points (bias gradients, dW1, dw4) run in FP32 on the
+// CUDA cores; the sums are warp butterflies then a fixed-order sum over the four
+// warps, so a step is deterministic. Rounding points (the FP64 restatement in
+// the tests follows them): A1 = bf16(silu(z1)), A2 = bf16(silu(z2)), dZ3 =
+// bf16(dz3), dZ2 = bf16(dz2); z2, z3, dA and dW stay FP32; bias and vector
+// gradients sum the FP32 dz. Per CTA the gradient partial is written in the
+// parameter layout (k_mlp_reduce sums the partials in a fixed order). Every
+// mbarrier wait is bounded; on expiry *status is set and the CTA stops.
+// ===========================================================================
+constexpr int kTcTrainPts = 128;
+constexpr uint32_t kTcTrainCols = 512;
+
+struct TcTrainSmem {
+  static constexpr size_t kW2 = 0;
+  static constexpr size_t kW3 = kW2 + kTcMatBytes;
+  static constexpr size_t kA1 = kW3 + kTcMatBytes;
+  static constexpr size_t kA2 = kA1 + kTcMatBytes;
+  static constexpr size_t kDZ = kA2 + kTcMatBytes;               // dZ3, then dZ2
+  static constexpr size_t kF = kDZ + kTcMatBytes;                // FP32 vectors
+  static constexpr size_t kFloats = 2 * kH + 4 * kH + 4 * kH;    // W1, b1 b2 b3 w4, red[4][kH]
+  static constexpr size_t kBar = kF + kFloats * sizeof(float);
+  static constexpr size_t kTmem = kBar + 8;
+  static constexpr size_t kFail = kTmem + 8;
+  static constexpr size_t kBytes = kFail + 16;
+};
+
+struct TcTrainArgs {
+  TrainArgs t;
+  int *status;   // set to 1 if a wait expired
+};
+
+// Sum over the 32 lanes of a warp, per index: after the call lane j holds
+// sum_lanes v[j] in v[0] (butterfly: at offset o a lane keeps the half of its
+// window that its bit o selects and adds the partner's copy of it).
+__device__ __forceinline__ float warp_transpose_sum(float (&v)[32], int lane) {
+#pragma unroll
+  for (int o = 16; o >= 1; o >>= 1) {
+    const bool up = (lane & o) != 0;
+#pragma unroll
+    for (int i = 0; i < o; ++i) {
+      const float send = up ? v[i] : v[i + o];
+      const float keep = up ? v[i + o] : v[i];
+      v[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+    }
+  }
+  return v[0];
+}
+
+__global__ void __launch_bounds__(kTcRows, 1) k_mlp_train_tc(TcTrainArgs ta) {
+  using L = TcTrainSmem;
+  extern __shared__ __align__(16) unsigned char smem[];
+  const TrainArgs &a = ta.t;
+  unsigned char *W2 = smem + L::kW2, *W3 = smem + L::kW3, *A1 = smem + L::kA1,
+                *A2 = smem + L::kA2, *DZ = smem + L::kDZ;
+  float *fp = reinterpret_cast<float *>(smem + L::kF);
+  float *W1 = fp, *b1 = W1 + 2 * kH, *b2 = b1 + kH, *b3 = b2 + kH, *w4 = b3 + kH;
+  float *red = w4 + kH;   // [4 warps][kH]
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smem + L::kBar);
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + L::kTmem);
+  volatile int *fail = reinterpret_cast<volatile int *>(smem + L::kFail);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+  for (int i = tid; i < kH * kH; i += kTcRows) {
+    const int n = i / kH, k = i % kH;
+    *reinterpret_cast<__nv_bfloat16 *>(W2 + tc_off(n, k)) = a.w2[i];
+    *reinterpret_cast<__nv_bfloat16 *>(W3 + tc_off(n, k)) = a.w3[i];
+  }
+  for (int i = tid; i < 2 * kH; i += kTcRows) W1[i] = a.params[kOffW1 + i];
+  for (int i = tid; i < kH; i += kTcRows) {
+    b1[i] = a.params[kOffB1 + i];
+    b2[i] = a.params[kOffB2 + i];
+    b3[i] = a.params[kOffB3 + i];
+    w4[i] = a.params[kOffW4 + i];
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)));
+    fail[0] = 0;
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                 ::"r"(smem_u32(tmem_slot)), "r"(kTcTrainCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  // This thread's point.
+  const int64_t p = (int64_t)blockIdx.x * kTcTrainPts + tid;
+  const bool valid = p < a.batch;
+  float x = 0.f, y = 0.f, target = 0.f;
+  if (valid) {
+    const int64_t row = a.index[p];
+    const float2 q = a.xy[row];
+    x = (q.x - a.norm.cx) * a.norm.sx;
+    y = (q.y - a.norm.cy) * a.norm.sy;
+    target = (a.target[row] - a.norm.mu) / a.norm.sigma;
+  }
+  fence_async_smem();
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t lanes = (uint32_t)(warp * 32) << 16;
+  const uint32_t tZ2 = tmem, tZ3 = tmem + 128, tW = tmem + 256;
+  const uint32_t mbar = smem_u32(bar);
+  const uint32_t sW2 = smem_u32(W2), sW3 = smem_u32(W3), sA1 = smem_u32(A1),
+                 sA2 = smem_u32(A2), sDZ = smem_u32(DZ);
+  uint32_t phase = 0;
+  const float b4 = a.params[kOffB4];
+  const float inv_b = 1.0f / (float)a.batch;
+  float *gp = a.grad_part + (int64_t)blockIdx.x * kParams;
+
+  // Issue the products of `body` from thread 0 once every thread's operand
+  // rows are in shared memory; wait for them (bounded). Uniform verdict.
+  auto run = [&](auto body) -> bool {
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    if (tid == 0) {
+      tc_fence_after();
+      body();
+      tc_commit(mbar);
+    }
+    if (!tc_wait(mbar, phase)) fail[0] = 1;
+    phase ^= 1u;
+    tc_fence_after();
+    __syncthreads();
+    return fail[0] == 0;
+  };
+  // Per-feature sums over the CTA's points of v (32 features from c0): the warp
+  // butterfly, then warp partials summed in warp order by thread c0 + lane.
+  auto colsum = [&](float (&v)[32], int c0, float *dst, int stride) {
+    const float s = warp_transpose_sum(v, lane);
+    red[warp * kH + c0 + lane] = s;
+    __syncthreads();
+    if (tid < 32) {
+      const int n = c0 + tid;
+      dst[n * stride] = ((red[n] + red[kH + n]) + red[2 * kH + n]) + red[3 * kH + n];
+    }
+    __syncthreads();
+  };
+  bool ok = true;
+
+  // ---- forward -----------------------------------------------------------
+#pragma unroll 1
+  for (int k0 = 0; k0 < kH; k0 += 8) {
+    float v[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int n = k0 + i;
+      v[i] = silu(fmaf(W1[2 * n], x, fmaf(W1[2 * n + 1], y, b1[n])));
+    }
+    tc_store8<false>(A1, nullptr, tid, k0, v);
+  }
+  ok = run([&] { tc_gemm128(tZ2, sA1, false, sW2, false, false); });
+  if (ok) {
+#pragma unroll 1
+    for (int c = 0; c < kH; c += 32) {
+      float v[32];
+      tc_ld32(tZ2 + lanes + (uint32_t)c, v);
+#pragma unroll
+      for (int i = 0; i < 32; ++i) v[i] = silu(v[i] + b2[c + i]);
+#pragma unroll
+      for (int j = 0; j < 32; j += 8) tc_store8<false>(A2, nullptr, tid, c + j, v + j);
+    }
+    ok = run([&] { tc_gemm128(tZ3, sA2, false, sW3, false, false); });
+  }
+  float out = 0.f;
+  if (ok) {
+#pragma unroll 1
+    for (int c = 0; c < kH; c += 32) {
+      float v[32];
+      tc_ld32(tZ3 + lanes + (uint32_t)c, v);
+#pragma unroll
+      for (int i = 0; i < 32; ++i) out = fmaf(w4[c + i], silu(v[i] + b3[c + i]), out);
+    }
+  }
+  // ---- output layer and dz3 ----------------------------------------------
+  const float e = valid ? out + b4 - target : 0.f;
+  const float dy = 2.f * e * inv_b;   // dL/dy
+  if (ok) {
+#pragma unroll 1
+    for (int c = 0; c < kH; c += 32) {
+      float z[32], dz[32], aw[32];
+      tc_ld32(tZ3 + lanes + (uint32_t)c, z);
+#pragma unroll
+      for (int i = 0; i < 32; ++i) {
+        const float zz = z[i] + b3[c + i];
+        dz[i] = dy * w4[c + i] * silu_grad(zz);
+        aw[i] = dy * silu(zz);
+      }
+#pragma unroll
+      for (int j = 0; j < 32; j += 8) tc_store8<false>(DZ, nullptr, tid, c + j, dz + j);
+      colsum(dz, c, gp + kOffB3, 1);
+      colsum(aw, c, gp + kOffW4, 1);
+    }
+    // dA2 = dZ3 W3 -> [128, 256); dW3 = dZ3^T A2 -> [256, 384)
+    ok = run([&] {
+      tc_gemm128(tZ3, sDZ, false, sW3, true, false);
+      tc_gemm128(tW, sDZ, true, sA2, true, false);
+    });
+  }
+  // ---- dz2, dW3 ------------------------------------------------------------
+  if (ok) {
+#pragma unroll 1
+    for (int c = 0; c < kH; c += 32) {
+      float d[32], z[32];
+      tc_ld32(tZ3 + lanes + (uint32_t)c, d);
+      tc_ld32(tZ2 + lanes + (uint32_t)c, z);
+#pragma unroll
+      for (int i = 0; i < 32; ++i) d[i] *= silu_grad(z[i] + b2[c + i]);
+#pragma unroll
+      for (int j = 0; j < 32; j += 8) tc_store8<false>(DZ, nullptr, tid, c + j, d + j);
+      colsum(d, c, gp + kOffB2, 1);
+    }
+#pragma unroll 1
+    for (int c = 0; c < kH; c += 32) {   // row tid of dW3
+      float g[32];
+      tc_ld32(tW + lanes + (uint32_t)c, g);
+      float4 *dst = reinterpret_cast<float4 *>(gp + kOffW3 + tid * kH + c);
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+        dst[i] = make_float4(g[4 * i], g[4 * i + 1], g[4 * i + 2], g[4 * i + 3]);
+    }
+    // dA1 = dZ2 W2 -> [128, 256); dW2 = dZ2^T A1 -> [256, 384)
+    ok = run([&] {
+      tc_gemm128(tZ3, sDZ, false, sW2, true, false);
+      tc_gemm128(tW, sDZ, true, sA1, true, false);
+    });
+  }
+  // ---- dz1 and the first layer; dW2 --------------------------------------
+  if (ok) {
+#pragma unroll 1
+    for (int c = 0; c < kH; c += 32) {
+      float d[32], dxv[32], dyv[32];
+      tc_ld32(tZ3 + lanes + (uint32_t)c, d);
+#pragma unroll
+      for (int i = 0; i < 32; ++i) {
+        const int n = c + i;
+        d[i] *= silu_grad(fmaf(W1[2 * n], x, fmaf(W1[2 * n + 1], y, b1[n])));
+        dxv[i] = d[i] * x;
+        dyv[i] = d[i] * y;
+      }
+      colsum(d, c, gp + kOffB1, 1);
+      colsum(dxv, c, gp + kOffW1, 2);       // dW1[n][0]
+      colsum(dyv, c, gp + kOffW1 + 1, 2);   // dW1[n][1]
+    }
+#pragma unroll 1
+    for (int c = 0; c < kH; c += 32) {   // row tid of dW2
+      float g[32];
+      tc_ld32(tW + lanes + (uint32_t)c, g);
+      float4 *dst = reinterpret_cast<float4 *>(gp + kOffW2 + tid * kH + c);
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+        dst[i] = make_float4(g[4 * i], g[4 * i + 1], g[4 * i + 2], g[4 * i + 3]);
+    }
+  }
+  // ---- db4 and the loss: fixed-order sums over the points ---------------
+  red[tid] = dy;
+  red[kH + tid] = e * e;
+  __syncthreads();
+  if (tid == 0) {
+    float sd = 0.f, se = 0.f;
+    for (int i = 0; i < kTcTrainPts; ++i) {
+      sd += red[i];
+      se += red[kH + i];
+    }
+    gp[kOffB4] = sd;
+    a.loss_part[blockIdx.x] = se * inv_b;
+  }
+  if (!ok && tid == 0) atomicExch(ta.status, 1);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(kTcTrainCols));
 }
 
 }  // namespace mlp

@@ -42,6 +42,10 @@ struct bbkde_surrogate {
   std::string err;
 };
 
+namespace bbkde {
+int surrogate_check(bbkde_surrogate *s);
+}  // namespace bbkde
+
 namespace {
 
 int sfail(bbkde_surrogate *s, int code, const std::string &m) {
@@ -164,6 +168,28 @@ TrainArgs train_args(bbkde_surrogate *s, int64_t batch) {
   return t;
 }
 
+// Gradient blocks of a batch: 128-point CTAs on tcgen05 (the default engine),
+// 64-point blocks on mma.sync.
+unsigned train_blocks(const bbkde_surrogate *s, int64_t batch) {
+  const int pts = s->engine == BBKDE_ENGINE_TCGEN05 ? kTcTrainPts : kTrainPts;
+  return (unsigned)((batch + pts - 1) / pts);
+}
+
+// One forward + backward pass over targs.batch points into the gradient
+// partials (one per block); returns the number of partials.
+unsigned launch_train(bbkde_surrogate *s, const TrainArgs &targs) {
+  const unsigned blocks = train_blocks(s, targs.batch);
+  if (s->engine == BBKDE_ENGINE_TCGEN05) {
+    TcTrainArgs ta;
+    ta.t = targs;
+    ta.status = s->status;
+    k_mlp_train_tc<<<blocks, kTcRows, TcTrainSmem::kBytes, s->stream>>>(ta);
+  } else {
+    k_mlp_train<<<blocks, kTrainWarps * 32, kTrainSmem, s->stream>>>(targs);
+  }
+  return blocks;
+}
+
 __global__ void k_iota(int64_t *idx, int64_t n) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) idx[i] = i;
@@ -213,7 +239,9 @@ int bbkde_surrogate_create(int device, uint64_t seed, bbkde_surrogate **out) {
         cudaFuncSetAttribute(k_mlp_infer_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)TcSmem<false>::kBytes) != cudaSuccess ||
         cudaFuncSetAttribute(k_mlp_infer_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)TcSmem<true>::kBytes) != cudaSuccess) {
+                             (int)TcSmem<true>::kBytes) != cudaSuccess ||
+        cudaFuncSetAttribute(k_mlp_train_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)TcTrainSmem::kBytes) != cudaSuccess) {
       rc = BBKDE_CUDA_ERROR;
       break;
     }
@@ -291,8 +319,7 @@ int bbkde_surrogate_gradient(bbkde_surrogate *s, int64_t n, const double *xy,
   S_TRY(upload_data(s, n, xy, target));
   S_TRY(ensure_parts(s, n));
   k_iota<<<(unsigned)((n + 255) / 256), 256, 0, s->stream>>>(s->index, n);
-  const unsigned blocks = (unsigned)((n + kTrainPts - 1) / kTrainPts);
-  k_mlp_train<<<blocks, kTrainWarps * 32, kTrainSmem, s->stream>>>(train_args(s, n));
+  const unsigned blocks = launch_train(s, train_args(s, n));
   AdamArgs a = {};
   a.grad_part = s->grad_part;
   a.nparts = (int)blocks;
@@ -311,6 +338,7 @@ int bbkde_surrogate_gradient(bbkde_surrogate *s, int64_t n, const double *xy,
                               s->stream));
   S_CUDA(s, cudaMemcpyAsync(&l, s->loss, sizeof(float), cudaMemcpyDeviceToHost, s->stream));
   S_CUDA(s, cudaStreamSynchronize(s->stream));
+  S_TRY(bbkde::surrogate_check(s));
   if (loss) *loss = l;
   return BBKDE_OK;
 }
@@ -343,7 +371,7 @@ int bbkde_surrogate_train(bbkde_surrogate *s, int64_t n, const double *xy, const
   S_TRY(upload_data(s, n, xy, target));
   const int64_t batch = cfg->batch;
   S_TRY(ensure_parts(s, batch));
-  const unsigned blocks = (unsigned)((batch + kTrainPts - 1) / kTrainPts);
+  const unsigned blocks = train_blocks(s, batch);
   const double b1 = cfg->beta1 > 0 ? cfg->beta1 : 0.9, b2 = cfg->beta2 > 0 ? cfg->beta2 : 0.999;
   const double eps = cfg->eps > 0 ? cfg->eps : 1e-8;
   const double lr0 = cfg->lr, lr1 = cfg->lr_final;
@@ -354,7 +382,7 @@ int bbkde_surrogate_train(bbkde_surrogate *s, int64_t n, const double *xy, const
     const double lr = lr1 + 0.5 * (lr0 - lr1) * (1.0 + std::cos(3.14159265358979323846 * frac));
     k_mlp_batch<<<(unsigned)((batch + 255) / 256), 256, 0, s->stream>>>(
         s->index, batch, n, cfg->seed, (uint64_t)(s->adam_step + k));
-    k_mlp_train<<<blocks, kTrainWarps * 32, kTrainSmem, s->stream>>>(targs);
+    launch_train(s, targs);
     AdamArgs a = {};
     a.grad_part = s->grad_part;
     a.nparts = (int)blocks;
@@ -398,6 +426,7 @@ int bbkde_surrogate_train(bbkde_surrogate *s, int64_t n, const double *xy, const
   float l = 0.f;
   S_CUDA(s, cudaMemcpyAsync(&l, s->loss, sizeof(float), cudaMemcpyDeviceToHost, s->stream));
   S_CUDA(s, cudaStreamSynchronize(s->stream));
+  S_TRY(bbkde::surrogate_check(s));
   if (final_loss) *final_loss = l;
   return BBKDE_OK;
 }
@@ -452,14 +481,14 @@ int surrogate_infer(bbkde_surrogate *s, cudaStream_t st, int64_t n, const float2
   return BBKDE_OK;
 }
 
-// After the stream has been synchronised: BBKDE_TIMEOUT if an inference kernel
-// gave up waiting on the tensor cores (the flag is cleared).
+// After the stream has been synchronised: BBKDE_TIMEOUT if a tcgen05 kernel
+// (inference or training) gave up waiting on the tensor cores (the flag is cleared).
 int surrogate_check(bbkde_surrogate *s) {
   int flag = 0;
   S_CUDA(s, cudaMemcpy(&flag, s->status, sizeof(int), cudaMemcpyDeviceToHost));
   if (flag) {
     cudaMemset(s->status, 0, sizeof(int));
-    return sfail(s, BBKDE_TIMEOUT, "surrogate inference: tensor-core wait expired");
+    return sfail(s, BBKDE_TIMEOUT, "surrogate: tensor-core wait expired");
   }
   return BBKDE_OK;
 }

@@ -933,7 +933,7 @@ def run_cv_batch(a, world, rank, local):
     clocks = sampler.stop()
     launches = (ctx.launch_count() - launches0) // (a.steps + a.warmup)
     _, pairs, _ = ctx.last_launch_stats()
-    lik_pairs, conv_pairs = ctx.cv_batch_counts()
+    lik_pairs, conv_pairs, plan, n_plans = ctx.cv_batch_info()
     lik, lsq = res["out"]
     # Exactness: a few (dataset, hx, hy) against the per-bandwidth FP64 pair sums.
     small = int(np.argmin([len(s) for s in sets]))
@@ -983,7 +983,9 @@ def run_cv_batch(a, world, rank, local):
                     "achieved": atomics / (kms / 1e3) / 1e9, "peak": peak / 1e9,
                     "unit": "G atomics/s", "frac": atomics / (kms / 1e3) / peak,
                     "traffic": None, "lik_pairs_in_support": lik_pairs,
-                    "conv_pairs_in_support": conv_pairs, "kernel_ms_per_launch": kms},
+                    "conv_pairs_in_support": conv_pairs, "kernel_ms_per_launch": kms,
+                    "work_item_plan": plan, "plans": n_plans,
+                    "plan_note": "autotuned on the warm-up calls (each untried plan once)"},
           gpu_launches=int(launches), exactness_vs_fp64_per_bandwidth=checks, cpu_baseline=cpu,
           pairs_per_s=pairs * world / (kms / 1e3))
     return 0

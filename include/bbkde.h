@@ -232,13 +232,24 @@ BBKDE_API int bbkde_cv_batch(bbkde_ctx *ctx, int kind, int n_sets, const bbkde_d
                              int n_hx, const double *hx, int n_hy, const double *hy,
                              int precision, double *lik_out, double *lsq_out);
 
-/* In-support pair counts of the last bbkde_cv_batch launch on this context (the
- * units of its shared-memory bound): lik_pairs ordered pairs with |dx| < hx_max
- * and |dy| < hy_max (4 64-bit shared-memory atomic adds each), conv_pairs
- * unordered pairs with |dx| < 2 hx_max and |dy| < 2 hy_max (16 each, 4 per
- * x-power group). No reference counterpart. */
-BBKDE_API int bbkde_cv_batch_counts(const bbkde_ctx *ctx, int64_t *lik_pairs,
-                                    int64_t *conv_pairs);
+/* Statistics of the last bbkde_cv_batch launch on this context: the in-support
+ * pair counts (the units of its shared-memory bound) -- lik_pairs ordered pairs
+ * with |dx| < hx_max and |dy| < hy_max (4 64-bit shared-memory atomic adds each),
+ * conv_pairs unordered pairs with |dx| < 2 hx_max and |dy| < 2 hy_max (16 each)
+ * -- and the work-item plan it ran, of n_plans. Any pointer may be NULL. No
+ * reference counterpart. */
+BBKDE_API int bbkde_cv_batch_info(const bbkde_ctx *ctx, int64_t *lik_pairs, int64_t *conv_pairs,
+                                  int *plan, int *n_plans);
+
+/* Work-item plan of the batched CV launch (likelihood items of 4096, 1024 or 2048
+ * queries; convolution items of up to 256, 256 or 128 queries of one grid cell).
+ * By default (-1) the context autotunes per problem class (number of sets, log2
+ * of the total points and of the pair count, grid shape): the first calls of a
+ * class each run a plan not yet tried -- every call returns complete results --
+ * and later calls keep the fastest measured. Results of different plans agree
+ * to FP64 rounding (the likelihood sums are grouped by item). plan in
+ * [0, n_plans) forces that plan. No reference counterpart. */
+BBKDE_API int bbkde_ctx_set_cv_plan(bbkde_ctx *ctx, int plan);
 
 /* ---- learned log-density surrogate ---------------------------------------- */
 
@@ -298,9 +309,14 @@ BBKDE_API int bbkde_surrogate_predict_device(bbkde_surrogate *s, int64_t n, cons
  * tensor-core work. */
 BBKDE_API int bbkde_surrogate_set_inference(bbkde_surrogate *s, int split_activations);
 
-/* Inference kernel: BBKDE_ENGINE_TCGEN05 (default; tcgen05.mma with TMEM
- * accumulators, 128-point tiles) or BBKDE_ENGINE_MMA_SYNC (mma.sync.m16n8k16,
- * 16 points per warp). Same arithmetic; results agree to FP32 summation order. */
+/* Tensor-core engine of inference, training and bbkde_surrogate_gradient:
+ * BBKDE_ENGINE_TCGEN05 (default; tcgen05.mma with TMEM accumulators, 128-point
+ * tiles; the backward products read the stored BF16 matrices transposed as
+ * MN-major operands) or BBKDE_ENGINE_MMA_SYNC (mma.sync.m16n8k16, 16 points per
+ * warp). Inference: same arithmetic, results agree to FP32 summation order.
+ * Training: the tcgen05 step keeps pre-activations and input gradients in FP32
+ * (TMEM) and rounds to BF16 only the operands of the products; the mma.sync step
+ * also stores pre-activations and gradients as BF16. */
 enum { BBKDE_ENGINE_TCGEN05 = 0, BBKDE_ENGINE_MMA_SYNC = 1 };
 BBKDE_API int bbkde_surrogate_set_engine(bbkde_surrogate *s, int engine);
 

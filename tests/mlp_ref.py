@@ -84,3 +84,37 @@ def loss_and_grad(p, xin, t, emulate_bf16=False):
     grads["W1"] = dz1.T @ xin
     grads["b1"] = dz1.sum(0)
     return loss, pack(grads)
+
+
+def loss_and_grad_tc(p, xin, t):
+    """Mean squared error and its gradient with the rounding points of the
+    tcgen05 training step (k_mlp_train_tc): BF16 hidden weights and BF16
+    activations and output gradients as the operands of the four 128 x 128
+    products, everything else (pre-activations, input gradients, bias and vector
+    gradients, the first and last layer) unrounded."""
+    n = xin.shape[0]
+    g = unpack(p)
+    W2, W3 = bf16(g["W2"]), bf16(g["W3"])
+    z1 = xin @ g["W1"].T + g["b1"]
+    a1 = bf16(silu(z1))
+    z2 = a1 @ W2.T + g["b2"]
+    a2 = bf16(silu(z2))
+    z3 = a2 @ W3.T + g["b3"]
+    a3 = silu(z3)
+    y = a3 @ g["w4"] + g["b4"][0]
+    e = y - t
+    loss = np.mean(e * e)
+    dy = 2.0 * e / n
+    grads = {"w4": a3.T @ dy, "b4": np.array([dy.sum()])}
+    dz3 = np.outer(dy, g["w4"]) * silu_grad(z3)
+    grads["b3"] = dz3.sum(0)
+    dZ3 = bf16(dz3)
+    grads["W3"] = dZ3.T @ a2
+    dz2 = (dZ3 @ W3) * silu_grad(z2)
+    grads["b2"] = dz2.sum(0)
+    dZ2 = bf16(dz2)
+    grads["W2"] = dZ2.T @ a1
+    dz1 = (dZ2 @ W2) * silu_grad(z1)
+    grads["W1"] = dz1.T @ xin
+    grads["b1"] = dz1.sum(0)
+    return loss, pack(grads)

@@ -93,3 +93,35 @@ def test_cv_batch_gaussian_loop_and_errors(ctx):
         ctx.cv_batch(bk.EPANECHNIKOV_PRODUCT_2D, datasets, np.linspace(0.01, 1, 65), hy)
     with pytest.raises(bk.BBKDEError):
         ctx.cv_batch(bk.GAUSSIAN, datasets, hx, hy)
+
+
+def test_cv_batch_plans_and_autotuner(ctx):
+    """Every work-item plan gives the same scores (likelihood to FP64 rounding,
+    LSQ bit-equal: fixed-point moments); without a forced plan the first calls of
+    a problem class run each plan once, then the fastest is kept; the launch
+    statistics count the in-support pairs."""
+    sets = W.config3_datasets(n_sets=2, sizes=[9000, 3000])
+    datasets = [(s, None) for s in sets]
+    h = W.config3_bandwidths()[::4]
+    res = []
+    for plan in range(3):
+        ctx.set_cv_plan(plan)
+        res.append(ctx.cv_batch(bk.EPANECHNIKOV_PRODUCT_2D, datasets, h, h))
+        lik_pairs, conv_pairs, used, n_plans = ctx.cv_batch_info()
+        assert used == plan and n_plans == 3
+        assert 0 < lik_pairs <= 9000 ** 2 + 3000 ** 2
+        assert 0 < conv_pairs <= (9000 ** 2 + 3000 ** 2) // 2
+    for lik, lsq in res[1:]:
+        _close(lik, res[0][0], 1e-12)
+        np.testing.assert_array_equal(lsq, res[0][1])
+    with pytest.raises(bk.InvalidArgument):
+        ctx.set_cv_plan(3)
+    ctx.set_cv_plan(-1)
+    sets2 = W.config3_datasets(n_sets=3, sizes=[5000, 4000, 3000])   # a new problem class
+    ds2 = [(s, None) for s in sets2]
+    used = []
+    for _ in range(5):
+        ctx.cv_batch(bk.EPANECHNIKOV_PRODUCT_2D, ds2, h, h)
+        used.append(ctx.cv_batch_info()[2])
+    assert sorted(used[:3]) == [0, 1, 2]
+    assert used[3] == used[4]
