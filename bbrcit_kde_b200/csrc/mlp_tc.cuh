@@ -548,10 +548,10 @@ __global__ void __launch_bounds__(kTcRows, 1) k_mlp_train_tc(TcTrainArgs ta) {
     for (int c = 0; c < kH; c += 32) {   // row tid of dW3
       float g[32];
       tc_ld32(tW + lanes + (uint32_t)c, g);
-      float4 *dst = reinterpret_cast<float4 *>(gp + kOffW3 + tid * kH + c);
+      // scalar stores: a partial starts at block * kParams floats, only 4-byte aligned
+      float *dst = gp + kOffW3 + tid * kH + c;
 #pragma unroll
-      for (int i = 0; i < 8; ++i)
-        dst[i] = make_float4(g[4 * i], g[4 * i + 1], g[4 * i + 2], g[4 * i + 3]);
+      for (int i = 0; i < 32; ++i) dst[i] = g[i];
     }
     // dA1 = dZ2 W2 -> [128, 256); dW2 = dZ2^T A1 -> [256, 384)
     ok = run([&] {
@@ -580,10 +580,9 @@ __global__ void __launch_bounds__(kTcRows, 1) k_mlp_train_tc(TcTrainArgs ta) {
     for (int c = 0; c < kH; c += 32) {   // row tid of dW2
       float g[32];
       tc_ld32(tW + lanes + (uint32_t)c, g);
-      float4 *dst = reinterpret_cast<float4 *>(gp + kOffW2 + tid * kH + c);
+      float *dst = gp + kOffW2 + tid * kH + c;
 #pragma unroll
-      for (int i = 0; i < 8; ++i)
-        dst[i] = make_float4(g[4 * i], g[4 * i + 1], g[4 * i + 2], g[4 * i + 3]);
+      for (int i = 0; i < 32; ++i) dst[i] = g[i];
     }
   }
   // ---- db4 and the loss: fixed-order sums over the points ---------------
