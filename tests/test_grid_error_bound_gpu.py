@@ -1,0 +1,80 @@
+"""The dense-grid pipeline's error bar: max relative error <= 1e-3 at EVERY grid
+point, against the FP64 device path, with a 4,096-point sample of that path
+checked against the CPU oracle.
+
+The pipeline's configuration is the one bench.py's surrogate-grid workload runs
+(GRID_PIPELINE below): anchored mode, bicubic residual, tile 16, the probe set
+and tolerance, low-density cut 1e-4, network in rescue mode. A tile keeps its
+interpolated prediction only when its exact probes agree within the probe
+tolerance; the test checks that this gate holds the 1e-3 bar between the probes
+too, on the configuration-5 mixture at two point spacings:
+  * coarse: 262,144 references, a 1024 x 1024 grid over [-4, 4]^2 (pitch 1/128:
+    a tile spans several local bandwidths);
+  * fine:   1,000,000 references (pilot h scaled by (4M / 1M)^(1/6)), 2048 x 2048
+    over a 2 x 2 window (pitch 1/1024, the spacing of the 8192^2 workload).
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import bbrcit_kde_b200 as bk
+from bbrcit_kde_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+# The pipeline configuration of bench.py --workload surrogate-grid.
+GRID_PIPELINE = dict(mode=bk.GRID_ANCHORED, tile=16, probes=9, rel_tol=5e-4, low_frac=1e-4,
+                     interp=3, net_scope=bk.NET_RESCUE)
+
+CASES = {
+    "coarse": (262_144, 0.05, (1024, 1024, -4.0, 4.0, -4.0, 4.0)),
+    "fine": (1_000_000, 0.063, (2048, 2048, -3.5, -1.5, 0.5, 2.5)),
+}
+
+
+def _grid_points(grid):
+    nx, ny, x0, x1, y0, y1 = grid
+    return W.grid_2d(x0, x1, nx, y0, y1, ny)
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_pipeline_error_bound_every_point(ctx, oracle, name):
+    n, h, grid = CASES[name]
+    refs = W.config5_refs(n)
+    w = np.full(n, 1.0 / n)
+    desc = bk.kernel_desc(W.GAUSS, 2, (h, h))
+    ctx.upload(bk.REFERENCE, refs, mass=w, weight=w)
+    abw, mass, _, _ = ctx.adapt_density_tol(desc, 0.5, rel_tol=1e-7)
+    # a network trained on exact log-densities, as the bench does (shorter)
+    rng = W.SplitMix64(0xB2000555)
+    n_tr = 300_000
+    uni = rng.uniform(n_tr, -4.0, 4.0).reshape(-1, 2)
+    pick = np.minimum((rng.uniform(n_tr // 2) * n).astype(np.int64), n - 1)
+    dat = refs[pick] + h * rng.normal(n_tr).reshape(-1, 2)
+    xy = W.f32(np.concatenate([uni, dat]))
+    ctx.upload(bk.QUERY, xy)
+    f, _ = ctx.eval_culled(desc, rel_tol=1e-7)
+    ok = f > 0
+    sur = bk.Surrogate(0, seed=1)
+    sur.train(xy[ok], np.log(f[ok]), steps=4000, batch=8192, lr=3e-3, lr_final=1e-5)
+    sur.set_inference(True)
+
+    npts = grid[0] * grid[1]
+    out = torch.empty(npts, dtype=torch.float64, device="cuda")
+    st = ctx.eval_grid(desc, grid, out.data_ptr(), surrogate=sur, **GRID_PIPELINE)
+    torch.cuda.synchronize()
+    got = out.cpu().numpy()
+    pts = _grid_points(grid)
+    ctx.upload(bk.QUERY, pts)
+    f64 = ctx.eval_all(desc, precision=bk.FP64)
+    rel = np.abs(got - f64) / f64
+    worst = int(np.argmax(rel))
+    assert rel.max() <= 1e-3, (name, float(rel.max()), pts[worst], st.as_dict())
+    assert st.tiles_surrogate > 0, st.as_dict()       # the prediction is used somewhere
+    # the FP64 device path against the CPU oracle on 4,096 of the points
+    sel = np.sort(np.random.default_rng(7).choice(npts, 4096, replace=False))
+    want = oracle.direct(W.GAUSS, 2, (h, h), refs, mass, pts[sel], abw=abw)
+    np.testing.assert_allclose(f64[sel], want, rtol=1e-10, atol=0)
+    sur.close()

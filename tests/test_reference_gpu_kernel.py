@@ -6,8 +6,8 @@ inputs, both against the FP64 oracle.
 The reference sums in plain FP32 (one running float per query, an expf and two
 divisions per pair); the FP32-compensated sum here holds the reference's own
 CPU-vs-GPU criterion approximately_equal(1e-6, 1e-8) (test/test_cukde2.cc:68-70)
-at every query, and the reference kernel is asserted only to its plain-FP32
-accuracy (1e-5 relative)."""
+at every query; the reference kernel is asserted only to plain-FP32 accuracy
+(1e-4 relative: one running float over 30,000 terms)."""
 from __future__ import annotations
 
 import ctypes as C
@@ -47,6 +47,6 @@ def test_reference_gpu_kernel_and_ours_against_fp64(ctx, oracle, kind, h):
     ours = ctx.eval_all(bk.kernel_desc(kind, 2, h))
     want = oracle.direct(kind, 2, h, refs, wn, qs)
     s_ours = error_stats(ours, want, 1e-6, 1e-8)
-    s_ref = error_stats(ref_out, want, 1e-5, 1e-8)
+    s_ref = error_stats(ref_out, want, 1e-4, 1e-8)
     assert s_ours["pass_rate"] == 1.0, s_ours
     assert s_ref["pass_rate"] == 1.0, s_ref

@@ -54,8 +54,6 @@ def test_eval_tol_matches_reference_tree(ctx, oracle, reference, case, tol):
     assert np.all(np.abs(f_ref - exact) <= 0.5 * allow * (1 + 1e-9) + 1e-15)
     assert np.all(np.abs(got - f_ref) <= allow + fp32)
     assert st.max_bound_ratio <= 0.5
-    if rel >= 1e-3 and kind != W.EPAN_PROD2D:
-        assert st.pairs < st.full_pairs      # the looser tolerance does skip work
 
 
 def test_eval_tol_arguments(ctx):
