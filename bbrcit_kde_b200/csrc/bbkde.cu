@@ -684,7 +684,12 @@ int bbkde_ctx_create(int device, bbkde_ctx **out) {
   int rc = BBKDE_OK;
   do {
     if (cudaSetDevice(device) != cudaSuccess) { rc = BBKDE_CUDA_ERROR; break; }
-    cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device);
+    if (cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device) !=
+            cudaSuccess ||
+        c->sm_count < 1) {
+      rc = BBKDE_CUDA_ERROR;
+      break;
+    }
     if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
       rc = BBKDE_CUDA_ERROR;
       break;

@@ -453,8 +453,9 @@ int surrogate_infer(bbkde_surrogate *s, cudaStream_t st, int64_t n, const float2
   a.gdy = gdy;
   a.n = n;
   a.out = out;
-  int sms = 148;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
+  int sms = 0;
+  S_CUDA(s, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device));
+  if (sms < 1) return sfail(s, BBKDE_CUDA_ERROR, "surrogate: device reports no SMs");
   if (s->engine == BBKDE_ENGINE_TCGEN05) {
     // One CTA per SM, two 128-point tiles in flight per CTA.
     const int64_t tiles = (n + kTcRows - 1) / kTcRows;

@@ -25,7 +25,9 @@ def test_adapt_density_matches_golden(ctx, oracle, name, precision):
     desc = bk.kernel_desc(kind, dim, h)
     abw, mass, pilot, gm = ctx.adapt_density(desc, 0.5, precision)
     pa, pb = match_by_coords(refs, g["tree_xy"].reshape(-1, dim))
-    rtol = 1e-10 if precision == bk.FP64 else 2e-6
+    # FP32C: the pilot sums are FP32-compensated (~1e-7), g and the attributes
+    # FP64, so abw and mass hold north_star's 1e-6 relative bar.
+    rtol = 1e-10 if precision == bk.FP64 else 1e-6
     np.testing.assert_allclose(abw[pa], g["tree_abw"][pb], rtol=rtol)
     np.testing.assert_allclose(mass[pa], g["tree_mass"][pb], rtol=rtol * 2)
     _, _, _, g_or = oracle.adapt(kind, dim, h, refs, wn, 0.5)
@@ -37,7 +39,10 @@ def test_adapt_density_matches_golden(ctx, oracle, name, precision):
     if precision == bk.FP64:
         np.testing.assert_allclose(vals, g["values"], rtol=1e-9)
     else:
-        assert_parity(vals, g["values"], 1e-5, 1e-8, what=name)
+        # the reference's own CPU-vs-GPU criterion approximately_equal(1e-6, 1e-8)
+        # at every query (pilot and evaluation both FP32-compensated)
+        s = assert_parity(vals, g["values"], 1e-6, 1e-8, what=name)
+        assert s["max_rel_1e3"] <= 1e-6, s
 
 
 def test_adapt_alpha_validation_and_reset(ctx):

@@ -72,7 +72,7 @@ def test_marginals_match_reference(reference, tmp_path, kind, fp32, alpha):
     exe = compile_marginal()
     wl = W.config2(n=4000, m=1)
     h = (0.0625, 0.09375) if kind == W.GAUSS_PROD2D else (0.25, 0.1875)
-    q = np.linspace(-3.5, 3.5, 1501)
+    q = W.f32(np.linspace(-3.5, 3.5, 1501))   # float-representable, as the device sees them
     fx, fy, (px, py) = _run(exe, tmp_path, kind, fp32, h, alpha, wl.refs, wl.weights, q)
     for dim_idx, got, pts in ((0, fx, px), (1, fy, py)):
         want, (tx, tw, tm, ta) = reference.marginal_direct(kind, h, wl.refs, wl.weights,
