@@ -214,9 +214,8 @@ __global__ void __launch_bounds__(T *T / 8, T == 32 ? 4 : 16)
       s_m[STG + i] = rec[u].z;
     }
     __syncthreads();
-    // Factor pair p of sub-chunk sub (references sub + 2p, + 1): its value (the
-    // staged columns are read-only here) and its slot in buffer b.
-    auto factor_val = [&](int sub, int p) -> float2 {
+    // Factor pair p of sub-chunk sub (references sub + 2p, + 1) into buffer b.
+    auto factor = [&](int b, int sub, int p) {
       const int j = foff + sub + 2 * p;
       const float2 c2 = *reinterpret_cast<const float2 *>(&s_c[j]);
       const float2 s2 = *reinterpret_cast<const float2 *>(&s_s[j]);
@@ -231,26 +230,20 @@ __global__ void __launch_bounds__(T *T / 8, T == 32 ? 4 : 16)
         u = __ffma2_rn(s2, dd, f2(1.0f));
         u = make_float2(fmaxf(u.x, 0.f), fmaxf(u.y, 0.f));
       }
-      return __fmul2_rn(m2, u);
+      fbase[b * FBUF + p * T + (fcol ^ swz(p))] = __fmul2_rn(m2, u);
     };
-    auto factor_slot = [&](int b, int p) -> float2 * {
-      return fbase + b * FBUF + p * T + (fcol ^ swz(p));
-    };
-    // The four 128-bit factor loads of step p (buffer b): y rows then x columns.
-    auto load = [&](int b, int p, float4 (&v)[4]) {
+    // acc[4 kr + kc] (+)= y[kr] * x[kc] for factor pair p of buffer b.
+    auto step = [&](int b, int p, float2 (&acc)[16], bool first) {
       const float2 *fx2 = s_fac + b * FBUF + p * T, *fy2 = fx2 + FROWS * T;
       const int w = swz(p);
-      v[0] = *reinterpret_cast<const float4 *>(&fy2[(2 * rg) ^ w]);
-      v[1] = *reinterpret_cast<const float4 *>(&fy2[(T / 2 + 2 * rg) ^ w]);
-      v[2] = *reinterpret_cast<const float4 *>(&fx2[(2 * cg) ^ w]);
-      v[3] = *reinterpret_cast<const float4 *>(&fx2[(T / 2 + 2 * cg) ^ w]);
-    };
-    // acc[4 kr + kc] (+)= y[kr] * x[kc].
-    auto fma16 = [&](const float4 (&v)[4], float2 (&acc)[16], bool first) {
-      const float2 y[4] = {make_float2(v[0].x, v[0].y), make_float2(v[0].z, v[0].w),
-                           make_float2(v[1].x, v[1].y), make_float2(v[1].z, v[1].w)};
-      const float2 x[4] = {make_float2(v[2].x, v[2].y), make_float2(v[2].z, v[2].w),
-                           make_float2(v[3].x, v[3].y), make_float2(v[3].z, v[3].w)};
+      const float4 ya = *reinterpret_cast<const float4 *>(&fy2[(2 * rg) ^ w]);
+      const float4 yb = *reinterpret_cast<const float4 *>(&fy2[(T / 2 + 2 * rg) ^ w]);
+      const float4 xa = *reinterpret_cast<const float4 *>(&fx2[(2 * cg) ^ w]);
+      const float4 xb = *reinterpret_cast<const float4 *>(&fx2[(T / 2 + 2 * cg) ^ w]);
+      const float2 y[4] = {make_float2(ya.x, ya.y), make_float2(ya.z, ya.w),
+                           make_float2(yb.x, yb.y), make_float2(yb.z, yb.w)};
+      const float2 x[4] = {make_float2(xa.x, xa.y), make_float2(xa.z, xa.w),
+                           make_float2(xb.x, xb.y), make_float2(xb.z, xb.w)};
 #pragma unroll
       for (int kr = 0; kr < 4; ++kr)
 #pragma unroll
@@ -258,51 +251,30 @@ __global__ void __launch_bounds__(T *T / 8, T == 32 ? 4 : 16)
           acc[4 * kr + kc] = first ? __fmul2_rn(y[kr], x[kc])
                                    : __ffma2_rn(y[kr], x[kc], acc[4 * kr + kc]);
     };
-    for (int p = ft; p < FROWS; p += NG) *factor_slot(0, p) = factor_val(0, p);
+    for (int p = ft; p < FROWS; p += NG) factor(0, 0, p);
     __syncthreads();
     for (int sb = 0; sb < NSUB; ++sb) {
       const int cur = sb & 1;
       const bool more = sb + 1 < NSUB;
       for (int ch = 0; ch < FROWS / 16; ++ch) {
         float2 acc[16];
-        float4 v[4];
-        load(cur, ch * 16 + sp, v);
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
-          // Software pipeline within the warp, in program order so that no load
-          // of this buffer has to pass a store to the other: the next
-          // sub-chunk's factors are computed into registers, the next step's
-          // operands loaded, this step's products accumulated, and only then
-          // the factors stored.
-          float2 fv[FPB];
-          int fp[FPB];
           if (more) {
 #pragma unroll
-            for (int f = 0; f < FPB; ++f) {
-              fp[f] = ft + ((ch * 8 + i) * FPB + f) * NG;
-              fv[f] = factor_val((sb + 1) * SUB, fp[f]);
-            }
+            for (int f = 0; f < FPB; ++f)
+              factor(cur ^ 1, (sb + 1) * SUB, ft + ((ch * 8 + i) * FPB + f) * NG);
           }
-          float4 vn[4];
-          if (i < 7) load(cur, ch * 16 + 2 * (i + 1) + sp, vn);
-          fma16(v, acc, i == 0);
-          if (more) {
-#pragma unroll
-            for (int f = 0; f < FPB; ++f) *factor_slot(cur ^ 1, fp[f]) = fv[f];
-          }
-          if (i < 7) {
-#pragma unroll
-            for (int u = 0; u < 4; ++u) v[u] = vn[u];
-          }
+          step(cur, ch * 16 + 2 * i + sp, acc, i == 0);
         }
         // Kahan fold, two points per packed op (a - b as fma(b, -1, a): exact
         // negation, one rounding, as the scalar subtraction).
         const float2 m1 = f2(-1.0f);
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
-          const float2 v2 = make_float2(acc[2 * k].x + acc[2 * k].y,
-                                        acc[2 * k + 1].x + acc[2 * k + 1].y);
-          const float2 y = __ffma2_rn(comp[k], m1, v2);
+          const float2 v = make_float2(acc[2 * k].x + acc[2 * k].y,
+                                       acc[2 * k + 1].x + acc[2 * k + 1].y);
+          const float2 y = __ffma2_rn(comp[k], m1, v);
           const float2 t2 = __fadd2_rn(sum[k], y);
           comp[k] = __ffma2_rn(y, m1, __ffma2_rn(sum[k], m1, t2));
           sum[k] = t2;
