@@ -25,6 +25,7 @@
 #include <random>  // the reference headers use std:: distributions without including it
 #include <cstring>
 #include <iostream>
+#include <mutex>
 #include <stdexcept>
 #include <thread>
 #include <vector>
@@ -54,11 +55,30 @@ enum Kind {
 // std::cerr (KernelDensityImpl.h:1113-1143), at rel = abs = 0 for nearly every
 // point; this mutes it for the duration of one call.
 struct MuteCerr {
-  std::streambuf *old;
-  MuteCerr() : old(std::cerr.rdbuf(nullptr)) {}
+  // Calls may run on several host threads at once (the CPU baselines): the first
+  // one in mutes the stream, the last one out restores it.
+  static std::mutex &mu() {
+    static std::mutex m;
+    return m;
+  }
+  static int &depth() {
+    static int d = 0;
+    return d;
+  }
+  static std::streambuf *&saved() {
+    static std::streambuf *b = nullptr;
+    return b;
+  }
+  MuteCerr() {
+    std::lock_guard<std::mutex> lock(mu());
+    if (depth()++ == 0) saved() = std::cerr.rdbuf(nullptr);
+  }
   ~MuteCerr() {
-    std::cerr.rdbuf(old);
-    std::cerr.clear();
+    std::lock_guard<std::mutex> lock(mu());
+    if (--depth() == 0) {
+      std::cerr.rdbuf(saved());
+      std::cerr.clear();
+    }
   }
 };
 
