@@ -1381,6 +1381,10 @@ namespace {
 // tile whose bound is within 2^-24 of the block's largest.
 constexpr float kCullCut = 24.0f;
 
+// Automatic probe set of the grid pipeline (bbkde_grid_config.probes = 0): 5 probes
+// while the tile span is at most this many narrowest kernel widths, else 9.
+constexpr double kGridProbeSpan = 0.75;
+
 // Morton order of n points (x[i * stride], y[i * stride]; y null for 1-D):
 // *perm_out = the sorted permutation (valid until the next sort).
 int morton_sort(bbkde_ctx *c, const float *x, const float *y, int stride, int64_t n,
@@ -1896,12 +1900,13 @@ extern "C" int bbkde_eval_grid(bbkde_ctx *c, bbkde_surrogate *sur, const bbkde_k
       !std::isfinite(grid->x0) || !std::isfinite(grid->x1) || !std::isfinite(grid->y0) ||
       !std::isfinite(grid->y1))
     return fail(c, BBKDE_INVALID_ARGUMENT, "grid: need nx, ny >= 1 and finite x0 < x1, y0 < y1");
-  const int mode = cfg->mode, T = cfg->tile, P = cfg->probes;
+  const int mode = cfg->mode, T = cfg->tile;
+  int P = cfg->probes;
   if (mode < BBKDE_GRID_EXACT || mode > BBKDE_GRID_ANCHORED)
     return fail(c, BBKDE_INVALID_ARGUMENT, "grid: unknown mode");
   if (T != 16 && T != 32) return fail(c, BBKDE_INVALID_ARGUMENT, "grid: tile must be 16 or 32");
-  if (P != 1 && P != 5 && P != 9)
-    return fail(c, BBKDE_INVALID_ARGUMENT, "grid: probes must be 1, 5 or 9");
+  if (P != 0 && P != 1 && P != 5 && P != 9)
+    return fail(c, BBKDE_INVALID_ARGUMENT, "grid: probes must be 0 (automatic), 1, 5 or 9");
   const int interp = cfg->interp == 0 ? 1 : cfg->interp;
   if (interp != 1 && interp != 3)
     return fail(c, BBKDE_INVALID_ARGUMENT, "grid: interp must be 1 (bilinear) or 3 (bicubic)");
@@ -1926,8 +1931,27 @@ extern "C" int bbkde_eval_grid(bbkde_ctx *c, bbkde_surrogate *sur, const bbkde_k
     return fail(c, BBKDE_OUT_OF_RANGE, "grid: too many tiles");
   const int64_t npts = g.nx * g.ny, ntiles = (int64_t)g.ntx * g.nty;
   const bool full = cfg->exact_culled == 0;
+  if (P == 0) {
+    // Automatic probe set: the centre and edge midpoints suffice while a tile spans
+    // at most kGridProbeSpan narrowest kernel widths (h times the smallest abw);
+    // wider tiles vary between those probes, so the quarter points join them.
+    double amin = 1.0;
+    if (rs.n > 0) {
+      k_min_positive<<<1, 1024, 0, c->stream>>>(rs.abw.as<double>(), rs.n,
+                                                c->scalars.as<double>() + 8);
+      COUNT_LAUNCH(c);
+      CUDA_TRY(c, cudaGetLastError());
+      CUDA_TRY(c, cudaMemcpyAsync(&amin, c->scalars.as<double>() + 8, sizeof(double),
+                                  cudaMemcpyDeviceToHost, c->stream));
+      CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    }
+    const double wmin = std::min(r.h1, r.h2) * amin;
+    const double span = T * std::max(g.dx, g.dy);
+    P = span <= kGridProbeSpan * wmin ? 5 : 9;
+  }
   bbkde_grid_stats st = {};
   st.tiles = ntiles;
+  st.probes_used = P;
   if (rs.n == 0) {
     CUDA_TRY(c, cudaMemsetAsync(out, 0, (size_t)npts * sizeof(double), c->stream));
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));

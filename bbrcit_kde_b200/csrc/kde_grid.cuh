@@ -157,6 +157,25 @@ __global__ void k_tile_reduce(GridDesc g, float *pred, const float *resid, int i
 }
 
 // Largest finite value of v[0, n) -> *out (single block).
+// out[0] = the smallest positive finite value of v[0, n) (1.0 if there is none);
+// one block.
+__global__ void k_min_positive(const double *v, int64_t n, double *out) {
+  __shared__ double s[32];
+  double m = INFINITY;
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+    const double x = v[i];
+    if (x > 0.0 && x < m) m = x;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmin(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = fmin(m, s[w]);
+    *out = m < INFINITY ? m : 1.0;
+  }
+}
+
 __global__ void k_max_finite(const float *v, int n, float *out) {
   __shared__ float s[32];
   float m = -INFINITY;

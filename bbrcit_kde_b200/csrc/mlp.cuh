@@ -29,6 +29,9 @@ constexpr int kOffB3 = kOffW3 + kH * kH;
 constexpr int kOffW4 = kOffB3 + kH;
 constexpr int kOffB4 = kOffW4 + kH;
 constexpr int kParams = kOffB4 + 1;   // 33537
+// Distance between two gradient partials in floats: kParams rounded up to a
+// multiple of 4, so that every partial (and its W2, W3 blocks) is 16-byte aligned.
+constexpr int kPartStride = (kParams + 3) & ~3;
 
 constexpr int kLd = kH + 8;           // padded row (bf16 elements) of smem matrices
 
@@ -292,7 +295,7 @@ struct TrainArgs {
   const float *target;          // log-density targets
   const int64_t *index;         // batch -> training row
   int64_t batch;
-  float *grad_part;             // [gridDim.x][kParams]
+  float *grad_part;             // [gridDim.x][kPartStride]
   float *loss_part;             // [gridDim.x]
 };
 
@@ -493,7 +496,7 @@ __global__ void __launch_bounds__(kTrainWarps * 32) k_mlp_train(TrainArgs a) {
   __syncthreads();
 
   // ---- weight gradients: dW3 = dZ3^T A2, dW2 = dZ2^T A1 on the tensor cores ----
-  float *gp = a.grad_part + (int64_t)blockIdx.x * kParams;
+  float *gp = a.grad_part + (int64_t)blockIdx.x * kPartStride;
   const int r0 = warp * 32;
   for (int layer = 0; layer < 2; ++layer) {
     const __nv_bfloat16 *dZ = layer == 0 ? Z3 : Z2;
@@ -589,7 +592,7 @@ __global__ void k_mlp_reduce(AdamArgs a) {
   }
   if (i >= kParams) return;
   float gsum = 0.f;
-  for (int k = 0; k < a.nparts; ++k) gsum += a.grad_part[(int64_t)k * kParams + i];
+  for (int k = 0; k < a.nparts; ++k) gsum += a.grad_part[(int64_t)k * kPartStride + i];
   if (a.grad_out) a.grad_out[i] = gsum;
   if (a.step > 0) {
     float m = a.beta1 * a.m[i] + (1.f - a.beta1) * gsum;

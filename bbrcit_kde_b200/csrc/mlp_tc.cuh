@@ -181,6 +181,24 @@ __device__ __forceinline__ void tc_store8(unsigned char *ahi, unsigned char *alo
     *reinterpret_cast<uint4 *>(alo + tc_off(r, k0)) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
 }
 
+// The two 128 x 128 BF16 weight matrices (row-major [n][k] in global memory)
+// into the canonical layout, 16 bytes (8 consecutive k of one row n) per copy:
+// consecutive threads take consecutive rows, so a warp's shared-memory stores
+// fill 512 contiguous bytes.
+__device__ __forceinline__ void tc_stage_weights(unsigned char *W2, unsigned char *W3,
+                                                 const __nv_bfloat16 *w2,
+                                                 const __nv_bfloat16 *w3, int tid,
+                                                 int nthreads) {
+  const uint4 *g2 = reinterpret_cast<const uint4 *>(w2);
+  const uint4 *g3 = reinterpret_cast<const uint4 *>(w3);
+  for (int i = tid; i < kH * kH / 8; i += nthreads) {
+    const int n = i % kH, k0 = (i / kH) * 8;
+    const int gi = n * (kH / 8) + k0 / 8;
+    *reinterpret_cast<uint4 *>(W2 + tc_off(n, k0)) = __ldg(g2 + gi);
+    *reinterpret_cast<uint4 *>(W3 + tc_off(n, k0)) = __ldg(g3 + gi);
+  }
+}
+
 struct TcArgs {
   InferArgs in;
   int *status;   // set to 1 if a wait expired
@@ -200,11 +218,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_mlp_infer_tc(TcArgs ta) {
 
   const int tid = threadIdx.x, wg = tid >> 7, row = tid & 127, warp = tid >> 5;
   // Weights into the canonical layout; FP32 vectors.
-  for (int i = tid; i < kH * kH; i += kTcThreads) {
-    const int n = i / kH, k = i % kH;
-    *reinterpret_cast<__nv_bfloat16 *>(W2 + tc_off(n, k)) = a.w2[i];
-    *reinterpret_cast<__nv_bfloat16 *>(W3 + tc_off(n, k)) = a.w3[i];
-  }
+  tc_stage_weights(W2, W3, a.w2, a.w3, tid, kTcThreads);
   for (int i = tid; i < 2 * kH; i += kTcThreads) W1[i] = a.params[kOffW1 + i];
   for (int i = tid; i < kH; i += kTcThreads) {
     b1[i] = a.params[kOffB1 + i];
@@ -393,11 +407,7 @@ __global__ void __launch_bounds__(kTcRows, 1) k_mlp_train_tc(TcTrainArgs ta) {
   volatile int *fail = reinterpret_cast<volatile int *>(smem + L::kFail);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
-  for (int i = tid; i < kH * kH; i += kTcRows) {
-    const int n = i / kH, k = i % kH;
-    *reinterpret_cast<__nv_bfloat16 *>(W2 + tc_off(n, k)) = a.w2[i];
-    *reinterpret_cast<__nv_bfloat16 *>(W3 + tc_off(n, k)) = a.w3[i];
-  }
+  tc_stage_weights(W2, W3, a.w2, a.w3, tid, kTcRows);
   for (int i = tid; i < 2 * kH; i += kTcRows) W1[i] = a.params[kOffW1 + i];
   for (int i = tid; i < kH; i += kTcRows) {
     b1[i] = a.params[kOffB1 + i];
@@ -439,7 +449,7 @@ __global__ void __launch_bounds__(kTcRows, 1) k_mlp_train_tc(TcTrainArgs ta) {
   uint32_t phase = 0;
   const float b4 = a.params[kOffB4];
   const float inv_b = 1.0f / (float)a.batch;
-  float *gp = a.grad_part + (int64_t)blockIdx.x * kParams;
+  float *gp = a.grad_part + (int64_t)blockIdx.x * kPartStride;
 
   // Issue the products of `body` from thread 0 once every thread's operand
   // rows are in shared memory; wait for them (bounded). Uniform verdict.
@@ -548,10 +558,11 @@ __global__ void __launch_bounds__(kTcRows, 1) k_mlp_train_tc(TcTrainArgs ta) {
     for (int c = 0; c < kH; c += 32) {   // row tid of dW3
       float g[32];
       tc_ld32(tW + lanes + (uint32_t)c, g);
-      // scalar stores: a partial starts at block * kParams floats, only 4-byte aligned
-      float *dst = gp + kOffW3 + tid * kH + c;
+      // 16-byte stores: partials are kPartStride floats apart (a multiple of 4)
+      float4 *dst = reinterpret_cast<float4 *>(gp + kOffW3 + tid * kH + c);
 #pragma unroll
-      for (int i = 0; i < 32; ++i) dst[i] = g[i];
+      for (int i = 0; i < 8; ++i)
+        dst[i] = make_float4(g[4 * i], g[4 * i + 1], g[4 * i + 2], g[4 * i + 3]);
     }
     // dA1 = dZ2 W2 -> [128, 256); dW2 = dZ2^T A1 -> [256, 384)
     ok = run([&] {
@@ -580,9 +591,10 @@ __global__ void __launch_bounds__(kTcRows, 1) k_mlp_train_tc(TcTrainArgs ta) {
     for (int c = 0; c < kH; c += 32) {   // row tid of dW2
       float g[32];
       tc_ld32(tW + lanes + (uint32_t)c, g);
-      float *dst = gp + kOffW2 + tid * kH + c;
+      float4 *dst = reinterpret_cast<float4 *>(gp + kOffW2 + tid * kH + c);
 #pragma unroll
-      for (int i = 0; i < 32; ++i) dst[i] = g[i];
+      for (int i = 0; i < 8; ++i)
+        dst[i] = make_float4(g[4 * i], g[4 * i + 1], g[4 * i + 2], g[4 * i + 3]);
     }
   }
   // ---- db4 and the loss: fixed-order sums over the points ---------------

@@ -143,7 +143,7 @@ int ensure_parts(bbkde_surrogate *s, int64_t batch) {
     s->grad_part = nullptr;
     s->loss_part = nullptr;
     s->part_cap = 0;
-    if (cudaMalloc(&s->grad_part, blocks * kParams * sizeof(float)) != cudaSuccess ||
+    if (cudaMalloc(&s->grad_part, blocks * kPartStride * sizeof(float)) != cudaSuccess ||
         cudaMalloc(&s->loss_part, blocks * sizeof(float)) != cudaSuccess) {
       cudaGetLastError();
       return sfail(s, BBKDE_ALLOC_FAILED, "cudaMalloc(gradient partials) failed");

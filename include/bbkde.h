@@ -389,10 +389,14 @@ typedef struct {
   int tile;          /* decision tile edge in grid points: 16 or 32 */
   int probes;        /* held-out probes per tile, judged with the tile's interpolant:
                         1 (centre), 5 (+ edge midpoints, shared with the neighbours)
-                        or 9 (+ quarter points). Anchors and the first 5 probes are
-                        the points of one lattice of pitch tile/2 (grid index units)
-                        from the grid's origin, one pitch past its end; the quarter
-                        points a second one: each is one exact grid sum. */
+                        or 9 (+ quarter points); 0 = automatic: 5 while a tile spans
+                        at most 0.75 narrowest kernel widths (h times the smallest
+                        abw of the reference set), else 9 -- the setting that holds
+                        the 1e-3 error bar at every point in the tests. Anchors and
+                        the first 5 probes are the points of one lattice of pitch
+                        tile/2 (grid index units) from the grid's origin, one pitch
+                        past its end; the quarter points a second one: each is one
+                        exact grid sum. */
   int exact_culled;  /* 1: exact parts use the culled sum; 0: the full direct sum */
   double rel_tol;    /* a tile keeps the prediction only if every probe is within */
   double low_frac;   /* tiles whose smallest predicted density is below low_frac
@@ -425,6 +429,7 @@ typedef struct {
                         the lattice and the missed tiles, with their re-check);
                         probe = exact lattices, residual interpolation and probe
                         check; fallback = exact tiles */
+  int64_t probes_used;        /* the probe set the call ran (resolves probes = 0) */
 } bbkde_grid_stats;
 
 /* Normalised density of the REFERENCE set (with its current attributes, e.g.
