@@ -363,10 +363,11 @@ struct Variant {
   int minb;    // __launch_bounds__ minimum resident blocks per SM
   int poly;    // every poly-th reference's exponentials on the FP32 pipe (0: none)
 };
-constexpr Variant kVariants[] = {{8, 256, 2, 0}, {4, 256, 3, 0}, {8, 128, 4, 0},
-                                 {4, 128, 6, 0}, {8, 256, 2, 8}, {8, 128, 4, 8},
-                                 {8, 128, 4, 4}};
-constexpr int kNumVariants = 7;
+constexpr Variant kVariants[] = {{8, 256, 2, 0},  {4, 256, 3, 0},  {8, 128, 4, 0},
+                                 {4, 128, 6, 0},  {8, 256, 2, 8},  {8, 128, 4, 8},
+                                 {8, 128, 4, 4},  {4, 128, 6, 8},  {4, 128, 6, 16},
+                                 {4, 128, 6, 32}, {8, 256, 2, 16}};
+constexpr int kNumVariants = 11;
 constexpr int kDefaultVariant = 0;
 constexpr int kTile = 256;
 constexpr int kBlock64 = 128;
@@ -418,7 +419,11 @@ void launch_f32(int variant, dim3 grid, cudaStream_t st, const SumArgs &a) {
     case 3: launch_shape<OP, D, 4, 128, 6>(grid, st, a); break;
     case 4: launch_shape<OP, D, 8, 256, 2, 8>(grid, st, a); break;
     case 5: launch_shape<OP, D, 8, 128, 4, 8>(grid, st, a); break;
-    default: launch_shape<OP, D, 8, 128, 4, 4>(grid, st, a); break;
+    case 6: launch_shape<OP, D, 8, 128, 4, 4>(grid, st, a); break;
+    case 7: launch_shape<OP, D, 4, 128, 6, 8>(grid, st, a); break;
+    case 8: launch_shape<OP, D, 4, 128, 6, 16>(grid, st, a); break;
+    case 9: launch_shape<OP, D, 4, 128, 6, 32>(grid, st, a); break;
+    default: launch_shape<OP, D, 8, 256, 2, 16>(grid, st, a); break;
   }
 }
 template <int OP, int D>

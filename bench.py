@@ -45,7 +45,7 @@ MUFU_EX2_PER_CLK_PER_SM = 16
 FP32_FMA_PER_CLK_PER_SM = 128
 # FP32-pipe poly stride of each pair-sum launch shape (bbkde_launch_variants order):
 # every k-th reference's exponentials on the FP32 pipe, 0 = all on MUFU.
-VARIANT_POLY = [0, 0, 0, 0, 8, 8, 4]
+VARIANT_POLY = [0, 0, 0, 0, 8, 8, 4, 8, 16, 32, 16]
 
 
 def pair_sum_bound_per_clk_per_sm(poly: int, fma_cycles: float = 12.0) -> tuple[float, str]:

@@ -466,7 +466,7 @@ BBKDE_API int bbkde_last_launch_stats(const bbkde_ctx *ctx, double *kernel_ms, d
 BBKDE_API int64_t bbkde_launch_count(const bbkde_ctx *ctx);
 
 /* Launch shapes of the FP32 pair-sum kernels (queries per thread x threads per
- * block, and for the Gaussians whether every 8th or 4th reference's exponentials
+ * block, and for the Gaussians whether every 4th, 8th, 16th or 32nd reference's exponentials
  * run on the FP32 pipe instead of MUFU.EX2). By default (variant -1) the context
  * autotunes: for problems of at least
  * 2e10 pairs it times every shape on a slice of the problem once per problem
