@@ -571,8 +571,9 @@ def run_surrogate_grid(a, world, rank, local):
     npts = G * G
     out = torch.empty(npts, dtype=torch.float64, device="cuda")
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    # exact parts (lattice, fallback) to 1e-5: 100x below the pipeline's 1e-3 bar
     main_cfg = dict(surrogate=sur, mode=bk.GRID_ANCHORED, tile=16, probes=0, rel_tol=5e-4,
-                    low_frac=1e-4, interp=3)
+                    low_frac=1e-4, interp=3, cull_rel=1e-5)
 
     def grid_step(dst, **kw):
         return ctx.eval_grid(desc, grid, dst.data_ptr(), **kw)
@@ -741,7 +742,8 @@ def run_surrogate_grid(a, world, rank, local):
         "config": {"workload": f"surrogate grid: adaptive Gaussian KDE of {n} refs (pilot "
                                f"h=0.05, alpha=0.5) on a {G}x{G} grid over [-4,4]^2",
                    "pipeline": "bbkde_eval_grid anchored mode, bicubic residual, tile 16, "
-                               "automatic probe set (5 at this spacing), probe tolerance 5e-4, low_frac 1e-4; network in "
+                               "automatic probe set (5 at this spacing), probe tolerance 5e-4, low_frac 1e-4, exact parts "
+                               "culled to 1e-5; network in "
                                "rescue mode (two-term BF16 inference on tcgen05 on the tiles "
                                "the interpolated exact anchors miss)",
                    "l2": "flushed between timed steps (256 MB write)"},

@@ -4,7 +4,8 @@ checked against the CPU oracle.
 
 The pipeline's configuration is the one bench.py's surrogate-grid workload runs
 (GRID_PIPELINE below): anchored mode, bicubic residual, tile 16, the automatic
-probe set, probe tolerance 5e-4, low-density cut 1e-4, network in rescue mode. A tile keeps its
+probe set, probe tolerance 5e-4, low-density cut 1e-4, exact parts (lattice
+and fallback tiles) culled to 1e-5, network in rescue mode. A tile keeps its
 interpolated prediction only when its exact probes agree within the probe
 tolerance; the test checks that this gate holds the 1e-3 bar between the probes
 too, on the configuration-5 mixture at two point spacings:
@@ -28,7 +29,7 @@ torch = pytest.importorskip("torch")
 # picks the probe set (probes = 0): centre and edge midpoints while a tile spans at
 # most 0.75 narrowest kernel widths, the quarter points besides on coarser grids.
 GRID_PIPELINE = dict(mode=bk.GRID_ANCHORED, tile=16, probes=0, rel_tol=5e-4, low_frac=1e-4,
-                     interp=3, net_scope=bk.NET_RESCUE)
+                     interp=3, net_scope=bk.NET_RESCUE, cull_rel=1e-5)
 
 # name -> (references, pilot h, grid, probe set the automatic rule must pick)
 CASES = {
