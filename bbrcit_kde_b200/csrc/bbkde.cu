@@ -1912,6 +1912,9 @@ extern "C" int bbkde_eval_grid(bbkde_ctx *c, bbkde_surrogate *sur, const bbkde_k
   if (T != 16 && T != 32) return fail(c, BBKDE_INVALID_ARGUMENT, "grid: tile must be 16 or 32");
   if (P != 0 && P != 1 && P != 5 && P != 9)
     return fail(c, BBKDE_INVALID_ARGUMENT, "grid: probes must be 0 (automatic), 1, 5 or 9");
+  const int LT = cfg->lattice_tile == 0 ? 16 : cfg->lattice_tile;
+  if (LT != 16 && LT != 32)
+    return fail(c, BBKDE_INVALID_ARGUMENT, "grid: lattice_tile must be 0, 16 or 32");
   const int interp = cfg->interp == 0 ? 1 : cfg->interp;
   if (interp != 1 && interp != 3)
     return fail(c, BBKDE_INVALID_ARGUMENT, "grid: interp must be 1 (bilinear) or 3 (bicubic)");
@@ -2021,7 +2024,7 @@ extern "C" int bbkde_eval_grid(bbkde_ctx *c, bbkde_surrogate *sur, const bbkde_k
     //    for 9 probes, on the quarter lattice; network values there.
     const int h = T / 2;
     const GridDesc gl = make_grid(2 * (int64_t)g.ntx + 1, 2 * (int64_t)g.nty + 1, g.x0,
-                                  h * g.dx, g.y0, h * g.dy, 16);
+                                  h * g.dx, g.y0, h * g.dy, LT);
     const int64_t n_lat = gl.nx * gl.ny;
     TRY(ensure(c, c->gr_lat_exact, (size_t)n_lat * sizeof(double)));
     TRY(tile_order(c, gl, c->gr_lat_order));
@@ -2044,7 +2047,7 @@ extern "C" int bbkde_eval_grid(bbkde_ctx *c, bbkde_surrogate *sur, const bbkde_k
     }
     int64_t n_q = 0;
     const GridDesc gq = make_grid(2 * (int64_t)g.ntx, 2 * (int64_t)g.nty, g.x0 + (T / 4) * g.dx,
-                                  h * g.dx, g.y0 + (T / 4) * g.dy, h * g.dy, 16);
+                                  h * g.dx, g.y0 + (T / 4) * g.dy, h * g.dy, LT);
     auto quarter_net = [&]() -> int {
       TRY(ensure(c, c->gr_q_net, (size_t)n_q * sizeof(float)));
       TRY(bbkde::surrogate_infer(sur, c->stream, n_q, nullptr, gq.nx, gq.x0, gq.dx, gq.y0,

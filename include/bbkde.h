@@ -414,6 +414,10 @@ typedef struct {
                         network only on the tiles whose probes miss, keeping it where
                         its probes pass; BBKDE_NET_EVERYWHERE (1) = network + residual
                         on every point */
+  int lattice_tile;  /* tile edge (in lattice points) of the factored exact sums on the
+                        anchor/probe lattices: 16 or 32; 0 = 16. A larger tile shares
+                        each kernel factor among more points but culls over a larger
+                        box */
 } bbkde_grid_config;
 
 enum { BBKDE_NET_RESCUE = 0, BBKDE_NET_EVERYWHERE = 1 };
