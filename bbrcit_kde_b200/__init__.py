@@ -89,7 +89,8 @@ class GridStats(C.Structure):
                 ("pairs", C.c_double), ("max_probe_err", C.c_double),
                 ("max_bound_ratio", C.c_double), ("ms_total", C.c_double),
                 ("ms_predict", C.c_double), ("ms_probe", C.c_double),
-                ("ms_fallback", C.c_double), ("probes_used", C.c_int64)]
+                ("ms_fallback", C.c_double), ("probes_used", C.c_int64),
+                ("lattice_tile_used", C.c_int64)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}

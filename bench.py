@@ -62,9 +62,10 @@ def pair_sum_bound_per_clk_per_sm(poly: int, fma_cycles: float = 12.0) -> tuple[
         bound = "sfu+fma (exp2 split: MUFU and FP32 polynomial)"
     return min(mufu, fma), bound
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per full-size launch of
-# the pair-sum kernel on this workload, from one ncu capture of the pilot and the
-# evaluation launch (57.40 MB and 55.27 MB): profiles/pair_sum_f32x2_adaptive_gaussprod2d_1M.md.
-TRAFFIC_BYTES_PER_LAUNCH = 56_335_000
+# the pair-sum kernel on this workload (the autotuned shape, 5 reference segments),
+# from one ncu capture of the pilot and the evaluation launch (25.30 MB and 26.57 MB):
+# profiles/pair_sum_f32x2_adaptive_gaussprod2d_1M.md.
+TRAFFIC_BYTES_PER_LAUNCH = 25_936_000
 
 
 def parse():
@@ -571,9 +572,11 @@ def run_surrogate_grid(a, world, rank, local):
     npts = G * G
     out = torch.empty(npts, dtype=torch.float64, device="cuda")
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-    # exact parts (lattice, fallback) to 1e-5: 100x below the pipeline's 1e-3 bar
+    # exact parts (lattice, fallback) to 1e-5: 100x below the pipeline's 1e-3 bar;
+    # every tile judged by its probes (no low-density cut); probe set and lattice
+    # tile picked by the library
     main_cfg = dict(surrogate=sur, mode=bk.GRID_ANCHORED, tile=16, probes=0, rel_tol=5e-4,
-                    low_frac=1e-4, interp=3, cull_rel=1e-5)
+                    low_frac=0.0, interp=3, cull_rel=1e-5, lattice_tile=0)
 
     def grid_step(dst, **kw):
         return ctx.eval_grid(desc, grid, dst.data_ptr(), **kw)
@@ -604,6 +607,7 @@ def run_surrogate_grid(a, world, rank, local):
     # Comparators, each once.
     comp = {}
     for name, kw in [("culled_exact", dict(mode=bk.GRID_EXACT, tile=16)),
+                     ("culled_exact_tile32", dict(mode=bk.GRID_EXACT, tile=32)),
                      ("culled_exact_pair_form", dict(mode=bk.GRID_EXACT, tile=16,
                                                      pair_form=True)),
                      ("network_pair_form", dict(main_cfg, pair_form=True)),
@@ -693,23 +697,26 @@ def run_surrogate_grid(a, world, rank, local):
         e2e = {"value": npts * a.steps / (sum(e2e_ms) / 1e3), "unit": GRID_METRIC_UNIT,
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(npts * 8)}
 
-    # Roofline of the factored culled sum (lattice and fallback kernel): on a
-    # 16 x 16 tile every reference costs 32 kernel factors (MUFU ex2) and 256
-    # multiply-adds, one per pair. The FMA pipe allows 128 pairs/clk/SM and MUFU
-    # 16 ex2/clk/SM = 16 x 256 / 32 = 128 pairs/clk/SM: both bounds coincide.
-    # Pairs at tile granularity of the culled-exact comparator over its device time.
-    ce = results["culled_exact"]
+    # Roofline of the factored culled sum at the lattice's tile edge T (the
+    # pipeline's largest launch): on a T x T tile every reference costs 2T kernel
+    # factors (MUFU ex2) and T^2 multiply-adds, one per pair. The FMA pipe allows
+    # 128 pairs/clk/SM; MUFU 16 ex2/clk/SM = 16 T^2 / 2T = 8T pairs/clk/SM (128 at
+    # T = 16, 256 at T = 32): the FMA pipe is the bound. Pairs at tile granularity
+    # of the culled-exact comparator at that tile edge over its device time.
+    lt = int(stats[-1]["lattice_tile_used"])
+    ce = results["culled_exact" if lt == 16 else "culled_exact_tile32"]
     peaks = measured_peaks()
     sm_max = float(peaks.get("sm_max_mhz") or clocks.get("sm_max_mhz") or 1965.0)
     peak = sm_count * FP32_FMA_PER_CLK_PER_SM * sm_max * 1e6
     ach = ce["pairs"] / (ce["ms_total"] / 1e3)
-    roofline = {"bound": "fp32+sfu", "kernel": "k_pair_sum_culled_sep<GAUSS_ISO,16> "
-                                               "(factored culled exact grid)",
+    roofline = {"bound": "fp32", "kernel": f"k_pair_sum_culled_sep<GAUSS_ISO,{lt}> "
+                                           "(factored culled exact grid; the pipeline's "
+                                           "lattice launch)",
                 "achieved": ach / 1e9, "peak": peak / 1e9, "unit": "Gpair/s",
                 "frac": ach / peak, "traffic": None,
                 "peak_basis": f"{sm_count} SMs x 128 FP32 FMA/clk x {sm_max:.0f} MHz "
-                              "(= 8 pairs per ex2 x 16 ex2/clk: both bounds coincide "
-                              "at tile 16); compute-bound, DRAM traffic negligible"}
+                              f"(MUFU allows {8 * lt} pairs/clk/SM at tile {lt}); "
+                              "compute-bound, DRAM traffic negligible"}
     cpu = None
     if rank == 0 and not a.no_cpu_baseline:
         wl = W.Workload("cfg5", W.GAUSS, 2, (0.05, 0.05), refs, w,
@@ -742,8 +749,10 @@ def run_surrogate_grid(a, world, rank, local):
         "config": {"workload": f"surrogate grid: adaptive Gaussian KDE of {n} refs (pilot "
                                f"h=0.05, alpha=0.5) on a {G}x{G} grid over [-4,4]^2",
                    "pipeline": "bbkde_eval_grid anchored mode, bicubic residual, tile 16, "
-                               "automatic probe set (5 at this spacing), probe tolerance 5e-4, low_frac 1e-4, exact parts "
-                               "culled to 1e-5; network in "
+                               f"automatic probe set ({stats[-1]['probes_used']} at this "
+                               "spacing) and lattice tile "
+                               f"({stats[-1]['lattice_tile_used']}), probe tolerance 5e-4, "
+                               "no low-density cut, exact parts culled to 1e-5; network in "
                                "rescue mode (two-term BF16 inference on tcgen05 on the tiles "
                                "the interpolated exact anchors miss)",
                    "l2": "flushed between timed steps (256 MB write)"},

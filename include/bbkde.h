@@ -415,9 +415,10 @@ typedef struct {
                         its probes pass; BBKDE_NET_EVERYWHERE (1) = network + residual
                         on every point */
   int lattice_tile;  /* tile edge (in lattice points) of the factored exact sums on the
-                        anchor/probe lattices: 16 or 32; 0 = 16. A larger tile shares
-                        each kernel factor among more points but culls over a larger
-                        box */
+                        anchor/probe lattices: 16 or 32; 0 = automatic: 32 while a
+                        32-point lattice tile spans at most 16 narrowest kernel widths,
+                        else 16. A larger tile shares each kernel factor among more
+                        points but culls over a larger box */
 } bbkde_grid_config;
 
 enum { BBKDE_NET_RESCUE = 0, BBKDE_NET_EVERYWHERE = 1 };
@@ -434,6 +435,7 @@ typedef struct {
                         probe = exact lattices, residual interpolation and probe
                         check; fallback = exact tiles */
   int64_t probes_used;        /* the probe set the call ran (resolves probes = 0) */
+  int64_t lattice_tile_used;  /* the lattice tile the call ran (resolves lattice_tile = 0) */
 } bbkde_grid_stats;
 
 /* Normalised density of the REFERENCE set (with its current attributes, e.g.

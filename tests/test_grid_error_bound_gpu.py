@@ -4,8 +4,9 @@ checked against the CPU oracle.
 
 The pipeline's configuration is the one bench.py's surrogate-grid workload runs
 (GRID_PIPELINE below): anchored mode, bicubic residual, tile 16, the automatic
-probe set, probe tolerance 5e-4, low-density cut 1e-4, exact parts (lattice
-and fallback tiles) culled to 1e-5, network in rescue mode. A tile keeps its
+probe set and lattice tile, probe tolerance 5e-4, no low-density cut (every
+tile is judged by its probes), exact parts (lattice and fallback tiles) culled
+to 1e-5, network in rescue mode. A tile keeps its
 interpolated prediction only when its exact probes agree within the probe
 tolerance; the test checks that this gate holds the 1e-3 bar between the probes
 too, on the configuration-5 mixture at two point spacings:
@@ -27,14 +28,17 @@ torch = pytest.importorskip("torch")
 
 # The pipeline configuration of bench.py --workload surrogate-grid: the library
 # picks the probe set (probes = 0): centre and edge midpoints while a tile spans at
-# most 0.75 narrowest kernel widths, the quarter points besides on coarser grids.
-GRID_PIPELINE = dict(mode=bk.GRID_ANCHORED, tile=16, probes=0, rel_tol=5e-4, low_frac=1e-4,
-                     interp=3, net_scope=bk.NET_RESCUE, cull_rel=1e-5)
+# most 0.75 narrowest kernel widths, the quarter points besides on coarser grids;
+# and the lattice tile (lattice_tile = 0): 32 while a 32-point lattice tile spans
+# at most 16 narrowest kernel widths, else 16.
+GRID_PIPELINE = dict(mode=bk.GRID_ANCHORED, tile=16, probes=0, rel_tol=5e-4, low_frac=0.0,
+                     interp=3, net_scope=bk.NET_RESCUE, cull_rel=1e-5, lattice_tile=0)
 
-# name -> (references, pilot h, grid, probe set the automatic rule must pick)
+# name -> (references, pilot h, grid, probe set and lattice tile the automatic
+# rules must pick)
 CASES = {
-    "coarse": (262_144, 0.05, (1024, 1024, -4.0, 4.0, -4.0, 4.0), 9),
-    "fine": (1_000_000, 0.063, (2048, 2048, -3.5, -1.5, 0.5, 2.5), 5),
+    "coarse": (262_144, 0.05, (1024, 1024, -4.0, 4.0, -4.0, 4.0), 9, 16),
+    "fine": (1_000_000, 0.063, (2048, 2048, -3.5, -1.5, 0.5, 2.5), 5, 32),
 }
 
 
@@ -45,7 +49,7 @@ def _grid_points(grid):
 
 @pytest.mark.parametrize("name", sorted(CASES))
 def test_pipeline_error_bound_every_point(ctx, oracle, name):
-    n, h, grid, probes = CASES[name]
+    n, h, grid, probes, lattice_tile = CASES[name]
     refs = W.config5_refs(n)
     w = np.full(n, 1.0 / n)
     desc = bk.kernel_desc(W.GAUSS, 2, (h, h))
@@ -78,6 +82,7 @@ def test_pipeline_error_bound_every_point(ctx, oracle, name):
     assert rel.max() <= 1e-3, (name, float(rel.max()), pts[worst], st.as_dict())
     assert st.tiles_surrogate > 0, st.as_dict()       # the prediction is used somewhere
     assert st.probes_used == probes, st.as_dict()
+    assert st.lattice_tile_used == lattice_tile, st.as_dict()
     # the FP64 device path against the CPU oracle on 4,096 of the points
     sel = np.sort(np.random.default_rng(7).choice(npts, 4096, replace=False))
     want = oracle.direct(W.GAUSS, 2, (h, h), refs, mass, pts[sel], abw=abw)
