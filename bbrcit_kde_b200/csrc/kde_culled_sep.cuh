@@ -69,19 +69,16 @@ __global__ void __launch_bounds__(T *T / 8, T == 32 ? 4 : 16)
   constexpr int FBUF = 2 * FROWS * T;  // factor pairs per buffer (x rows, then y rows)
   constexpr int NG = BLOCK / (2 * T);  // factor teams (references split between them)
   constexpr int FPB = 2 / NG;          // factor pairs per lane per accumulation step
-  constexpr int NPR = kRefTile / 2;    // reference pairs per tile
+  constexpr int STG = kRefTile + 4;    // staged column stride (x and y on different banks)
   constexpr bool kGauss = op_gauss(OP);
   constexpr bool kExt = op_has_extra(OP);
   static_assert(BLOCK == 2 * LPS, "two splits");
   static_assert(NG * FPB == 2 && kChunk == 32, "one factor step per accumulation step");
   static_assert(kRefTile % SUB == 0 && FROWS % (kChunk / 2) == 0, "shape");
   static_assert(2 * FBUF * 2 >= 2 * T * T, "exchange area");
-  // Staged references, per axis (x pairs, then y pairs) and reference pair:
-  // (-coordinate even, -coordinate odd, scale even, scale odd) -- one 128-bit
-  // load per factor pair; the masses of the pairs and, at [NPR], (1, 1) for the
-  // x factors.
-  __shared__ __align__(16) float4 s_rec[2 * NPR];
-  __shared__ __align__(16) float2 s_mp[NPR + 1];
+  __shared__ __align__(16) float s_c[2 * STG];     // -x | -y of the staged references
+  __shared__ __align__(16) float s_s[2 * STG];     // x scale | y scale
+  __shared__ __align__(16) float s_m[2 * STG];     // 1 | mass
   // Two buffers of u_x rows ([pair][column], (even, odd)) then m u_y rows;
   // reused to hand split 1's sums to split 0.
   __shared__ __align__(16) float2 s_fac[2 * FBUF];
@@ -104,7 +101,7 @@ __global__ void __launch_bounds__(T *T / 8, T == 32 ? 4 : 16)
     s_qx[tid] = grid_coord(q.gx0, q.gdx, i0 + tid);
     s_qy[tid] = grid_coord(q.gy0, q.gdy, j0 + tid);
   }
-  if (tid == 0) s_mp[NPR] = f2(1.0f);
+  for (int i = tid; i < kRefTile; i += BLOCK) s_m[i] = 1.0f;
   if (tid < NS) {
     // slot tid: rows j0 + tid T/8 .. + T/8 - 1 and all columns, inside the grid
     const int64_t jlo = j0 + (int64_t)tid * SPR;
@@ -147,8 +144,7 @@ __global__ void __launch_bounds__(T *T / 8, T == 32 ? 4 : 16)
   const int fw = tid % (2 * T), ft = tid / (2 * T);
   const bool fx = fw < T;
   const float fq = fx ? s_qx[fw] : s_qy[fw - T];
-  const float4 *const frec = s_rec + (fx ? 0 : NPR);
-  const int fmo = fx ? NPR : 0;   // x factors read the (1, 1) entry
+  const int foff = fx ? 0 : STG;
   const int fcol = fx ? fw : fw - T;
   float2 *const fbase = s_fac + (fx ? 0 : FROWS * T);
   // Column swizzle of factor row p (see the layout note).
@@ -208,24 +204,23 @@ __global__ void __launch_bounds__(T *T / 8, T == 32 ? 4 : 16)
       rec[u] = rr < t1 ? __ldg(a.refs + rr) : make_float4(0.f, 0.f, 0.f, 0.f);
       ext[u] = kExt ? (rr < t1 ? __ldg(a.extra + rr) : 0.f) : rec[u].w;
     }
-    float *const rf = reinterpret_cast<float *>(s_rec);
 #pragma unroll
     for (int u = 0; u < PER; ++u) {
-      const int i = u * BLOCK + tid, pr = i >> 1, od = i & 1;
-      rf[4 * pr + od] = -rec[u].x;
-      rf[4 * pr + 2 + od] = rec[u].w;
-      rf[4 * (NPR + pr) + od] = -rec[u].y;
-      rf[4 * (NPR + pr) + 2 + od] = ext[u];
-      reinterpret_cast<float *>(s_mp)[i] = rec[u].z;
+      const int i = u * BLOCK + tid;
+      s_c[i] = -rec[u].x;
+      s_c[STG + i] = -rec[u].y;
+      s_s[i] = rec[u].w;
+      s_s[STG + i] = ext[u];
+      s_m[STG + i] = rec[u].z;
     }
     __syncthreads();
     // Factor pair p of sub-chunk sub (references sub + 2p, + 1) into buffer b.
     auto factor = [&](int b, int sub, int p) {
-      const int j2 = (sub >> 1) + p;
-      const float4 r4 = frec[j2];
-      const float2 m2 = s_mp[fx ? fmo : j2];
-      const float2 s2 = make_float2(r4.z, r4.w);
-      const float2 d = __fadd2_rn(f2(fq), make_float2(r4.x, r4.y));
+      const int j = foff + sub + 2 * p;
+      const float2 c2 = *reinterpret_cast<const float2 *>(&s_c[j]);
+      const float2 s2 = *reinterpret_cast<const float2 *>(&s_s[j]);
+      const float2 m2 = *reinterpret_cast<const float2 *>(&s_m[j]);
+      const float2 d = __fadd2_rn(f2(fq), c2);
       const float2 dd = __fmul2_rn(d, d);
       float2 u;
       if (kGauss) {
@@ -258,11 +253,16 @@ __global__ void __launch_bounds__(T *T / 8, T == 32 ? 4 : 16)
     };
     for (int p = ft; p < FROWS; p += NG) factor(0, 0, p);
     __syncthreads();
+    // One FP32 partial per sub-chunk and split (16 references at T = 16, 32 at
+    // T = 32: two interleaved halves, as the pair form's kChunk), then its Kahan
+    // fold, two points per packed op (a - b as fma(b, -1, a): exact negation, one
+    // rounding, as the scalar subtraction).
     for (int sb = 0; sb < NSUB; ++sb) {
       const int cur = sb & 1;
       const bool more = sb + 1 < NSUB;
+      float2 acc[16];
+#pragma unroll
       for (int ch = 0; ch < FROWS / 16; ++ch) {
-        float2 acc[16];
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
           if (more) {
@@ -270,20 +270,18 @@ __global__ void __launch_bounds__(T *T / 8, T == 32 ? 4 : 16)
             for (int f = 0; f < FPB; ++f)
               factor(cur ^ 1, (sb + 1) * SUB, ft + ((ch * 8 + i) * FPB + f) * NG);
           }
-          step(cur, ch * 16 + 2 * i + sp, acc, i == 0);
+          step(cur, ch * 16 + 2 * i + sp, acc, ch == 0 && i == 0);
         }
-        // Kahan fold, two points per packed op (a - b as fma(b, -1, a): exact
-        // negation, one rounding, as the scalar subtraction).
-        const float2 m1 = f2(-1.0f);
+      }
+      const float2 m1 = f2(-1.0f);
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
-          const float2 v = make_float2(acc[2 * k].x + acc[2 * k].y,
-                                       acc[2 * k + 1].x + acc[2 * k + 1].y);
-          const float2 y = __ffma2_rn(comp[k], m1, v);
-          const float2 t2 = __fadd2_rn(sum[k], y);
-          comp[k] = __ffma2_rn(y, m1, __ffma2_rn(sum[k], m1, t2));
-          sum[k] = t2;
-        }
+      for (int k = 0; k < 8; ++k) {
+        const float2 v = make_float2(acc[2 * k].x + acc[2 * k].y,
+                                     acc[2 * k + 1].x + acc[2 * k + 1].y);
+        const float2 y = __ffma2_rn(comp[k], m1, v);
+        const float2 t2 = __fadd2_rn(sum[k], y);
+        comp[k] = __ffma2_rn(y, m1, __ffma2_rn(sum[k], m1, t2));
+        sum[k] = t2;
       }
       __syncthreads();
     }
