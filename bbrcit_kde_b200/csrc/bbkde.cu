@@ -128,8 +128,12 @@ struct bbkde_ctx {
       cb_smin, cb_tiles, cb_stats;
   DevBuf gr_pred, gr_order, gr_tmin, gr_tmax, gr_bad, gr_terr, gr_flag, gr_flag_ord, gr_list,
       gr_nsel, gr_counts, gr_gmax, gr_lat_order, gr_lat_exact, gr_lat_net, gr_q_order, gr_q_exact,
-      gr_q_net, gr_resid, gr_cand_ord, gr_cand_xy, gr_cand_net, gr_out;
+      gr_q_net, gr_resid, gr_cand_ord, gr_cand_xy, gr_cand_net, gr_out, gr_part;
   cudaEvent_t ev3 = nullptr;
+  // smallest positive abw of the reference set, for the (coordinate, attribute)
+  // versions it was computed at
+  double abw_min = 1.0;
+  uint64_t abw_min_cv = ~0ull, abw_min_av = ~0ull;
   std::string err;
 };
 
@@ -741,7 +745,8 @@ int bbkde_ctx_destroy(bbkde_ctx *c) {
                     &c->gr_terr, &c->gr_flag, &c->gr_flag_ord, &c->gr_list, &c->gr_nsel,
                     &c->gr_counts, &c->gr_gmax, &c->gr_lat_order, &c->gr_lat_exact,
                     &c->gr_lat_net, &c->gr_q_order, &c->gr_q_exact, &c->gr_q_net, &c->gr_resid,
-                    &c->gr_cand_ord, &c->gr_cand_xy, &c->gr_cand_net, &c->gr_out})
+                    &c->gr_cand_ord, &c->gr_cand_xy, &c->gr_cand_net, &c->gr_out,
+                    &c->gr_part})
     release(*b);
   if (c->cv_graph) cudaGraphExecDestroy(c->cv_graph);
   if (c->ev3) cudaEventDestroy(c->ev3);
@@ -1479,12 +1484,51 @@ void launch_cull_op(int shape, unsigned nblk, cudaStream_t st, const CullArgs &a
     k_pair_sum_culled<OP, D, 4, 64, 8><<<nblk, 64, 0, st>>>(a);
 }
 
+// Tile-16 lists shorter than this many tiles per SM are split: each tile's
+// reference groups are shared by a cluster of 2, 4 or 8 blocks (the resident
+// tile-16 blocks per SM: 12 by shared memory).
+constexpr int kSepResidentPerSm = 12;
+
+template <int OP, int S>
+cudaError_t launch_cull_sep_split(unsigned nblk, cudaStream_t st, const CullArgs &a) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(nblk * S);
+  cfg.blockDim = dim3(16 * 16 / 8);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = S;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k_pair_sum_culled_sep<OP, 16, S>, a);
+}
+
+// parts = 1: one block per tile; 2, 4, 8 (tile 16 only): clusters of that many.
 template <int OP>
-void launch_cull_sep(int tile, unsigned nblk, cudaStream_t st, const CullArgs &a) {
-  if (tile == 32)
+cudaError_t launch_cull_sep(int tile, int parts, unsigned nblk, cudaStream_t st,
+                            const CullArgs &a) {
+  if (tile == 32) {
     k_pair_sum_culled_sep<OP, 32><<<nblk, 32 * 32 / 8, 0, st>>>(a);
-  else
-    k_pair_sum_culled_sep<OP, 16><<<nblk, 16 * 16 / 8, 0, st>>>(a);
+    return cudaGetLastError();
+  }
+  switch (parts) {
+    case 2: return launch_cull_sep_split<OP, 2>(nblk, st, a);
+    case 4: return launch_cull_sep_split<OP, 4>(nblk, st, a);
+    case 8: return launch_cull_sep_split<OP, 8>(nblk, st, a);
+    default:
+      k_pair_sum_culled_sep<OP, 16><<<nblk, 16 * 16 / 8, 0, st>>>(a);
+      return cudaGetLastError();
+  }
+}
+
+// Parts per tile for a factored launch of nblk tiles of edge `tile`.
+int sep_parts(const bbkde_ctx *c, int tile, unsigned nblk) {
+  if (tile != 16) return 1;
+  const double per = (double)c->sm_count * kSepResidentPerSm / (double)nblk;
+  return per >= 8 ? 8 : per >= 4 ? 4 : per >= 2 ? 2 : 1;
 }
 
 // One culled (or, with full, complete) sum over nblk query blocks; adds its
@@ -1519,10 +1563,17 @@ int launch_culled(bbkde_ctx *c, const Resolved &r, int shape, unsigned nblk,
   a.blk_tiles = c->cb_tiles.as<int>();
   const bool d2 = r.dim == 2;
   if (sep_tile > 0) {
+    const int parts = sep_parts(c, sep_tile, nblk);
     switch (r.op) {
-      case OP_GAUSS_ISO: launch_cull_sep<OP_GAUSS_ISO>(sep_tile, nblk, c->stream, a); break;
-      case OP_GAUSS_PROD: launch_cull_sep<OP_GAUSS_PROD>(sep_tile, nblk, c->stream, a); break;
-      case OP_EPAN_PROD: launch_cull_sep<OP_EPAN_PROD>(sep_tile, nblk, c->stream, a); break;
+      case OP_GAUSS_ISO:
+        CUDA_TRY(c, launch_cull_sep<OP_GAUSS_ISO>(sep_tile, parts, nblk, c->stream, a));
+        break;
+      case OP_GAUSS_PROD:
+        CUDA_TRY(c, launch_cull_sep<OP_GAUSS_PROD>(sep_tile, parts, nblk, c->stream, a));
+        break;
+      case OP_EPAN_PROD:
+        CUDA_TRY(c, launch_cull_sep<OP_EPAN_PROD>(sep_tile, parts, nblk, c->stream, a));
+        break;
       default: return fail(c, BBKDE_UNSUPPORTED, "culled sum: kernel does not factor");
     }
   } else switch (r.op) {
@@ -1952,14 +2003,23 @@ extern "C" int bbkde_eval_grid(bbkde_ctx *c, bbkde_surrogate *sur, const bbkde_k
     // wider tiles vary between those probes, so the quarter points join them.
     // Automatic lattice tile: kGridLatticeSpan.
     double amin = 1.0;
-    if (rs.n > 0) {
-      k_min_positive<<<1, 1024, 0, c->stream>>>(rs.abw.as<double>(), rs.n,
-                                                c->scalars.as<double>() + 8);
-      COUNT_LAUNCH(c);
+    if (rs.n > 0 && c->abw_min_cv == rs.coord_version && c->abw_min_av == rs.attr_version) {
+      amin = c->abw_min;
+    } else if (rs.n > 0) {
+      const unsigned nb = std::min<unsigned>(grid1d(rs.n), (unsigned)c->sm_count * 4);
+      TRY(ensure(c, c->gr_part, (size_t)nb * sizeof(double)));
+      k_min_positive<<<nb, 256, 0, c->stream>>>(rs.abw.as<double>(), rs.n,
+                                                c->gr_part.as<double>(), false);
+      k_min_positive<<<1, 1024, 0, c->stream>>>(c->gr_part.as<double>(), (int64_t)nb,
+                                                c->scalars.as<double>() + 8, true);
+      c->launch_total += 2;
       CUDA_TRY(c, cudaGetLastError());
       CUDA_TRY(c, cudaMemcpyAsync(&amin, c->scalars.as<double>() + 8, sizeof(double),
                                   cudaMemcpyDeviceToHost, c->stream));
       CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+      c->abw_min = amin;
+      c->abw_min_cv = rs.coord_version;
+      c->abw_min_av = rs.attr_version;
     }
     const double wmin = std::min(r.h1, r.h2) * amin;
     const double span = T * std::max(g.dx, g.dy);
@@ -2017,6 +2077,7 @@ extern "C" int bbkde_eval_grid(bbkde_ctx *c, bbkde_surrogate *sur, const bbkde_k
     COUNT_LAUNCH(c);
   } else {
     // 1. Prediction at every point (log-density): the network, or zero.
+    bool pred_zero = false;
     TRY(ensure(c, c->gr_pred, (size_t)npts * sizeof(float)));
     float *pred = c->gr_pred.as<float>();
     if (net_all) {
@@ -2026,7 +2087,7 @@ extern "C" int bbkde_eval_grid(bbkde_ctx *c, bbkde_surrogate *sur, const bbkde_k
               : fail(c, BBKDE_CUDA_ERROR, "grid: surrogate inference failed"));
       COUNT_LAUNCH(c);
     } else {
-      CUDA_TRY(c, cudaMemsetAsync(pred, 0, (size_t)npts * sizeof(float), c->stream));
+      pred_zero = true;   // written by the interpolation below, never read as zeros
     }
     if (!rescue) CUDA_TRY(c, cudaEventRecord(c->ev1, c->stream));
     // 2. Exact values on the half-pitch lattice (anchors and probes; one regular
@@ -2089,14 +2150,25 @@ extern "C" int bbkde_eval_grid(bbkde_ctx *c, bbkde_surrogate *sur, const bbkde_k
       COUNT_LAUNCH(c);
       resid = c->gr_resid.as<float>();
     }
-    k_tile_reduce<<<(unsigned)ntiles, 256, 0, c->stream>>>(g, pred, resid, interp,
-                                                         c->gr_tmin.as<float>(),
-                                                         c->gr_tmax.as<float>(),
-                                                         c->gr_bad.as<int>());
+    if (pred_zero && !resid) {
+      CUDA_TRY(c, cudaMemsetAsync(pred, 0, (size_t)npts * sizeof(float), c->stream));
+      pred_zero = false;
+    }
+    k_tile_reduce<<<(unsigned)((ntiles + kTileReduceWarps - 1) / kTileReduceWarps),
+                    32 * kTileReduceWarps, 0, c->stream>>>(g, pred, resid, interp, pred_zero ? 1 : 0,
+                                                           c->gr_tmin.as<float>(),
+                                                           c->gr_tmax.as<float>(),
+                                                           c->gr_bad.as<int>());
     COUNT_LAUNCH(c);
-    k_max_finite<<<1, 1024, 0, c->stream>>>(c->gr_tmax.as<float>(), (int)ntiles,
-                                            c->gr_gmax.as<float>());
-    COUNT_LAUNCH(c);
+    {
+      const unsigned nb = std::min<unsigned>(grid1d(ntiles), (unsigned)c->sm_count * 4);
+      TRY(ensure(c, c->gr_part, (size_t)nb * sizeof(double)));
+      k_max_finite<<<nb, 256, 0, c->stream>>>(c->gr_tmax.as<float>(), (int)ntiles,
+                                              c->gr_part.as<float>());
+      k_max_finite<<<1, 1024, 0, c->stream>>>(c->gr_part.as<float>(), (int)nb,
+                                              c->gr_gmax.as<float>());
+      c->launch_total += 2;
+    }
     // 4. Held-out probes: every tile's interpolant against the exact lattice values.
     ProbeArgs pa;
     pa.g = g;
@@ -2181,8 +2253,10 @@ extern "C" int bbkde_eval_grid(bbkde_ctx *c, bbkde_surrogate *sur, const bbkde_k
       CUDA_TRY(c, cudaEventRecord(c->ev2, c->stream));
     }
     // 6. Predicted values on the tiles that keep them.
-    const unsigned ab = std::min<unsigned>(grid1d(npts), (unsigned)c->sm_count * 16);
-    k_apply<<<ab, 256, 0, c->stream>>>(g, c->gr_pred.as<float>(), c->gr_flag.as<int>(), out);
+    const dim3 ab((unsigned)std::min<int64_t>((g.nx + 255) / 256, 64),
+                  (unsigned)std::min<int64_t>(g.ny, 65535));
+    k_apply<<<ab, 256, 0, c->stream>>>(g, T == 32 ? 5 : 4, c->gr_pred.as<float>(),
+                                       c->gr_flag.as<int>(), out);
     COUNT_LAUNCH(c);
   }
   // 7. Exact fallback on the flagged tiles.

@@ -206,15 +206,17 @@ __device__ __forceinline__ int block_append(bool pred, int value, int *dst, int 
 // tests their members in parallel (tile_needed), BLOCK at a time. The needed
 // tiles of the batch are listed in ascending order in s_list[0, total) (capacity
 // cull_list_len(BLOCK)) and handed to sum_list(total), which every thread calls.
-// Returns the number of tiles listed.
+// With parts > 1 the block takes every parts-th batch from batch `part` on (the
+// blocks of one tile then share its reference groups). Returns the number of
+// tiles listed.
 template <int BLOCK, class GroupNeeded, class TileNeeded, class SumList>
 __device__ __forceinline__ int cull_pass(const CullArgs &a, int *s_list, int *s_glist, int *s_wc,
                                          GroupNeeded group_needed, TileNeeded tile_needed,
-                                         SumList sum_list) {
+                                         SumList sum_list, int part = 0, int parts = 1) {
   constexpr int GR = cull_groups_per_batch(BLOCK);
   const int tid = threadIdx.x;
   int summed = 0;
-  for (int g0 = 0; g0 < a.n_groups; g0 += GR) {
+  for (int g0 = part * GR; g0 < a.n_groups; g0 += parts * GR) {
     const int gi = g0 + tid;
     const bool gneed = tid < GR && gi < a.n_groups && group_needed(a.groups[gi]);
     const int ng = block_append<BLOCK>(gneed, gi, s_glist, s_wc);

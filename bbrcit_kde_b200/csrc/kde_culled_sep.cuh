@@ -42,6 +42,7 @@
 // split 1) -- deterministic.
 #pragma once
 
+#include <cooperative_groups.h>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -53,7 +54,16 @@ __host__ __device__ constexpr bool op_separable(int op) {
   return op == OP_GAUSS_ISO || op == OP_GAUSS_PROD || op == OP_EPAN_PROD;
 }
 
-template <int OP, int T>
+// Split tiles (S > 1, launched as clusters of S blocks per tile): for short tile
+// lists, where one block per tile would leave most SMs idle while the densest
+// tiles finish, block `part` of a tile's cluster sums every S-th batch of tile
+// groups. Every part scans all groups for the largest bound (the same near/far
+// split), the parts exchange their near-field sums through distributed shared
+// memory so that all of them use the thresholds of the total near-field sum, and
+// part 0 adds the parts' point sums in rank order. The skipped units of the
+// parts are disjoint subsets of one tile's units, so their bounds add up to the
+// single-block bound (reported by part 0 from the parts' sums).
+template <int OP, int T, int S = 1>
 __global__ void __launch_bounds__(T *T / 8, T == 32 ? 4 : 16)
     k_pair_sum_culled_sep(CullArgs a) {
   static_assert(T == 16 || T == 32, "tile edge");
@@ -75,7 +85,8 @@ __global__ void __launch_bounds__(T *T / 8, T == 32 ? 4 : 16)
   static_assert(BLOCK == 2 * LPS, "two splits");
   static_assert(NG * FPB == 2 && kChunk == 32, "one factor step per accumulation step");
   static_assert(kRefTile % SUB == 0 && FROWS % (kChunk / 2) == 0, "shape");
-  static_assert(2 * FBUF * 2 >= 2 * T * T, "exchange area");
+  static_assert(FBUF >= T * T, "exchange area: two T x T double arrays");
+  static_assert(S == 1 || S == 2 || S == 4 || S == 8, "cluster size");
   __shared__ __align__(16) float s_c[2 * STG];     // -x | -y of the staged references
   __shared__ __align__(16) float s_s[2 * STG];     // x scale | y scale
   __shared__ __align__(16) float s_m[2 * STG];     // 1 | mass
@@ -91,11 +102,16 @@ __global__ void __launch_bounds__(T *T / 8, T == 32 ? 4 : 16)
   __shared__ unsigned s_min[NS];       // bits of the slot's smallest near-field sum (>= 0)
   __shared__ float s_red[NW];
   __shared__ double s_d[NS][NW];
+  __shared__ float s_near[S > 1 ? T * T : 1];   // this part's near-field point sums
+  __shared__ double s_b[NS];                      // this part's skipped bound per slot
+  __shared__ int s_summed;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int sp = tid / LPS, rg = (tid % LPS) / CG, cg = (tid % LPS) % CG;
   const CullQueries &q = a.q;
-  const int t = q.tile_list[blockIdx.x];
+  const int part = S > 1 ? (int)(blockIdx.x % S) : 0;
+  const int64_t tile_slot = blockIdx.x / S;
+  const int t = q.tile_list[tile_slot];
   const int64_t i0 = (int64_t)(t % q.ntx) * T, j0 = (int64_t)(t / q.ntx) * T;
   if (tid < T) {
     s_qx[tid] = grid_coord(q.gx0, q.gdx, i0 + tid);
@@ -297,7 +313,7 @@ __global__ void __launch_bounds__(T *T / 8, T == 32 ? 4 : 16)
   auto pass = [&](int phase) {
     summed += cull_pass<BLOCK>(
         a, s_list, s_glist, s_wc, [&](const RefTile &g) { return needed(g, phase, true); },
-        [&](const RefTile &rt) { return needed(rt, phase, false); }, sum_list);
+        [&](const RefTile &rt) { return needed(rt, phase, false); }, sum_list, part, S);
   };
 
   // Point k = 4 kr + kc of this lane: row own(rg, kr), column own(cg, kc).
@@ -316,12 +332,32 @@ __global__ void __launch_bounds__(T *T / 8, T == 32 ? 4 : 16)
       for (int k = 0; k < 16; ++k) xf[own(rg, k >> 2) * T + own(cg, k & 3)] = point_sum(k);
     }
     __syncthreads();
+    if constexpr (S > 1) {
+      if (sp == 0) {
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+          const int idx = own(rg, k >> 2) * T + own(cg, k & 3);
+          s_near[idx] = point_sum(k) + xf[idx];
+        }
+      }
+      cooperative_groups::this_cluster().sync();
+    }
     if (sp == 0) {
       float m0 = INFINITY, m1 = INFINITY;   // slots of rows k < 2 and k >= 2
 #pragma unroll
       for (int k = 0; k < 16; ++k) {
         if (!valid(k)) continue;
-        const float v = fmaxf(point_sum(k) + xf[own(rg, k >> 2) * T + own(cg, k & 3)], 0.f);
+        const int idx = own(rg, k >> 2) * T + own(cg, k & 3);
+        float tot;
+        if constexpr (S > 1) {
+          // the total near-field sum, parts added in rank order
+          tot = 0.f;
+          for (int r = 0; r < S; ++r)
+            tot += cooperative_groups::this_cluster().map_shared_rank(s_near, r)[idx];
+        } else {
+          tot = point_sum(k) + xf[idx];
+        }
+        const float v = fmaxf(tot, 0.f);
         if ((k >> 2) < 2) m0 = fminf(m0, v);
         else m1 = fminf(m1, v);
       }
@@ -345,25 +381,26 @@ __global__ void __launch_bounds__(T *T / 8, T == 32 ? 4 : 16)
       if (lane == 0) s_d[k][warp] = sk;
     }
     __syncthreads();
+    if (tid < NS) {
+      double b = 0.0;
+#pragma unroll
+      for (int w = 0; w < NW; ++w) b += s_d[tid][w];
+      s_b[tid] = b;
+    }
+    __syncthreads();
     smin_all = INFINITY;
 #pragma unroll
     for (int k = 0; k < NS; ++k) {
-      double b = 0.0;
-#pragma unroll
-      for (int w = 0; w < NW; ++w) b += s_d[k][w];
       const double mk = (double)__uint_as_float(s_min[k]);
       smin_all = fmin(smin_all, mk);
-      if (b > 0.0) ratio = fmax(ratio, b * exp2((double)s_th[k]) / fmax(a.rel * mk, a.abs_n));
+      if (S == 1 && s_b[k] > 0.0)
+        ratio = fmax(ratio, s_b[k] * exp2((double)s_th[k]) / fmax(a.rel * mk, a.abs_n));
     }
   } else {
     pass(0);
+    if (tid < NS) s_b[tid] = 0.0;
   }
-  if (tid == 0) {
-    a.blk_bound[blockIdx.x] = ratio;
-    a.blk_smin[blockIdx.x] = smin_all;
-    a.blk_tiles[blockIdx.x] = summed;
-  }
-  // Split 1's sums to split 0, which writes split 0 + split 1.
+  // Split 1's sums to split 0, which adds split 0 + split 1.
   double *const xd = reinterpret_cast<double *>(s_fac);
   __syncthreads();
   if (sp == 1) {
@@ -372,14 +409,63 @@ __global__ void __launch_bounds__(T *T / 8, T == 32 ? 4 : 16)
       xd[own(rg, k >> 2) * T + own(cg, k & 3)] = point_sum_d(k);
   }
   __syncthreads();
-  if (sp == 0) {
-#pragma unroll
-    for (int k = 0; k < 16; ++k) {
-      if (!valid(k)) continue;
-      const int row = own(rg, k >> 2), col = own(cg, k & 3);
-      q.out[(j0 + row) * q.gnx + (i0 + col)] =
-          q.scale * (point_sum_d(k) + xd[row * T + col]);
+  if constexpr (S == 1) {
+    if (tid == 0) {
+      a.blk_bound[tile_slot] = ratio;
+      a.blk_smin[tile_slot] = smin_all;
+      a.blk_tiles[tile_slot] = summed;
     }
+    if (sp == 0) {
+#pragma unroll
+      for (int k = 0; k < 16; ++k) {
+        if (!valid(k)) continue;
+        const int row = own(rg, k >> 2), col = own(cg, k & 3);
+        q.out[(j0 + row) * q.gnx + (i0 + col)] =
+            q.scale * (point_sum_d(k) + xd[row * T + col]);
+      }
+    }
+  } else {
+    // This part's point sums beside split 1's; part 0 adds the parts in rank order.
+    double *const xp = xd + T * T;
+    if (sp == 0) {
+#pragma unroll
+      for (int k = 0; k < 16; ++k) {
+        const int idx = own(rg, k >> 2) * T + own(cg, k & 3);
+        xp[idx] = point_sum_d(k) + xd[idx];
+      }
+    }
+    if (tid == 0) s_summed = summed;
+    auto cluster = cooperative_groups::this_cluster();
+    cluster.sync();
+    if (part == 0) {
+      if (sp == 0) {
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+          if (!valid(k)) continue;
+          const int row = own(rg, k >> 2), col = own(cg, k & 3), idx = row * T + col;
+          double v = 0.0;
+          for (int r = 0; r < S; ++r) v += cluster.map_shared_rank(xp, r)[idx];
+          q.out[(j0 + row) * q.gnx + (i0 + col)] = q.scale * v;
+        }
+      }
+      if (tid == 0) {
+        int tiles = 0;
+        for (int r = 0; r < S; ++r) tiles += *cluster.map_shared_rank(&s_summed, r);
+        if (kGauss) {
+          for (int k = 0; k < NS; ++k) {
+            double b = 0.0;
+            for (int r = 0; r < S; ++r) b += cluster.map_shared_rank(s_b, r)[k];
+            const double mk = (double)__uint_as_float(s_min[k]);
+            if (b > 0.0)
+              ratio = fmax(ratio, b * exp2((double)s_th[k]) / fmax(a.rel * mk, a.abs_n));
+          }
+        }
+        a.blk_bound[tile_slot] = ratio;
+        a.blk_smin[tile_slot] = smin_all;
+        a.blk_tiles[tile_slot] = tiles;
+      }
+    }
+    cluster.sync();   // the parts' shared memory stays valid until part 0 has read it
   }
 }
 

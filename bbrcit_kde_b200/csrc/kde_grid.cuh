@@ -103,32 +103,42 @@ __device__ __forceinline__ float resid_interp(const float (&r)[4][4], float u, f
   return (1.f - w) * ((1.f - u) * r[1][1] + u * r[1][2]) + w * ((1.f - u) * r[2][1] + u * r[2][2]);
 }
 
-// One block per tile: pred += interpolated residual (anchored mode; point
-// (li, lj) of the tile at (u, w) = (li / T, lj / T)), tile min / max of pred,
-// bad flag for non-finite values (a NaN anchor makes its tiles exact).
-__global__ void k_tile_reduce(GridDesc g, float *pred, const float *resid, int interp,
-                              float *tmin, float *tmax, int *bad) {
-  __shared__ float s_mn[32], s_mx[32];
-  __shared__ int s_bad[32];
-  __shared__ float s_r[4][4];
-  const int t = blockIdx.x;
-  const int tx = t % g.ntx, ty = t / g.ntx;
-  if (resid && threadIdx.x < 16) {
-    const int a = threadIdx.x & 3, c = threadIdx.x >> 2;
-    s_r[c][a] = resid[anchor_index(g, tx, ty, a, c, interp)];
+// One warp per tile (kTileReduceWarps tiles per block): pred (+)= interpolated
+// residual (anchored mode; point (li, lj) of the tile at (u, w) = (li / T,
+// lj / T)), tile min / max of pred, bad flag for non-finite values (a NaN anchor
+// makes its tiles exact). pred_zero: pred holds zeros (it is written, not read).
+constexpr int kTileReduceWarps = 8;
+__global__ void __launch_bounds__(32 * kTileReduceWarps)
+    k_tile_reduce(GridDesc g, float *pred, const float *resid, int interp, int pred_zero,
+                  float *tmin, float *tmax, int *bad) {
+  __shared__ float s_r[kTileReduceWarps][4][4];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int64_t t = (int64_t)blockIdx.x * kTileReduceWarps + wid;
+  if (t >= (int64_t)g.ntx * g.nty) return;   // whole warps leave together
+  const int tx = (int)(t % g.ntx), ty = (int)(t / g.ntx);
+  if (resid && lane < 16) {
+    const int a = lane & 3, c = lane >> 2;
+    s_r[wid][c][a] = resid[anchor_index(g, tx, ty, a, c, interp)];
   }
-  __syncthreads();
+  __syncwarp();
+  float r[4][4];
+  if (resid) {
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+#pragma unroll
+      for (int a = 0; a < 4; ++a) r[c][a] = s_r[wid][c][a];
+  }
   float mn = INFINITY, mx = -INFINITY;
   int b = 0;
   const int T = g.tile;
-  for (int l = threadIdx.x; l < T * T; l += blockDim.x) {
+  for (int l = lane; l < T * T; l += 32) {
     const int li = l % T, lj = l / T;
     const int64_t i = (int64_t)tx * T + li, j = (int64_t)ty * T + lj;
     if (i >= g.nx || j >= g.ny) continue;
     const int64_t p = j * g.nx + i;
-    float v = pred[p];
+    float v = pred_zero ? 0.f : pred[p];
     if (resid) {
-      v += resid_interp(s_r, (float)li / T, (float)lj / T, interp);
+      v += resid_interp(r, (float)li / T, (float)lj / T, interp);
       pred[p] = v;
     }
     if (!(v > -INFINITY && v < INFINITY)) b = 1;   // also catches NaN
@@ -141,28 +151,22 @@ __global__ void k_tile_reduce(GridDesc g, float *pred, const float *resid, int i
     mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
     b |= __shfl_xor_sync(0xffffffffu, b, o);
   }
-  const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  if ((threadIdx.x & 31) == 0) { s_mn[warp] = mn; s_mx[warp] = mx; s_bad[warp] = b; }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    for (int w = 1; w < nw; ++w) {
-      mn = fminf(mn, s_mn[w]);
-      mx = fmaxf(mx, s_mx[w]);
-      b |= s_bad[w];
-    }
+  if (lane == 0) {
     tmin[t] = mn;
     tmax[t] = mx;
     bad[t] = b;
   }
 }
 
-// Largest finite value of v[0, n) -> *out (single block).
-// out[0] = the smallest positive finite value of v[0, n) (1.0 if there is none);
-// one block.
-__global__ void k_min_positive(const double *v, int64_t n, double *out) {
+// Smallest positive finite value of v[0, n): per block into part[blockIdx.x]
+// (INFINITY if none); with final, one block over part[0, n) -> out[0] (1.0 if
+// there is none). Launch: k_min_positive(v, n, part, false) on up to a few
+// thousand blocks, then k_min_positive(part, blocks, out, true) on one.
+__global__ void k_min_positive(const double *v, int64_t n, double *out, bool final) {
   __shared__ double s[32];
   double m = INFINITY;
-  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
     const double x = v[i];
     if (x > 0.0 && x < m) m = x;
   }
@@ -172,14 +176,16 @@ __global__ void k_min_positive(const double *v, int64_t n, double *out) {
   __syncthreads();
   if (threadIdx.x == 0) {
     for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = fmin(m, s[w]);
-    *out = m < INFINITY ? m : 1.0;
+    out[blockIdx.x] = final ? (m < INFINITY ? m : 1.0) : m;
   }
 }
 
+// Largest value below +inf of v[0, n) (NaN ignored), two stages as
+// k_min_positive: per block into out[blockIdx.x], then one block.
 __global__ void k_max_finite(const float *v, int n, float *out) {
   __shared__ float s[32];
   float m = -INFINITY;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const float x = v[i];
     if (x < INFINITY) m = fmaxf(m, x);
   }
@@ -189,7 +195,7 @@ __global__ void k_max_finite(const float *v, int n, float *out) {
   __syncthreads();
   if (threadIdx.x == 0) {
     for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = fmaxf(m, s[w]);
-    *out = m;
+    out[blockIdx.x] = m;
   }
 }
 
@@ -267,21 +273,38 @@ struct FlagArgs {
   unsigned long long *counts;   // [0] low, [1] flagged, [2] max probe error bits (non-low)
 };
 
+// Counts of a warp's tiles added with one atomic per counter (lane 0).
+__device__ __forceinline__ void flag_counts_add(unsigned long long *counts, bool low, bool flagged,
+                                                unsigned err_bits) {
+  const unsigned nl = __popc(__ballot_sync(0xffffffffu, low));
+  const unsigned nf = __popc(__ballot_sync(0xffffffffu, flagged));
+  const unsigned em = __reduce_max_sync(0xffffffffu, err_bits);
+  if ((threadIdx.x & 31) == 0) {
+    if (nl) atomicAdd(&counts[0], (unsigned long long)nl);
+    if (nf) atomicAdd(&counts[1], (unsigned long long)nf);
+    if (em) atomicMax(&counts[2], (unsigned long long)em);
+  }
+}
+
 __global__ void k_flag_tiles(FlagArgs a) {
   const int o = blockIdx.x * blockDim.x + threadIdx.x;
-  if (o >= a.g.ntx * a.g.nty) return;
-  const int t = a.order[o];
-  int f = a.all;
-  if (!f) {
-    const bool low = !(a.tmin[t] >= *a.gmax + a.log_low);
-    const float err = a.terr ? __uint_as_float(a.terr[t]) : 0.f;
-    f = a.bad[t] || low || !(err <= a.rel_tol);
-    if (low) atomicAdd(&a.counts[0], 1ull);
-    else atomicMax(&a.counts[2], (unsigned long long)__float_as_uint(err));
+  const bool in = o < a.g.ntx * a.g.nty;   // whole warps reach the counts
+  bool low = false;
+  int f = 0;
+  unsigned eb = 0;
+  if (in) {
+    const int t = a.order[o];
+    f = a.all;
+    if (!f) {
+      low = !(a.tmin[t] >= *a.gmax + a.log_low);
+      const float err = a.terr ? __uint_as_float(a.terr[t]) : 0.f;
+      f = a.bad[t] || low || !(err <= a.rel_tol);
+      if (!low) eb = __float_as_uint(err);
+    }
+    a.flag[t] = f;
+    a.flag_ord[o] = f;
   }
-  if (f) atomicAdd(&a.counts[1], 1ull);
-  a.flag[t] = f;
-  a.flag_ord[o] = f;
+  flag_counts_add(a.counts, low, f != 0, eb);
 }
 
 // Rescue candidates: tiles flagged by their probes alone (not low, no
@@ -350,22 +373,28 @@ __global__ void k_rescue_update(const int *list, int64_t n, const int *bad, cons
 // counts[2] start at 0).
 __global__ void k_flag_recount(FlagArgs a) {
   const int o = blockIdx.x * blockDim.x + threadIdx.x;
-  if (o >= a.g.ntx * a.g.nty) return;
-  const int t = a.order[o];
-  const int f = a.flag[t];
-  a.flag_ord[o] = f;
-  if (f) atomicAdd(&a.counts[1], 1ull);
-  if (a.tmin[t] >= *a.gmax + a.log_low) atomicMax(&a.counts[2], (unsigned long long)a.terr[t]);
+  const bool in = o < a.g.ntx * a.g.nty;   // whole warps reach the counts
+  int f = 0;
+  unsigned eb = 0;
+  if (in) {
+    const int t = a.order[o];
+    f = a.flag[t];
+    a.flag_ord[o] = f;
+    if (a.tmin[t] >= *a.gmax + a.log_low) eb = a.terr[t];
+  }
+  flag_counts_add(a.counts, false, f != 0, eb);
 }
 
-// out = exp(pred) on the tiles that keep the prediction.
-__global__ void k_apply(GridDesc g, const float *pred, const int *flag, double *out) {
-  const int64_t n = g.nx * g.ny;
-  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n;
-       p += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t i = p % g.nx, j = p / g.nx;
-    const int t = (int)(j / g.tile) * g.ntx + (int)(i / g.tile);
-    if (!flag[t]) out[p] = exp((double)pred[p]);
+// out = exp(pred) on the tiles that keep the prediction; rows over blockIdx.y,
+// columns over blockIdx.x (no 64-bit division per point); tile = 1 << tshift.
+__global__ void k_apply(GridDesc g, int tshift, const float *pred, const int *flag, double *out) {
+  for (int64_t j = blockIdx.y; j < g.ny; j += gridDim.y) {
+    const int64_t row = j * g.nx;
+    const int64_t trow = (j >> tshift) * g.ntx;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < g.nx;
+         i += (int64_t)gridDim.x * blockDim.x) {
+      if (!flag[trow + (i >> tshift)]) out[row + i] = exp((double)pred[row + i]);
+    }
   }
 }
 

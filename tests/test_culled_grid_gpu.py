@@ -257,6 +257,26 @@ def test_grid_exact_matches_direct(ctx):
     assert_parity(got32, want, 1e-6 + 1e-7, 1e-8, what="grid exact tile 32")
 
 
+@pytest.mark.parametrize("tiles_per_axis", [8, 16, 24, 32])
+def test_grid_exact_split_tiles(ctx, tiles_per_axis):
+    """Short tile-16 lists are summed by clusters of 8, 4 or 2 blocks per tile (each
+    part sums every S-th batch of reference groups; the parts share the thresholds
+    of the total near-field sum through distributed shared memory and part 0 adds
+    them in rank order). On 148 SMs these tile counts (64, 256, 576, 1024) run 8,
+    4, 2 and 1 parts; every one matches the direct sum, keeps the bound, and
+    repeats bitwise."""
+    desc = _setup_adaptive(ctx)
+    m = 16 * tiles_per_axis
+    grid = (m, m, -4.0, 4.0, -4.0, 4.0)
+    want = _direct_on_grid(ctx, desc, grid)
+    got, st = _grid_eval(ctx, desc, grid, mode=bk.GRID_EXACT, tile=16)
+    assert_parity(got, want, 1e-6 + 1e-7, 1e-8, what=f"{tiles_per_axis}^2 tiles")
+    assert st.max_bound_ratio <= 1e-7
+    assert st.tiles == tiles_per_axis ** 2 and st.exact_points == m * m
+    again, _ = _grid_eval(ctx, desc, grid, mode=bk.GRID_EXACT, tile=16)
+    assert np.array_equal(got, again)
+
+
 @pytest.mark.parametrize("kind,h", [(W.GAUSS_PROD2D, (0.05, 0.09)), (W.EPAN_PROD2D, (0.2, 0.15)),
                                     (W.EPAN, (0.2, 0.2))])
 def test_grid_exact_factored_and_pair_forms(ctx, kind, h):
