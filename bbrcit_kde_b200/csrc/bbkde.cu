@@ -125,7 +125,7 @@ struct bbkde_ctx {
   // bounds; dense-grid pipeline buffers
   CullCache cull;
   DevBuf ms_keys, ms_keys2, ms_perm, ms_perm2, ms_box, ms_tmp, cq_x, cq_y, cq_out, cb_bound,
-      cb_smin, cb_tiles, cb_stats;
+      cb_smin, cb_tiles, cb_stats, cb_key, cb_key2, cb_sched;
   DevBuf gr_pred, gr_order, gr_tmin, gr_tmax, gr_bad, gr_terr, gr_flag, gr_flag_ord, gr_list,
       gr_nsel, gr_counts, gr_gmax, gr_lat_order, gr_lat_exact, gr_lat_net, gr_q_order, gr_q_exact,
       gr_q_net, gr_resid, gr_cand_ord, gr_cand_xy, gr_cand_net, gr_out, gr_part;
@@ -741,6 +741,7 @@ int bbkde_ctx_destroy(bbkde_ctx *c) {
   for (DevBuf *b : {&c->cull.rec, &c->cull.ext, &c->cull.tiles, &c->cull.groups, &c->ms_keys,
                     &c->ms_keys2, &c->ms_perm, &c->ms_perm2, &c->ms_box, &c->ms_tmp, &c->cq_x,
                     &c->cq_y, &c->cq_out, &c->cb_bound, &c->cb_smin, &c->cb_tiles, &c->cb_stats,
+                    &c->cb_key, &c->cb_key2, &c->cb_sched,
                     &c->gr_pred, &c->gr_order, &c->gr_tmin, &c->gr_tmax, &c->gr_bad,
                     &c->gr_terr, &c->gr_flag, &c->gr_flag_ord, &c->gr_list, &c->gr_nsel,
                     &c->gr_counts, &c->gr_gmax, &c->gr_lat_order, &c->gr_lat_exact,
@@ -1524,6 +1525,37 @@ cudaError_t launch_cull_sep(int tile, int parts, unsigned nblk, cudaStream_t st,
   }
 }
 
+// Resident factored blocks per SM: 4 at tile 32 (registers), 12 at tile 16.
+int sep_resident(int tile) { return tile == 32 ? 4 : kSepResidentPerSm; }
+
+// Reach (log2 units) of the launch-order cost proxy of factored tiles: the
+// groups within 2^-32 of a tile's largest group bound.
+constexpr float kSepCostReach = 32.0f;
+
+template <int OP>
+int sep_schedule(bbkde_ctx *c, CullArgs &a, unsigned nblk) {
+  TRY(ensure(c, c->cb_key, (size_t)nblk * sizeof(unsigned)));
+  TRY(ensure(c, c->cb_key2, (size_t)nblk * sizeof(unsigned)));
+  TRY(ensure(c, c->cb_sched, (size_t)nblk * sizeof(int)));
+  k_sep_tile_cost<OP><<<(unsigned)((nblk * 32 + 255) / 256), 256, 0, c->stream>>>(
+      a, (int64_t)nblk, kSepCostReach, c->cb_key.as<unsigned>());
+  COUNT_LAUNCH(c);
+  CUDA_TRY(c, cudaGetLastError());
+  size_t tmp = 0;
+  CUDA_TRY(c, cub::DeviceRadixSort::SortPairs(nullptr, tmp, c->cb_key.as<unsigned>(),
+                                              c->cb_key2.as<unsigned>(), a.q.tile_list,
+                                              c->cb_sched.as<int>(), (int)nblk, 0, 32,
+                                              c->stream));
+  TRY(ensure(c, c->ms_tmp, tmp));
+  CUDA_TRY(c, cub::DeviceRadixSort::SortPairs(c->ms_tmp.p, tmp, c->cb_key.as<unsigned>(),
+                                              c->cb_key2.as<unsigned>(), a.q.tile_list,
+                                              c->cb_sched.as<int>(), (int)nblk, 0, 32,
+                                              c->stream));
+  c->launch_total += 4;
+  a.q.tile_list = c->cb_sched.as<int>();
+  return BBKDE_OK;
+}
+
 // Parts per tile for a factored launch of nblk tiles of edge `tile`.
 int sep_parts(const bbkde_ctx *c, int tile, unsigned nblk) {
   if (tile != 16) return 1;
@@ -1564,6 +1596,16 @@ int launch_culled(bbkde_ctx *c, const Resolved &r, int shape, unsigned nblk,
   const bool d2 = r.dim == 2;
   if (sep_tile > 0) {
     const int parts = sep_parts(c, sep_tile, nblk);
+    // More than one wave: launch the tiles most expensive first.
+    if (parts == 1 && q.mode == 1 &&
+        (int64_t)nblk > (int64_t)c->sm_count * sep_resident(sep_tile)) {
+      switch (r.op) {
+        case OP_GAUSS_ISO: TRY(sep_schedule<OP_GAUSS_ISO>(c, a, nblk)); break;
+        case OP_GAUSS_PROD: TRY(sep_schedule<OP_GAUSS_PROD>(c, a, nblk)); break;
+        case OP_EPAN_PROD: TRY(sep_schedule<OP_EPAN_PROD>(c, a, nblk)); break;
+        default: break;
+      }
+    }
     switch (r.op) {
       case OP_GAUSS_ISO:
         CUDA_TRY(c, launch_cull_sep<OP_GAUSS_ISO>(sep_tile, parts, nblk, c->stream, a));

@@ -469,4 +469,40 @@ __global__ void __launch_bounds__(T *T / 8, T == 32 ? 4 : 16)
   }
 }
 
+// Launch order of a long factored tile list, most expensive first (so that the
+// last wave is not left to the densest tiles): key[w] = ~(the number of
+// reference groups whose bound over tile tile_list[w]'s box lies within `reach`
+// (log2 units) of the largest such bound; for the Epanechnikov product, groups
+// whose support meets the box) -- about the groups the culled sum opens. One
+// warp per listed tile; an ascending stable sort of (key, tile) gives the order.
+template <int OP>
+__global__ void k_sep_tile_cost(CullArgs a, int64_t n, float reach, unsigned *key) {
+  const int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (w >= n) return;   // whole warps leave together
+  const CullQueries &q = a.q;
+  const int t = q.tile_list[w];
+  const int T = q.tile;
+  const int64_t i0 = (int64_t)(t % q.ntx) * T, j0 = (int64_t)(t / q.ntx) * T;
+  const int64_t i1 = (i0 + T < q.gnx ? i0 + T : q.gnx) - 1;
+  const int64_t j1 = (j0 + T < q.gny ? j0 + T : q.gny) - 1;
+  const float x0 = grid_coord(q.gx0, q.gdx, i0), x1 = grid_coord(q.gx0, q.gdx, i1);
+  const float y0 = grid_coord(q.gy0, q.gdy, j0), y1 = grid_coord(q.gy0, q.gdy, j1);
+  unsigned cnt = 0;
+  if (op_gauss(OP)) {
+    float e = -INFINITY;
+    for (int gi = lane; gi < a.n_groups; gi += 32)
+      e = fmaxf(e, a.groups[gi].lm + tile_peak<OP, 2>(a.groups[gi], x0, x1, y0, y1));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) e = fmaxf(e, __shfl_xor_sync(0xffffffffu, e, o));
+    for (int gi = lane; gi < a.n_groups; gi += 32)
+      cnt += a.groups[gi].lm + tile_peak<OP, 2>(a.groups[gi], x0, x1, y0, y1) >= e - reach;
+  } else {
+    for (int gi = lane; gi < a.n_groups; gi += 32)
+      cnt += tile_peak<OP, 2>(a.groups[gi], x0, x1, y0, y1) > 0.f;
+  }
+  cnt = __reduce_add_sync(0xffffffffu, cnt);
+  if (lane == 0) key[w] = ~cnt;
+}
+
 }  // namespace bbkde
