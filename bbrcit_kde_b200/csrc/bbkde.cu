@@ -128,7 +128,8 @@ struct bbkde_ctx {
       cb_smin, cb_tiles, cb_stats, cb_key, cb_key2, cb_sched;
   DevBuf gr_pred, gr_order, gr_tmin, gr_tmax, gr_bad, gr_terr, gr_flag, gr_flag_ord, gr_list,
       gr_nsel, gr_counts, gr_gmax, gr_lat_order, gr_lat_exact, gr_lat_net, gr_q_order, gr_q_exact,
-      gr_q_net, gr_resid, gr_cand_ord, gr_cand_xy, gr_cand_net, gr_out, gr_part;
+      gr_q_net, gr_resid, gr_cand_ord, gr_cand_xy, gr_cand_net, gr_out, gr_part, gr_rl_idx,
+      gr_rl_xy, gr_rl_net;
   cudaEvent_t ev3 = nullptr;
   // smallest positive abw of the reference set, for the (coordinate, attribute)
   // versions it was computed at
@@ -747,7 +748,7 @@ int bbkde_ctx_destroy(bbkde_ctx *c) {
                     &c->gr_counts, &c->gr_gmax, &c->gr_lat_order, &c->gr_lat_exact,
                     &c->gr_lat_net, &c->gr_q_order, &c->gr_q_exact, &c->gr_q_net, &c->gr_resid,
                     &c->gr_cand_ord, &c->gr_cand_xy, &c->gr_cand_net, &c->gr_out,
-                    &c->gr_part})
+                    &c->gr_part, &c->gr_rl_idx, &c->gr_rl_xy, &c->gr_rl_net})
     release(*b);
   if (c->cv_graph) cudaGraphExecDestroy(c->cv_graph);
   if (c->ev3) cudaEventDestroy(c->ev3);
@@ -1487,7 +1488,8 @@ void launch_cull_op(int shape, unsigned nblk, cudaStream_t st, const CullArgs &a
 
 // Tile-16 lists shorter than this many tiles per SM are split: each tile's
 // reference groups are shared by a cluster of 2, 4 or 8 blocks (the resident
-// tile-16 blocks per SM: 12 by shared memory).
+// tile-16 blocks per SM: 12 by shared memory; 16-block clusters measured slower:
+// 1.57 vs 1.31 ms on the 8192^2 fallback).
 constexpr int kSepResidentPerSm = 12;
 
 template <int OP, int S>
@@ -2253,7 +2255,26 @@ extern "C" int bbkde_eval_grid(bbkde_ctx *c, bbkde_surrogate *sur, const bbkde_k
       CUDA_TRY(c, cudaStreamSynchronize(c->stream));
       if (ncand > 0) {
         const int *cand = c->gr_list.as<int>();
-        TRY(lattice_net());
+        // The network on the lattice points the candidates read (their anchors
+        // and probes), not on the whole lattice; NaN elsewhere (read by nothing).
+        const int64_t nl = (int64_t)ncand * kRescueSlots;
+        TRY(ensure(c, c->gr_lat_net, (size_t)n_lat * sizeof(float)));
+        TRY(ensure(c, c->gr_rl_idx, (size_t)nl * sizeof(int64_t)));
+        TRY(ensure(c, c->gr_rl_xy, (size_t)nl * sizeof(float2)));
+        TRY(ensure(c, c->gr_rl_net, (size_t)nl * sizeof(float)));
+        CUDA_TRY(c, cudaMemsetAsync(c->gr_lat_net.p, 0xff, (size_t)n_lat * sizeof(float),
+                                    c->stream));
+        k_rescue_lattice_points<<<grid1d(nl), 256, 0, c->stream>>>(
+            g, gl, cand, ncand, c->gr_rl_idx.as<int64_t>(), c->gr_rl_xy.as<float2>());
+        COUNT_LAUNCH(c);
+        TRY(bbkde::surrogate_infer(sur, c->stream, nl, c->gr_rl_xy.as<float2>(), 0, 0.0, 0.0,
+                                   0.0, 0.0, c->gr_rl_net.as<float>()) == BBKDE_OK
+                ? BBKDE_OK
+                : fail(c, BBKDE_CUDA_ERROR, "grid: surrogate inference failed"));
+        COUNT_LAUNCH(c);
+        k_scatter_net<<<grid1d(nl), 256, 0, c->stream>>>(
+            c->gr_rl_idx.as<int64_t>(), c->gr_rl_net.as<float>(), nl, c->gr_lat_net.as<float>());
+        COUNT_LAUNCH(c);
         lat_net = c->gr_lat_net.as<float>();
         if (P == 9) {
           TRY(quarter_net());
@@ -2295,8 +2316,8 @@ extern "C" int bbkde_eval_grid(bbkde_ctx *c, bbkde_surrogate *sur, const bbkde_k
       CUDA_TRY(c, cudaEventRecord(c->ev2, c->stream));
     }
     // 6. Predicted values on the tiles that keep them.
-    const dim3 ab((unsigned)std::min<int64_t>((g.nx + 255) / 256, 64),
-                  (unsigned)std::min<int64_t>(g.ny, 65535));
+    const dim3 ab((unsigned)std::min<int64_t>((g.nx + 1023) / 1024, 16),
+                  (unsigned)std::min<int64_t>(g.ny, (int64_t)c->sm_count * 8));
     k_apply<<<ab, 256, 0, c->stream>>>(g, T == 32 ? 5 : 4, c->gr_pred.as<float>(),
                                        c->gr_flag.as<int>(), out);
     COUNT_LAUNCH(c);

@@ -121,24 +121,48 @@ __global__ void __launch_bounds__(32 * kTileReduceWarps)
     s_r[wid][c][a] = resid[anchor_index(g, tx, ty, a, c, interp)];
   }
   __syncwarp();
-  float r[4][4];
+  // T (16 or 32) divides 32 * k for the lane's points l = lane + 32 k, so a lane
+  // keeps one column li: the column weights fold into the four row values once.
+  const int T = g.tile;
+  const int tsh = T == 32 ? 5 : 4;
+  const int li = lane & (T - 1);
+  const float invT = 1.0f / (float)T;
+  float rc[4] = {0.f, 0.f, 0.f, 0.f};   // bicubic: sum_a wu[a] r[c][a]
+  float r11 = 0.f, r12 = 0.f, r21 = 0.f, r22 = 0.f;
   if (resid) {
+    const float u = (float)li * invT;
+    if (interp == 3) {
+      float wu[4];
+      cr_weights(u, wu);
 #pragma unroll
-    for (int c = 0; c < 4; ++c)
-#pragma unroll
-      for (int a = 0; a < 4; ++a) r[c][a] = s_r[wid][c][a];
+      for (int c = 0; c < 4; ++c)
+        rc[c] = wu[0] * s_r[wid][c][0] + wu[1] * s_r[wid][c][1] + wu[2] * s_r[wid][c][2] +
+                wu[3] * s_r[wid][c][3];
+    } else {
+      r11 = s_r[wid][1][1]; r12 = s_r[wid][1][2];
+      r21 = s_r[wid][2][1]; r22 = s_r[wid][2][2];
+    }
   }
   float mn = INFINITY, mx = -INFINITY;
   int b = 0;
-  const int T = g.tile;
+  const int64_t i = (int64_t)tx * T + li;
   for (int l = lane; l < T * T; l += 32) {
-    const int li = l % T, lj = l / T;
-    const int64_t i = (int64_t)tx * T + li, j = (int64_t)ty * T + lj;
+    const int lj = l >> tsh;
+    const int64_t j = (int64_t)ty * T + lj;
     if (i >= g.nx || j >= g.ny) continue;
     const int64_t p = j * g.nx + i;
     float v = pred_zero ? 0.f : pred[p];
     if (resid) {
-      v += resid_interp(r, (float)li / T, (float)lj / T, interp);
+      // the same interpolant as resid_interp, evaluated column-first
+      const float w = (float)lj * invT;
+      if (interp == 3) {
+        float wv[4];
+        cr_weights(w, wv);
+        v += wv[0] * rc[0] + wv[1] * rc[1] + wv[2] * rc[2] + wv[3] * rc[3];
+      } else {
+        const float u = (float)li * invT;
+        v += (1.f - w) * ((1.f - u) * r11 + u * r12) + w * ((1.f - u) * r21 + u * r22);
+      }
       pred[p] = v;
     }
     if (!(v > -INFINITY && v < INFINITY)) b = 1;   // also catches NaN
@@ -366,6 +390,38 @@ __global__ void k_rescue_update(const int *list, int64_t n, const int *bad, cons
   if (i >= n) return;
   const int t = list[i];
   flag[t] = bad[t] || !(__uint_as_float(terr[t]) <= rel_tol);
+}
+
+// Lattice points that the rescue reads for candidate tile cand[c]: slots 0-15
+// its 4 x 4 anchors (the bicubic stencil, clamped at the lattice's edge; bilinear
+// reads its inner 2 x 2), slots 16-20 its centre and edge-midpoint probes. Entry
+// k = c * kRescueSlots + s gets the half-pitch lattice index idx[k] and the point's
+// coordinates xy[k], computed as the inference computes lattice coordinates, so
+// the network values equal the whole-lattice ones.
+constexpr int kRescueSlots = 21;
+__global__ void k_rescue_lattice_points(GridDesc g, GridDesc gl, const int *cand, int64_t n,
+                                        int64_t *idx, float2 *xy) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n * kRescueSlots) return;
+  const int t = cand[k / kRescueSlots];
+  const int s = (int)(k % kRescueSlots);
+  const int tx = t % g.ntx, ty = t / g.ntx;
+  int64_t lx, ly;
+  if (s < 16) {
+    lx = 2 * (int64_t)min(max(tx - 1 + (s & 3), 0), g.ntx);
+    ly = 2 * (int64_t)min(max(ty - 1 + (s >> 2), 0), g.nty);
+  } else {
+    lx = 2 * (int64_t)tx + kProbeDA[s - 16];
+    ly = 2 * (int64_t)ty + kProbeDB[s - 16];
+  }
+  idx[k] = ly * gl.nx + lx;
+  xy[k] = make_float2((float)(gl.x0 + (double)lx * gl.dx), (float)(gl.y0 + (double)ly * gl.dy));
+}
+
+// dst[idx[k]] = v[k] (repeated indices carry equal values).
+__global__ void k_scatter_net(const int64_t *idx, const float *v, int64_t n, float *dst) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) dst[idx[k]] = v[k];
 }
 
 // Flags per Morton position, flagged count and largest probe error over tiles

@@ -257,13 +257,13 @@ def test_grid_exact_matches_direct(ctx):
     assert_parity(got32, want, 1e-6 + 1e-7, 1e-8, what="grid exact tile 32")
 
 
-@pytest.mark.parametrize("tiles_per_axis", [8, 16, 24, 32])
+@pytest.mark.parametrize("tiles_per_axis", [8, 12, 16, 24, 32])
 def test_grid_exact_split_tiles(ctx, tiles_per_axis):
     """Short tile-16 lists are summed by clusters of 8, 4 or 2 blocks per tile (each
     part sums every S-th batch of reference groups; the parts share the thresholds
     of the total near-field sum through distributed shared memory and part 0 adds
-    them in rank order). On 148 SMs these tile counts (64, 256, 576, 1024) run 8,
-    4, 2 and 1 parts; every one matches the direct sum, keeps the bound, and
+    them in rank order). On 148 SMs these tile counts (64, 144, 256, 576, 1024) run
+    8, 8, 4, 2 and 1 parts; every one matches the direct sum, keeps the bound, and
     repeats bitwise."""
     desc = _setup_adaptive(ctx)
     m = 16 * tiles_per_axis
