@@ -157,11 +157,19 @@ __global__ void __launch_bounds__(T *T / 8, T == 32 ? 4 : 16)
   };
 
   // This thread's factor: column w or row w - T of team ft.
-  const int fw = tid % (2 * T), ft = tid / (2 * T);
-  const bool fx = fw < T;
-  const float fq = fx ? s_qx[fw] : s_qy[fw - T];
+  // T = 16: thread w of each 2T-thread team computes column w (w < T) or row
+  // w - T. T = 32: every warp is a team whose lane l computes columns (or, from
+  // lane 16 on, rows) 2 (l mod 16) and 2 (l mod 16) + 1, so that each broadcast
+  // load of a reference pair's record feeds two factors.
+  constexpr bool kTwoCol = T == 32;
+  constexpr int NT2 = BLOCK / 32;      // teams of the two-column mapping
+  const int fw = kTwoCol ? 2 * (lane & 15) : tid % (2 * T);
+  const int ft = kTwoCol ? warp : tid / (2 * T);
+  const bool fx = kTwoCol ? lane < 16 : fw < T;
+  const int fcol = fx || kTwoCol ? fw : fw - T;
+  const float fq = fx ? s_qx[fcol] : s_qy[fcol];
+  const float fq1 = kTwoCol ? (fx ? s_qx[fcol + 1] : s_qy[fcol + 1]) : 0.f;
   const int foff = fx ? 0 : STG;
-  const int fcol = fx ? fw : fw - T;
   float2 *const fbase = s_fac + (fx ? 0 : FROWS * T);
   // Column swizzle of factor row p (see the layout note).
   auto swz = [](int p) { return T == 16 ? (p & 1) << 3 : 0; };
@@ -246,7 +254,25 @@ __global__ void __launch_bounds__(T *T / 8, T == 32 ? 4 : 16)
         u = __ffma2_rn(s2, dd, f2(1.0f));
         u = make_float2(fmaxf(u.x, 0.f), fmaxf(u.y, 0.f));
       }
-      fbase[b * FBUF + p * T + (fcol ^ swz(p))] = __fmul2_rn(m2, u);
+      if constexpr (kTwoCol) {
+        // the second column, the same reference pair; both stored as one 128-bit
+        // record (columns fcol, fcol + 1 are adjacent; no swizzle at T = 32)
+        const float2 d1 = __fadd2_rn(f2(fq1), c2);
+        const float2 dd1 = __fmul2_rn(d1, d1);
+        float2 u1;
+        if (kGauss) {
+          const float2 e1 = __fmul2_rn(s2, dd1);
+          u1 = make_float2(ex2_approx(e1.x), ex2_approx(e1.y));
+        } else {
+          u1 = __ffma2_rn(s2, dd1, f2(1.0f));
+          u1 = make_float2(fmaxf(u1.x, 0.f), fmaxf(u1.y, 0.f));
+        }
+        const float2 v0 = __fmul2_rn(m2, u), v1 = __fmul2_rn(m2, u1);
+        *reinterpret_cast<float4 *>(&fbase[b * FBUF + p * T + fcol]) =
+            make_float4(v0.x, v0.y, v1.x, v1.y);
+      } else {
+        fbase[b * FBUF + p * T + (fcol ^ swz(p))] = __fmul2_rn(m2, u);
+      }
     };
     // acc[4 kr + kc] (+)= y[kr] * x[kc] for factor pair p of buffer b.
     auto step = [&](int b, int p, float2 (&acc)[16], bool first) {
@@ -267,7 +293,11 @@ __global__ void __launch_bounds__(T *T / 8, T == 32 ? 4 : 16)
           acc[4 * kr + kc] = first ? __fmul2_rn(y[kr], x[kc])
                                    : __ffma2_rn(y[kr], x[kc], acc[4 * kr + kc]);
     };
-    for (int p = ft; p < FROWS; p += NG) factor(0, 0, p);
+    if constexpr (kTwoCol) {
+      for (int p = ft; p < FROWS; p += NT2) factor(0, 0, p);
+    } else {
+      for (int p = ft; p < FROWS; p += NG) factor(0, 0, p);
+    }
     __syncthreads();
     // One FP32 partial per sub-chunk and split (16 references at T = 16, 32 at
     // T = 32: two interleaved halves, as the pair form's kChunk), then its Kahan
@@ -282,9 +312,15 @@ __global__ void __launch_bounds__(T *T / 8, T == 32 ? 4 : 16)
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
           if (more) {
+            if constexpr (kTwoCol) {
+              // FROWS / NT2 = 8 calls per sub-chunk: one every other step
+              static_assert(FROWS / NT2 == 8 && FROWS / 16 == 2, "two-column schedule");
+              if ((i & 1) == 0) factor(cur ^ 1, (sb + 1) * SUB, ft + (ch * 4 + i / 2) * NT2);
+            } else {
 #pragma unroll
-            for (int f = 0; f < FPB; ++f)
-              factor(cur ^ 1, (sb + 1) * SUB, ft + ((ch * 8 + i) * FPB + f) * NG);
+              for (int f = 0; f < FPB; ++f)
+                factor(cur ^ 1, (sb + 1) * SUB, ft + ((ch * 8 + i) * FPB + f) * NG);
+            }
           }
           step(cur, ch * 16 + 2 * i + sp, acc, ch == 0 && i == 0);
         }
