@@ -77,13 +77,11 @@ __global__ void __launch_bounds__(T *T / 8, T == 32 ? 4 : 16)
   constexpr int NSUB = kRefTile / SUB;
   constexpr int FROWS = SUB / 2;       // reference pairs per sub-chunk
   constexpr int FBUF = 2 * FROWS * T;  // factor pairs per buffer (x rows, then y rows)
-  constexpr int NG = BLOCK / (2 * T);  // factor teams (references split between them)
-  constexpr int FPB = 2 / NG;          // factor pairs per lane per accumulation step
   constexpr int STG = kRefTile + 4;    // staged column stride (x and y on different banks)
   constexpr bool kGauss = op_gauss(OP);
   constexpr bool kExt = op_has_extra(OP);
   static_assert(BLOCK == 2 * LPS, "two splits");
-  static_assert(NG * FPB == 2 && kChunk == 32, "one factor step per accumulation step");
+  static_assert(kChunk == 32, "partials of the pair form's chunk");
   static_assert(kRefTile % SUB == 0 && FROWS % (kChunk / 2) == 0, "shape");
   static_assert(FBUF >= T * T, "exchange area: two T x T double arrays");
   static_assert(S == 1 || S == 2 || S == 4 || S == 8, "cluster size");
@@ -157,18 +155,17 @@ __global__ void __launch_bounds__(T *T / 8, T == 32 ? 4 : 16)
   };
 
   // This thread's factor: column w or row w - T of team ft.
-  // T = 16: thread w of each 2T-thread team computes column w (w < T) or row
-  // w - T. T = 32: every warp is a team whose lane l computes columns (or, from
-  // lane 16 on, rows) 2 (l mod 16) and 2 (l mod 16) + 1, so that each broadcast
-  // load of a reference pair's record feeds two factors.
-  constexpr bool kTwoCol = T == 32;
-  constexpr int NT2 = BLOCK / 32;      // teams of the two-column mapping
-  const int fw = kTwoCol ? 2 * (lane & 15) : tid % (2 * T);
-  const int ft = kTwoCol ? warp : tid / (2 * T);
-  const bool fx = kTwoCol ? lane < 16 : fw < T;
-  const int fcol = fx || kTwoCol ? fw : fw - T;
+  // Factor teams of T threads: thread f of a team computes columns (f < T/2) or
+  // rows (f >= T/2) 2 (f mod T/2) and 2 (f mod T/2) + 1, two references at a
+  // time, so that each broadcast load of a reference pair's record feeds two
+  // factors; team ft takes the pairs ft, ft + NTM, ... of a sub-chunk.
+  constexpr int NTM = BLOCK / T;       // factor teams: 4 at T = 32, 2 at T = 16
+  static_assert(FROWS / NTM == 8, "eight factor calls per sub-chunk and lane");
+  const int fl = tid % T, ft = tid / T;
+  const bool fx = fl < T / 2;
+  const int fcol = 2 * (fl % (T / 2));
   const float fq = fx ? s_qx[fcol] : s_qy[fcol];
-  const float fq1 = kTwoCol ? (fx ? s_qx[fcol + 1] : s_qy[fcol + 1]) : 0.f;
+  const float fq1 = fx ? s_qx[fcol + 1] : s_qy[fcol + 1];
   const int foff = fx ? 0 : STG;
   float2 *const fbase = s_fac + (fx ? 0 : FROWS * T);
   // Column swizzle of factor row p (see the layout note).
@@ -254,9 +251,9 @@ __global__ void __launch_bounds__(T *T / 8, T == 32 ? 4 : 16)
         u = __ffma2_rn(s2, dd, f2(1.0f));
         u = make_float2(fmaxf(u.x, 0.f), fmaxf(u.y, 0.f));
       }
-      if constexpr (kTwoCol) {
+      {
         // the second column, the same reference pair; both stored as one 128-bit
-        // record (columns fcol, fcol + 1 are adjacent; no swizzle at T = 32)
+        // record (columns fcol, fcol + 1 stay adjacent under the swizzle)
         const float2 d1 = __fadd2_rn(f2(fq1), c2);
         const float2 dd1 = __fmul2_rn(d1, d1);
         float2 u1;
@@ -268,10 +265,8 @@ __global__ void __launch_bounds__(T *T / 8, T == 32 ? 4 : 16)
           u1 = make_float2(fmaxf(u1.x, 0.f), fmaxf(u1.y, 0.f));
         }
         const float2 v0 = __fmul2_rn(m2, u), v1 = __fmul2_rn(m2, u1);
-        *reinterpret_cast<float4 *>(&fbase[b * FBUF + p * T + fcol]) =
+        *reinterpret_cast<float4 *>(&fbase[b * FBUF + p * T + (fcol ^ swz(p))]) =
             make_float4(v0.x, v0.y, v1.x, v1.y);
-      } else {
-        fbase[b * FBUF + p * T + (fcol ^ swz(p))] = __fmul2_rn(m2, u);
       }
     };
     // acc[4 kr + kc] (+)= y[kr] * x[kc] for factor pair p of buffer b.
@@ -293,11 +288,7 @@ __global__ void __launch_bounds__(T *T / 8, T == 32 ? 4 : 16)
           acc[4 * kr + kc] = first ? __fmul2_rn(y[kr], x[kc])
                                    : __ffma2_rn(y[kr], x[kc], acc[4 * kr + kc]);
     };
-    if constexpr (kTwoCol) {
-      for (int p = ft; p < FROWS; p += NT2) factor(0, 0, p);
-    } else {
-      for (int p = ft; p < FROWS; p += NG) factor(0, 0, p);
-    }
+    for (int p = ft; p < FROWS; p += NTM) factor(0, 0, p);
     __syncthreads();
     // One FP32 partial per sub-chunk and split (16 references at T = 16, 32 at
     // T = 32: two interleaved halves, as the pair form's kChunk), then its Kahan
@@ -312,14 +303,12 @@ __global__ void __launch_bounds__(T *T / 8, T == 32 ? 4 : 16)
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
           if (more) {
-            if constexpr (kTwoCol) {
-              // FROWS / NT2 = 8 calls per sub-chunk: one every other step
-              static_assert(FROWS / NT2 == 8 && FROWS / 16 == 2, "two-column schedule");
-              if ((i & 1) == 0) factor(cur ^ 1, (sb + 1) * SUB, ft + (ch * 4 + i / 2) * NT2);
+            // eight calls per sub-chunk: every other step at T = 32 (two parts),
+            // every step at T = 16
+            if constexpr (T == 32) {
+              if ((i & 1) == 0) factor(cur ^ 1, (sb + 1) * SUB, ft + (ch * 4 + i / 2) * NTM);
             } else {
-#pragma unroll
-              for (int f = 0; f < FPB; ++f)
-                factor(cur ^ 1, (sb + 1) * SUB, ft + ((ch * 8 + i) * FPB + f) * NG);
+              factor(cur ^ 1, (sb + 1) * SUB, ft + i * NTM);
             }
           }
           step(cur, ch * 16 + 2 * i + sp, acc, ch == 0 && i == 0);
