@@ -1132,20 +1132,42 @@ extern "C" int bbkde_cv_batch(bbkde_ctx *c, int kind, int n_sets, const bbkde_da
     s.gx = (int)std::floor((xmax - xmin) * s.inv_cell) + 1;
     s.gy = (int)std::floor((ymax - ymin) * s.inv_cell) + 1;
     const int64_t ncell = (int64_t)s.gx * s.gy;
-    std::vector<int64_t> cnt(ncell + 1, 0), key(n);
+    // Sort key: the cell, then the Morton order of the position inside the cell
+    // (16 bits per axis), so that consecutive points of a cell are neighbours.
+    auto spread16 = [](uint32_t v) {
+      v &= 0xffffu;
+      v = (v | (v << 8)) & 0x00ff00ffu;
+      v = (v | (v << 4)) & 0x0f0f0f0fu;
+      v = (v | (v << 2)) & 0x33333333u;
+      v = (v | (v << 1)) & 0x55555555u;
+      return v;
+    };
+    std::vector<int64_t> cnt(ncell + 1, 0);
+    std::vector<uint64_t> key(n);
     for (int64_t i = 0; i < n; ++i) {
-      int cx = std::min(s.gx - 1, std::max(0, (int)std::floor((d.coords[2 * i] - xmin) * s.inv_cell)));
-      int cy = std::min(s.gy - 1, std::max(0, (int)std::floor((d.coords[2 * i + 1] - ymin) * s.inv_cell)));
-      key[i] = (int64_t)cy * s.gx + cx;
-      ++cnt[key[i] + 1];
+      const double fx = (d.coords[2 * i] - xmin) * s.inv_cell;
+      const double fy = (d.coords[2 * i + 1] - ymin) * s.inv_cell;
+      const int cx = std::min(s.gx - 1, std::max(0, (int)std::floor(fx)));
+      const int cy = std::min(s.gy - 1, std::max(0, (int)std::floor(fy)));
+      const int64_t cell_id = (int64_t)cy * s.gx + cx;
+      auto sub = [](double f) {
+        return (uint32_t)std::min(65535.0, std::max(0.0, std::floor(f * 65536.0)));
+      };
+      key[i] = ((uint64_t)cell_id << 32) |
+               (spread16(sub(fx - cx)) | (spread16(sub(fy - cy)) << 1));
+      ++cnt[cell_id + 1];
     }
     for (int64_t k = 0; k < ncell; ++k) cnt[k + 1] += cnt[k];
     cells.insert(cells.end(), cnt.begin(), cnt.end());   // set-relative cell_start
-    std::vector<int64_t> pos(cnt.begin(), cnt.end() - 1);
+    std::vector<int64_t> order(n);
+    for (int64_t i = 0; i < n; ++i) order[i] = i;
+    std::sort(order.begin(), order.end(), [&](int64_t u, int64_t v) {
+      return key[u] != key[v] ? key[u] < key[v] : u < v;
+    });
     X.resize(s.begin + n); Y.resize(s.begin + n); Wt.resize(s.begin + n);
     double diag = 0;
-    for (int64_t i = 0; i < n; ++i) {                      // stable counting sort
-      const int64_t at = s.begin + pos[key[i]]++;
+    for (int64_t r = 0; r < n; ++r) {
+      const int64_t i = order[r], at = s.begin + r;
       const double w = (d.weights ? d.weights[i] : 1.0) / wt;
       X[at] = d.coords[2 * i];
       Y[at] = d.coords[2 * i + 1];

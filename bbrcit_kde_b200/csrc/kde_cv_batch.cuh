@@ -24,8 +24,9 @@
 //   accumulated over all pairs (i < j, doubled) rather than per query.
 //
 // Pairs are enumerated from a uniform grid over each dataset (points sorted by
-// grid cell on the host), visiting only cells within the largest support. All
-// arithmetic of the final scores is FP64; the moments are exact 64-bit fixed point.
+// grid cell on the host, in Morton order inside each cell), visiting only cells
+// within the largest support. All arithmetic of the final scores is FP64; the
+// moments are exact 64-bit fixed point.
 #pragma once
 
 #include <cstdint>
@@ -143,16 +144,52 @@ __device__ __forceinline__ void cv_ranges(const CvSet &s, const int64_t *cs, int
 constexpr double kCvFixLik = 4611686018427387904.0;   // 2^62: sum of masses <= 1
 constexpr double kCvFixConv = 2305843009213693952.0;  // 2^61: sum of 2 w_i m_j <= 2
 
+// Run accumulation: a thread keeps the four fixed-point moments of its latest
+// cell in registers while consecutive pairs fall into the same (p, q) cell, and
+// adds them to the histograms when the cell changes (and at the end of its
+// pairs). Points are Morton-ordered within each grid cell, so consecutive pairs
+// of a thread are spatial neighbours and share a cell wherever the bandwidth
+// bins are wider than the point spacing. The sums are the same integers in
+// another order: exact, and the histograms identical.
+struct CvRun {
+  int c = -1;
+  unsigned long long a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+};
+
 // Fire-and-forget shared-memory reduction (no returned value, so the warp does
 // not wait for it); exact 64-bit integer addition.
-__device__ __forceinline__ void cv_add(unsigned long long *h, double v) {
-  const unsigned long long iv = (unsigned long long)__double2ll_rn(v);
+__device__ __forceinline__ void cv_red(unsigned long long *h, unsigned long long iv) {
   const unsigned addr = (unsigned)__cvta_generic_to_shared(h);
   asm volatile("red.shared.add.u64 [%0], %1;" ::"r"(addr), "l"(iv) : "memory");
 }
 
+__device__ __forceinline__ void cv_run_flush(unsigned long long *H, CvRun &r) {
+  if (r.c >= 0) {
+    cv_red(&H[r.c], r.a0);
+    cv_red(&H[kCvHist + r.c], r.a1);
+    cv_red(&H[2 * kCvHist + r.c], r.a2);
+    cv_red(&H[3 * kCvHist + r.c], r.a3);
+    r.c = -1;
+  }
+}
+
+__device__ __forceinline__ void cv_run_add(unsigned long long *H, CvRun &r, int c, double v0,
+                                           double v1, double v2, double v3) {
+  const unsigned long long i0 = (unsigned long long)__double2ll_rn(v0);
+  const unsigned long long i1 = (unsigned long long)__double2ll_rn(v1);
+  const unsigned long long i2 = (unsigned long long)__double2ll_rn(v2);
+  const unsigned long long i3 = (unsigned long long)__double2ll_rn(v3);
+  if (c != r.c) {
+    cv_run_flush(H, r);
+    r.c = c;
+    r.a0 = i0; r.a1 = i1; r.a2 = i2; r.a3 = i3;
+  } else {
+    r.a0 += i0; r.a1 += i1; r.a2 += i2; r.a3 += i3;
+  }
+}
+
 constexpr int kCvQBlock = 256;   // queries of one convolution item (staged in smem)
-constexpr int kCvUnroll = 4;     // consecutive candidates per thread and step
+constexpr int kCvUnroll = 2;     // consecutive candidates per thread and step
 
 // Shared memory: H[4][kCvHist] (fixed point, then FP64 in place) | hx | hy |
 // 1/hx | 1/hy | 1/hx^2 | 1/hy^2 | query block x, y, 2 w | ranges | misc | LUTs.
@@ -222,6 +259,7 @@ __global__ void __launch_bounds__(1024, 1) k_cv_batch(CvArgs a) {
         const int nr = misc[1];
         const int64_t total = pre[nr];
         int r = 0;
+        CvRun run;
         for (int64_t base = (int64_t)tid * kCvUnroll; base < total;
              base += (int64_t)nt * kCvUnroll) {
           int64_t js[kCvUnroll];
@@ -256,12 +294,10 @@ __global__ void __launch_bounds__(1024, 1) k_cv_batch(CvArgs a) {
             const double ms = ws[u] * kCvFixLik;
             const double xt = ax * ihx[p], yt = ay * ihy[q];
             const double x2 = xt * xt, y2 = yt * yt;
-            cv_add(&H[c], ms);
-            cv_add(&H[kCvHist + c], ms * x2);
-            cv_add(&H[2 * kCvHist + c], ms * y2);
-            cv_add(&H[3 * kCvHist + c], ms * x2 * y2);
+            cv_run_add(H, run, c, ms, ms * x2, ms * y2, ms * x2 * y2);
           }
         }
+        cv_run_flush(H, run);
         __syncthreads();
         // Fixed point -> FP64 moments sum m dx^k dy^l (k, l in {0, 2}).
         for (int c = tid; c < kCvCells; c += nt) {
@@ -336,6 +372,7 @@ __global__ void __launch_bounds__(1024, 1) k_cv_batch(CvArgs a) {
       const int64_t total = pre[nr];
       const double hx2 = 2.0 * hxmax, hy2 = 2.0 * hymax;
       int r = 0;
+      CvRun run;
       for (int64_t k = tid; k < total; k += nt) {
         while (k >= pre[r + 1]) ++r;
         const int64_t j = rb[r] + (k - pre[r]);
@@ -361,12 +398,10 @@ __global__ void __launch_bounds__(1024, 1) k_cv_batch(CvArgs a) {
           else if (g == 3) xk = x2 * x2 * xt;
           const double v = v0 * xk;
           const double y2 = yt * yt;
-          cv_add(&H[c], v);
-          cv_add(&H[kCvHist + c], v * y2);
-          cv_add(&H[2 * kCvHist + c], v * y2 * yt);
-          cv_add(&H[3 * kCvHist + c], v * y2 * y2 * yt);
+          cv_run_add(H, run, c, v, v * y2, v * y2 * yt, v * y2 * y2 * yt);
         }
       }
+      cv_run_flush(H, run);
       __syncthreads();
       unsigned long long *dst = reinterpret_cast<unsigned long long *>(a.conv_hist) +
                                 ((int64_t)item.set * 16 + 4 * g) * kCvCells;
