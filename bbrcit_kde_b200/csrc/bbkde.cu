@@ -391,7 +391,8 @@ struct Plan {
 
 // Split the reference range into segments so that the grid fills the device
 // with ~16 waves of blocks (load balance through the hardware block scheduler),
-// but never below 512 references per segment.
+// but never below one staging tile of references per segment (small problems:
+// 10,000 x 10,000 pairs would otherwise run on half the SMs).
 Plan plan_launch(const bbkde_ctx *c, int64_t n_ref, int64_t q_count, int q_per_block,
                  int tile) {
   Plan p;
@@ -399,7 +400,7 @@ Plan plan_launch(const bbkde_ctx *c, int64_t n_ref, int64_t q_count, int q_per_b
   p.gx = (unsigned)std::max<int64_t>(qtiles, 1);
   int64_t target = (int64_t)c->sm_count * 4 * 16;
   int64_t want = (target + qtiles - 1) / std::max<int64_t>(qtiles, 1);
-  int64_t max_seg = std::max<int64_t>(1, (n_ref + 511) / 512);
+  int64_t max_seg = std::max<int64_t>(1, (n_ref + tile - 1) / tile);
   p.nseg = std::min<int64_t>(std::max<int64_t>(want, 1), std::min<int64_t>(max_seg, 65535));
   p.seg_len = (n_ref + p.nseg - 1) / p.nseg;
   p.seg_len = (p.seg_len + tile - 1) / tile * tile;
