@@ -26,7 +26,7 @@ def test_adapt_density_matches_golden(ctx, oracle, name, precision):
     abw, mass, pilot, gm = ctx.adapt_density(desc, 0.5, precision)
     pa, pb = match_by_coords(refs, g["tree_xy"].reshape(-1, dim))
     # FP32C: the pilot sums are FP32-compensated (~1e-7), g and the attributes
-    # FP64, so abw and mass hold north_star's 1e-6 relative bar.
+    # FP64, so abw and mass hold the 1e-6 relative bar of FP32-compensated sums.
     rtol = 1e-10 if precision == bk.FP64 else 1e-6
     np.testing.assert_allclose(abw[pa], g["tree_abw"][pb], rtol=rtol)
     np.testing.assert_allclose(mass[pa], g["tree_mass"][pb], rtol=rtol * 2)
