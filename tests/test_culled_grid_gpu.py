@@ -277,6 +277,24 @@ def test_grid_exact_split_tiles(ctx, tiles_per_axis):
     assert np.array_equal(got, again)
 
 
+@pytest.mark.parametrize("grid,tile", [((100, 70, -3.0, 2.5, -2.0, 3.0), 16),   # 35 ragged tiles: 8 parts
+                                       ((700, 690, -4.0, 4.0, -4.0, 4.0), 16),   # 1,936 tiles: cost order
+                                       ((1000, 990, -4.0, 4.0, -4.0, 4.0), 32)])  # 1,024 tiles: cost order
+def test_grid_exact_ragged_split_and_ordered(ctx, grid, tile):
+    """Ragged grids (edges that cut tiles) through the two launch forms that long
+    and short tile lists take: clusters of parts per tile (short lists) and the
+    most-expensive-first launch order (lists longer than one wave); both match
+    the direct sum at every point, keep the bound and repeat bitwise."""
+    desc = _setup_adaptive(ctx)
+    want = _direct_on_grid(ctx, desc, grid)
+    got, st = _grid_eval(ctx, desc, grid, mode=bk.GRID_EXACT, tile=tile)
+    assert_parity(got, want, 1e-6 + 1e-7, 1e-8, what=f"grid {grid[:2]} tile {tile}")
+    assert st.max_bound_ratio <= 1e-7
+    assert st.exact_points == grid[0] * grid[1]
+    again, _ = _grid_eval(ctx, desc, grid, mode=bk.GRID_EXACT, tile=tile)
+    assert np.array_equal(got, again)
+
+
 @pytest.mark.parametrize("kind,h", [(W.GAUSS_PROD2D, (0.05, 0.09)), (W.EPAN_PROD2D, (0.2, 0.15)),
                                     (W.EPAN, (0.2, 0.2))])
 def test_grid_exact_factored_and_pair_forms(ctx, kind, h):
