@@ -80,7 +80,7 @@ class GridConfig(C.Structure):
     _fields_ = [("mode", C.c_int), ("tile", C.c_int), ("probes", C.c_int),
                 ("exact_culled", C.c_int), ("rel_tol", C.c_double), ("low_frac", C.c_double),
                 ("cull_rel", C.c_double), ("interp", C.c_int), ("pair_form", C.c_int),
-                ("net_scope", C.c_int), ("lattice_tile", C.c_int)]
+                ("net_scope", C.c_int), ("lattice_tile", C.c_int), ("tensor_cores", C.c_int)]
 
 
 class GridStats(C.Structure):
@@ -417,13 +417,13 @@ class Context:
     def eval_grid(self, desc: KernelDesc, grid, out_ptr: int, surrogate=None,
                   mode=GRID_EXACT, tile=16, probes=5, exact_culled=True, rel_tol=5e-4,
                   low_frac=1e-4, cull_rel=1e-7, interp=1, pair_form=False,
-                  net_scope=NET_RESCUE, lattice_tile=0) -> GridStats:
+                  net_scope=NET_RESCUE, lattice_tile=0, tensor_cores=0) -> GridStats:
         """Density on a dense grid into device memory out_ptr (nx * ny doubles).
 
         grid = (nx, ny, x0, x1, y0, y1). Returns the GridStats."""
         g = Grid(*grid)
         cfg = GridConfig(mode, tile, probes, int(exact_culled), rel_tol, low_frac, cull_rel,
-                         interp, int(pair_form), net_scope, lattice_tile)
+                         interp, int(pair_form), net_scope, lattice_tile, tensor_cores)
         st = GridStats()
         sh = surrogate.h if surrogate is not None else None
         self._check(self.lib.bbkde_eval_grid(self.h, sh, C.byref(desc), C.byref(g), C.byref(cfg),

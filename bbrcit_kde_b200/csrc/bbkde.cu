@@ -29,6 +29,7 @@
 #include "kde_cv_batch.cuh"
 #include "kde_culled.cuh"
 #include "kde_culled_sep.cuh"
+#include "kde_culled_sep_tc.cuh"
 #include "kde_grid.cuh"
 
 using namespace bbkde;
@@ -1532,10 +1533,24 @@ cudaError_t launch_cull_sep_split(unsigned nblk, cudaStream_t st, const CullArgs
   return cudaLaunchKernelEx(&cfg, k_pair_sum_culled_sep<OP, 16, S>, a);
 }
 
+// Tensor-core form of the tile-32 factored sum: the dynamic shared memory it
+// requests (beyond its static arrays) keeps four blocks per SM, which together
+// hold all 512 tensor-memory columns.
+template <int OP>
+cudaError_t launch_cull_sep_tc(unsigned nblk, cudaStream_t st, const CullArgs &a) {
+  static const cudaError_t attr = cudaFuncSetAttribute(
+      k_pair_sum_culled_sep_tc<OP>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSepTcPadBytes);
+  if (attr != cudaSuccess) return attr;
+  k_pair_sum_culled_sep_tc<OP><<<nblk, kSepTcThreads, kSepTcPadBytes, st>>>(a);
+  return cudaGetLastError();
+}
+
 // parts = 1: one block per tile; 2, 4, 8 (tile 16 only): clusters of that many.
+// tc: tile 32 on the tensor cores (k_pair_sum_culled_sep_tc).
 template <int OP>
 cudaError_t launch_cull_sep(int tile, int parts, unsigned nblk, cudaStream_t st,
-                            const CullArgs &a) {
+                            const CullArgs &a, bool tc = false) {
+  if (tile == 32 && tc) return launch_cull_sep_tc<OP>(nblk, st, a);
   if (tile == 32) {
     k_pair_sum_culled_sep<OP, 32><<<nblk, 32 * 32 / 8, 0, st>>>(a);
     return cudaGetLastError();
@@ -1595,14 +1610,16 @@ int sep_parts(const bbkde_ctx *c, int tile, unsigned nblk) {
 // abs_n > 0 adds an absolute allowance (unnormalised units): a query's skipped
 // part stays below max(rel * S, abs_n) / 2, and *ratio is then the worst skipped
 // bound over that allowance; with abs_n = 0 it is the worst bound over S.
+// sep_tc: a tile-32 factored sum runs on the tensor cores (k_pair_sum_culled_sep_tc).
 int launch_culled(bbkde_ctx *c, const Resolved &r, int shape, unsigned nblk,
                   const CullQueries &q, double rel, bool full, double *pairs, double *ratio,
-                  int sep_tile = 0, double abs_n = 0.0) {
+                  int sep_tile = 0, double abs_n = 0.0, bool sep_tc = false) {
   if (nblk == 0) return BBKDE_OK;
   TRY(ensure(c, c->cb_bound, (size_t)nblk * sizeof(double)));
   TRY(ensure(c, c->cb_smin, (size_t)nblk * sizeof(double)));
   TRY(ensure(c, c->cb_tiles, (size_t)nblk * sizeof(int)));
-  TRY(ensure(c, c->cb_stats, 2 * sizeof(double)));
+  TRY(ensure(c, c->cb_stats, 3 * sizeof(double)));   // [2]: status word of the launch
+  const bool tc = sep_tc && sep_tile == 32;
   CullArgs a;
   a.refs = c->cull.rec.as<float4>();
   a.extra = c->cull.ext.as<float>();
@@ -1618,6 +1635,8 @@ int launch_culled(bbkde_ctx *c, const Resolved &r, int shape, unsigned nblk,
   a.blk_bound = c->cb_bound.as<double>();
   a.blk_smin = c->cb_smin.as<double>();
   a.blk_tiles = c->cb_tiles.as<int>();
+  a.status = reinterpret_cast<int *>(c->cb_stats.as<double>() + 2);
+  if (tc) CUDA_TRY(c, cudaMemsetAsync(a.status, 0, sizeof(int), c->stream));
   const bool d2 = r.dim == 2;
   if (sep_tile > 0) {
     const int parts = sep_parts(c, sep_tile, nblk);
@@ -1633,13 +1652,13 @@ int launch_culled(bbkde_ctx *c, const Resolved &r, int shape, unsigned nblk,
     }
     switch (r.op) {
       case OP_GAUSS_ISO:
-        CUDA_TRY(c, launch_cull_sep<OP_GAUSS_ISO>(sep_tile, parts, nblk, c->stream, a));
+        CUDA_TRY(c, launch_cull_sep<OP_GAUSS_ISO>(sep_tile, parts, nblk, c->stream, a, tc));
         break;
       case OP_GAUSS_PROD:
-        CUDA_TRY(c, launch_cull_sep<OP_GAUSS_PROD>(sep_tile, parts, nblk, c->stream, a));
+        CUDA_TRY(c, launch_cull_sep<OP_GAUSS_PROD>(sep_tile, parts, nblk, c->stream, a, tc));
         break;
       case OP_EPAN_PROD:
-        CUDA_TRY(c, launch_cull_sep<OP_EPAN_PROD>(sep_tile, parts, nblk, c->stream, a));
+        CUDA_TRY(c, launch_cull_sep<OP_EPAN_PROD>(sep_tile, parts, nblk, c->stream, a, tc));
         break;
       default: return fail(c, BBKDE_UNSUPPORTED, "culled sum: kernel does not factor");
     }
@@ -1661,9 +1680,17 @@ int launch_culled(bbkde_ctx *c, const Resolved &r, int shape, unsigned nblk,
                                          c->cb_stats.as<double>());
   COUNT_LAUNCH(c);
   CUDA_TRY(c, cudaGetLastError());
-  double st[2];
-  CUDA_TRY(c, cudaMemcpyAsync(st, c->cb_stats.p, sizeof(st), cudaMemcpyDeviceToHost, c->stream));
+  double st[3];
+  CUDA_TRY(c, cudaMemcpyAsync(st, c->cb_stats.p, (tc ? 3 : 2) * sizeof(double),
+                              cudaMemcpyDeviceToHost, c->stream));
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  if (tc) {
+    int status = 0;
+    std::memcpy(&status, &st[2], sizeof(int));
+    if (status != 0)
+      return fail(c, BBKDE_CUDA_ERROR,
+                  "culled sum: a tensor-core wait expired (the results are not written)");
+  }
   if (pairs) *pairs += st[1] * kRefTile * kCullQpb[shape];
   if (ratio) *ratio = std::max(*ratio, abs_n > 0.0 ? st[0] : st[0] * rel);
   return BBKDE_OK;
@@ -1998,9 +2025,12 @@ GridDesc make_grid(int64_t nx, int64_t ny, double x0, double dx, double y0, doub
 
 // Exact sums at the points of every listed tile of g (results row-major into out),
 // in the factored form where the kernel factors over the axes unless pair_form.
+// tensor_cores (bbkde_grid_config.tensor_cores): 0 = tile-32 factored sums on the
+// tensor cores when rel >= kSepTcMinRel (culled) and the list is long (at least
+// kSepTcMinWaves waves of resident blocks), 1 = never, 2 = always.
 int grid_exact(bbkde_ctx *c, const Resolved &r, const GridDesc &g, const int *list, int64_t n,
                double rel, bool full, double *out, double *pairs, double *ratio,
-               bool pair_form = false) {
+               bool pair_form = false, int tensor_cores = 1) {
   CullQueries q = {};
   q.mode = 1;
   q.tile_list = list;
@@ -2016,7 +2046,11 @@ int grid_exact(bbkde_ctx *c, const Resolved &r, const GridDesc &g, const int *li
   q.scale = r.norm;
   const int shape = g.tile == 32 ? 0 : 1;
   const int sep = (!pair_form && r.dim == 2 && op_separable(r.op)) ? g.tile : 0;
-  return launch_culled(c, r, shape, (unsigned)n, q, rel, full, pairs, ratio, sep);
+  const bool tc =
+      sep == 32 && (tensor_cores == 2 ||
+                    (tensor_cores == 0 && !full && rel >= kSepTcMinRel &&
+                     n >= (int64_t)kSepTcMinWaves * kSepTcResident * c->sm_count));
+  return launch_culled(c, r, shape, (unsigned)n, q, rel, full, pairs, ratio, sep, 0.0, tc);
 }
 
 }  // namespace
@@ -2040,6 +2074,8 @@ extern "C" int bbkde_eval_grid(bbkde_ctx *c, bbkde_surrogate *sur, const bbkde_k
   int LT = cfg->lattice_tile;
   if (LT != 0 && LT != 16 && LT != 32)
     return fail(c, BBKDE_INVALID_ARGUMENT, "grid: lattice_tile must be 0, 16 or 32");
+  if (cfg->tensor_cores < 0 || cfg->tensor_cores > 2)
+    return fail(c, BBKDE_INVALID_ARGUMENT, "grid: tensor_cores must be 0, 1 or 2");
   const int interp = cfg->interp == 0 ? 1 : cfg->interp;
   if (interp != 1 && interp != 3)
     return fail(c, BBKDE_INVALID_ARGUMENT, "grid: interp must be 1 (bilinear) or 3 (bicubic)");
@@ -2168,7 +2204,7 @@ extern "C" int bbkde_eval_grid(bbkde_ctx *c, bbkde_surrogate *sur, const bbkde_k
     TRY(tile_order(c, gl, c->gr_lat_order));
     TRY(grid_exact(c, r, gl, c->gr_lat_order.as<int>(), (int64_t)gl.ntx * gl.nty,
                    cfg->cull_rel, full, c->gr_lat_exact.as<double>(), &st.pairs,
-                   &st.max_bound_ratio, cfg->pair_form != 0));
+                   &st.max_bound_ratio, cfg->pair_form != 0, cfg->tensor_cores));
     auto lattice_net = [&]() -> int {
       TRY(ensure(c, c->gr_lat_net, (size_t)n_lat * sizeof(float)));
       TRY(bbkde::surrogate_infer(sur, c->stream, n_lat, nullptr, gl.nx, gl.x0, gl.dx, gl.y0,
@@ -2201,7 +2237,7 @@ extern "C" int bbkde_eval_grid(bbkde_ctx *c, bbkde_surrogate *sur, const bbkde_k
       TRY(tile_order(c, gq, c->gr_q_order));
       TRY(grid_exact(c, r, gq, c->gr_q_order.as<int>(), (int64_t)gq.ntx * gq.nty, cfg->cull_rel,
                      full, c->gr_q_exact.as<double>(), &st.pairs, &st.max_bound_ratio,
-                     cfg->pair_form != 0));
+                     cfg->pair_form != 0, cfg->tensor_cores));
       if (net_all) {
         TRY(quarter_net());
         q_net = c->gr_q_net.as<float>();
@@ -2364,7 +2400,7 @@ extern "C" int bbkde_eval_grid(bbkde_ctx *c, bbkde_surrogate *sur, const bbkde_k
                               c->stream));
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   TRY(grid_exact(c, r, g, c->gr_list.as<int>(), nsel, cfg->cull_rel, full, out, &st.pairs,
-                 &st.max_bound_ratio, cfg->pair_form != 0));
+                 &st.max_bound_ratio, cfg->pair_form != 0, cfg->tensor_cores));
   CUDA_TRY(c, cudaEventRecord(c->ev3, c->stream));
   // Points in the flagged tiles (edge tiles may be partial).
   std::vector<int> flags((size_t)ntiles);

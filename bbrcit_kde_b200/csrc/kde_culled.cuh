@@ -93,6 +93,7 @@ struct CullArgs {
   double *blk_bound;      // per block: worst (skipped bound / slot allowance A_k)
   double *blk_smin;       // per block: smallest unnormalised sum of its queries
   int *blk_tiles;         // per block: reference tiles summed
+  int *status;            // tensor-core form: set to 1 if a wait expired (or null)
 };
 
 __device__ __forceinline__ float grid_coord(double x0, double dx, int64_t i) {

@@ -27,6 +27,7 @@
 #include <cuda_runtime.h>
 
 #include "mlp.cuh"
+#include "tc_util.cuh"
 
 namespace bbkde {
 namespace mlp {
@@ -40,7 +41,6 @@ constexpr uint32_t kTcMatBytes = 128 * 128 * 2;   // one 128 x 128 BF16 operand
 // (bits 24..28: M / 16); c_format F32 = 1 at bit 4, a/b_format BF16 = 1 at bits 7, 10.
 constexpr uint32_t kTcIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((128u >> 3) << 17) |
                               ((128u >> 4) << 24);
-constexpr long long kTcWaitLimit = 1ll << 26;   // try_wait polls before giving up
 
 template <bool kSplit>
 struct TcSmem {
@@ -57,10 +57,6 @@ struct TcSmem {
 
 __device__ __forceinline__ uint32_t tc_off(int r, int k) {
   return (uint32_t)((k >> 3) * 2048 + (r >> 3) * 128 + (r & 7) * 16 + (k & 7) * 2);
-}
-
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
 }
 
 // Shared-memory matrix descriptor: K-major, no swizzle, LBO 2048 B, SBO 128 B,
@@ -95,12 +91,6 @@ __device__ __forceinline__ void tc_mma(uint32_t tmem_d, uint64_t adesc, uint64_t
       : "r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(zero));
 }
 
-__device__ __forceinline__ void tc_commit(uint32_t mbar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
-               ::"r"(mbar)
-               : "memory");
-}
-
 // D (+)= A x B over K = 128 (8 instructions of K = 16), M = N = 128. A and B are
 // stored 128 x 128 BF16 matrices at tc_off; a_mn / b_mn read them transposed.
 __device__ __forceinline__ void tc_gemm128(uint32_t tmem_d, uint32_t a, bool a_mn, uint32_t b,
@@ -114,31 +104,6 @@ __device__ __forceinline__ void tc_gemm128(uint32_t tmem_d, uint32_t a, bool a_m
   }
 }
 
-// Bounded wait for the mbarrier phase `parity` to complete; false on expiry.
-__device__ __forceinline__ bool tc_wait(uint32_t mbar, uint32_t parity) {
-  for (long long i = 0; i < kTcWaitLimit; ++i) {
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}\n"
-        : "=r"(done)
-        : "r"(mbar), "r"(parity)
-        : "memory");
-    if (done) return true;
-  }
-  return false;
-}
-
-__device__ __forceinline__ void tc_fence_after() {
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-}
-__device__ __forceinline__ void tc_fence_before() {
-  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-}
-__device__ __forceinline__ void fence_async_smem() {
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
 __device__ __forceinline__ void wg_sync(int wg) {
   asm volatile("bar.sync %0, 128;" ::"r"(1 + wg) : "memory");
 }
@@ -331,7 +296,6 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_mlp_infer_tc(TcArgs ta) {
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
                  "r"(kTcTmemCols));
 }
-
 
 // ===========================================================================
 // Training step on tcgen05: forward and backward of 128 points per CTA.

@@ -608,6 +608,12 @@ def run_surrogate_grid(a, world, rank, local):
     comp = {}
     for name, kw in [("culled_exact", dict(mode=bk.GRID_EXACT, tile=16)),
                      ("culled_exact_tile32", dict(mode=bk.GRID_EXACT, tile=32)),
+                     # the whole grid at the pipeline's exact-part tolerance, tile 32,
+                     # accumulation on the FP32 pipe and on the tcgen05 tensor cores
+                     ("culled_exact_tile32_1e-5_fp32_pipe",
+                      dict(mode=bk.GRID_EXACT, tile=32, cull_rel=1e-5, tensor_cores=1)),
+                     ("culled_exact_tile32_1e-5_tensor_cores",
+                      dict(mode=bk.GRID_EXACT, tile=32, cull_rel=1e-5, tensor_cores=2)),
                      ("culled_exact_pair_form", dict(mode=bk.GRID_EXACT, tile=16,
                                                      pair_form=True)),
                      ("network_pair_form", dict(main_cfg, pair_form=True)),
