@@ -617,6 +617,7 @@ def run_surrogate_grid(a, world, rank, local):
                      ("culled_exact_pair_form", dict(mode=bk.GRID_EXACT, tile=16,
                                                      pair_form=True)),
                      ("network_pair_form", dict(main_cfg, pair_form=True)),
+                     ("network_tensor_cores", dict(main_cfg, tensor_cores=2)),
                      ("network_everywhere", dict(main_cfg, net_scope=bk.NET_EVERYWHERE)),
                      ("anchored_without_network", dict(main_cfg, surrogate=None)),
                      ("network_bilinear", dict(main_cfg, interp=1)),
