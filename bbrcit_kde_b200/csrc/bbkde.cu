@@ -1535,10 +1535,11 @@ cudaError_t launch_cull_sep_split(unsigned nblk, cudaStream_t st, const CullArgs
 
 // Tensor-core form of the tile-32 factored sum: the dynamic shared memory it
 // requests (beyond its static arrays) keeps four blocks per SM, which together
-// hold all 512 tensor-memory columns.
+// hold all 512 tensor-memory columns. The attribute is set on every launch, for
+// the device that is current (function attributes are per device).
 template <int OP>
 cudaError_t launch_cull_sep_tc(unsigned nblk, cudaStream_t st, const CullArgs &a) {
-  static const cudaError_t attr = cudaFuncSetAttribute(
+  const cudaError_t attr = cudaFuncSetAttribute(
       k_pair_sum_culled_sep_tc<OP>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSepTcPadBytes);
   if (attr != cudaSuccess) return attr;
   k_pair_sum_culled_sep_tc<OP><<<nblk, kSepTcThreads, kSepTcPadBytes, st>>>(a);
