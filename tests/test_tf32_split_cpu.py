@@ -1,0 +1,121 @@
+"""Host-side checks of the tensor-core factored grid sum (csrc/kde_culled_sep_tc.cuh).
+
+1. The two-term TF32 split of a kernel factor (veltkamp11 / tf32_split2): with
+   c = 8193 v, hi = c - (c - v) and lo the same split of v - hi. numpy float32
+   arithmetic rounds to nearest like the device's FP32 pipe (the kernel writes
+   a - b as fma(b, -1, a), which rounds once, as a subtraction). Checked: hi and lo
+   carry at most 11 significant bits (exact TF32 operands), and v - hi - lo is at
+   most 2^-22 |v| over factors from 1e-30 to 1e4.
+2. The index mapping between the operand rows and the accumulator fragment: A's
+   row 16 w + 8 p + i holds part p (hi, lo) of tile row 8 w + i, B's row c + 32 p
+   part p of column c; an M = 64 accumulator row m sits in TMEM lane
+   (m / 16) * 32 + m % 16; a tcgen05.ld 16x256b.x8 gives thread t of warp w
+   register 4 j + e = (lane t / 4, column 8 j + 2 (t % 4) + e) and register
+   4 j + 2 + e = (lane 8 + t / 4, the same column) of its warp's lanes. Checked:
+   the four registers the fold adds for each of a thread's 8 points are the four
+   quadrant products of that point's own row and column, and the 128 threads
+   cover the 32 x 32 tile once.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+f32 = np.float32
+
+
+def _veltkamp11(v):
+    c = (v * f32(8193.0)).astype(f32)
+    t = (c - v).astype(f32)
+    return (c - t).astype(f32)
+
+
+def _split(v):
+    hi = _veltkamp11(v)
+    lo = _veltkamp11((v - hi).astype(f32))
+    return hi, lo
+
+
+def _significant_bits(x):
+    """Bits from the leading one to the last one of the float32 significand."""
+    b = x.astype(f32).view(np.uint32)
+    mant = (b & np.uint32(0x7FFFFF)) | np.uint32(0x800000)
+    tz = np.zeros(b.shape, dtype=np.int64)
+    m = mant.astype(np.int64)
+    for _ in range(24):
+        odd = (m & 1) == 1
+        tz = np.where(odd, tz, tz + 1)
+        m = np.where(odd, m, m >> 1)
+    return np.where(x == 0, 0, 24 - tz)
+
+
+def test_tf32_split_terms_are_exact_and_remainder_bounded():
+    rng = np.random.default_rng(7)
+    v = np.concatenate([
+        f32(10.0) ** rng.uniform(-30, 4, 200_000).astype(f32),
+        rng.uniform(0, 1, 100_000).astype(f32),
+        np.array([1.0, 0.5, 2 ** -20, 1 - 2 ** -24, 3.0, 1e-38], dtype=f32),
+    ]).astype(f32)
+    v = v[np.isfinite(v) & (v > 0) & (v >= f32(1e-30))]
+    hi, lo = _split(v)
+    assert _significant_bits(hi).max() <= 11
+    assert _significant_bits(lo[lo != 0]).max() <= 11
+    rest = v.astype(np.float64) - hi.astype(np.float64) - lo.astype(np.float64)
+    assert np.all(np.abs(rest) <= 2.0 ** -22 * v.astype(np.float64))
+    # hi alone would leave up to 2^-12 of v
+    assert np.max(np.abs(v.astype(np.float64) - hi) / v) > 2.0 ** -14
+
+
+def test_quadrant_product_of_split_factors():
+    """Y X^T from the four quadrants of [Y_hi; Y_lo] [X_hi; X_lo]^T against FP64 of
+    the FP32 factors, with exact (FP64) products: what is left is the split."""
+    rng = np.random.default_rng(11)
+    y = (2.0 ** rng.uniform(-20, 0, (32, 32))).astype(f32)
+    x = (2.0 ** rng.uniform(-20, 0, (32, 32))).astype(f32)
+    yh, yl = _split(y)
+    xh, xl = _split(x)
+    a = np.concatenate([yh, yl]).astype(np.float64)
+    b = np.concatenate([xh, xl]).astype(np.float64)
+    d = a @ b.T
+    got = d[32:, :32] + d[:32, 32:] + d[32:, 32:] + d[:32, :32]
+    want = y.astype(np.float64) @ x.astype(np.float64).T
+    assert np.max(np.abs(got - want) / want) <= 2.0 ** -21
+
+
+def test_operand_rows_and_fragment_give_each_point_its_quadrants():
+    # accumulator entry (m, n) tagged by the product it holds
+    def a_row(tile_row, part):
+        return 16 * (tile_row // 8) + 8 * part + tile_row % 8
+
+    tag = {}
+    for r in range(32):
+        for p in range(2):
+            for c in range(32):
+                for q in range(2):
+                    tag[(a_row(r, p), c + 32 * q)] = (r, c, p, q)
+    assert len(tag) == 64 * 64
+    lane_of_row = {m: (m // 16) * 32 + m % 16 for m in range(64)}
+    row_of_lane = {ln: m for m, ln in lane_of_row.items()}
+    covered = np.zeros((32, 32), dtype=int)
+    for warp in range(4):
+        for t in range(32):
+            regs = {}
+            for j in range(8):
+                for e in range(2):
+                    col = 8 * j + 2 * (t % 4) + e
+                    regs[4 * j + e] = (warp * 32 + t // 4, col)
+                    regs[4 * j + 2 + e] = (warp * 32 + 8 + t // 4, col)
+            prow = 8 * warp + t // 4
+            for k in range(8):
+                j, e = k // 2, k % 2
+                pcol = 8 * j + 2 * (t % 4) + e
+                # the fold adds registers 4j+2+e, 4(j+4)+e, 4(j+4)+2+e, 4j+e
+                want = {(1, 0), (0, 1), (1, 1), (0, 0)}
+                got = set()
+                for rg in (4 * j + 2 + e, 4 * (j + 4) + e, 4 * (j + 4) + 2 + e, 4 * j + e):
+                    lane, col = regs[rg]
+                    r, c, p, q = tag[(row_of_lane[lane], col)]
+                    assert (r, c) == (prow, pcol)
+                    got.add((p, q))
+                assert got == want
+                covered[prow, pcol] += 1
+    assert np.all(covered == 1)
