@@ -9,7 +9,8 @@
 // product per reference tile, which the FFMA form feeds from shared memory at 2
 // bytes of loads per multiply-add. Here it is a tcgen05.mma chain instead:
 //   * each FP32 factor v is split into two TF32 terms, hi = v rounded to TF32
-//     and lo = v - hi rounded to TF32 (hi + lo carries 22 of v's 24 bits), and one
+//     and lo = v - hi, of which the tensor core reads the leading 11 bits (hi +
+//     lo carries 21 or more of v's 24 bits), and one
 //     kind::tf32 MMA of M = 64, N = 64, K = 8 multiplies A = [Y_hi; Y_lo] (rows)
 //     by B = [X_hi; X_lo] (columns), so its four 32 x 32 quadrants are the four
 //     cross products; a point's value is the sum of its four quadrant entries,
@@ -30,7 +31,7 @@
 // thread both parts of its row: thread t of warp w owns tile row 8 w + t / 4 and
 // columns 8 j + 2 (t % 4) + e (j < 4, e < 2).
 //
-// Accuracy: the split leaves at most 2^-22 of each factor; the MMA chain's FP32
+// Accuracy: the split leaves less than 2^-21 of each factor; the MMA chain's FP32
 // accumulation over 32 references was measured at up to 6e-7 relative (mean 2e-7)
 // against FP64 of the same FP32 factors. The host uses this kernel only for sums
 // whose tolerance is at least kSepTcMinRel.
@@ -49,10 +50,10 @@ namespace bbkde {
 
 constexpr double kSepTcMinRel = 1e-5;   // smallest tolerance the tensor-core form serves
 // Resident blocks per SM (all 512 tensor-memory columns), and the list length in
-// waves of them from which the automatic setting takes the tensor cores: a block
-// runs fewer pairs per clock than a block of the FP32-pipe form but the SM more
-// (measured on the 8192^2 grid of 4M references at 1e-5: 65,536 tiles 17.5 vs 16.1
-// Tpair/s; the 1025^2 lattice, 1,089 tiles in 1.8 waves: 7.5 vs 6.8 ms).
+// waves of them from which the automatic setting takes the tensor cores
+// (measured on the 8192^2 grid of 4M references at 1e-5: 65,536 tiles 19.2 vs 16.1
+// Tpair/s; on the 1025^2 lattice of that grid's pipeline, 1,089 tiles in 1.8
+// waves, the two forms are level: pipeline 8.25 vs 8.33 ms).
 constexpr int kSepTcResident = 4;
 constexpr int kSepTcMinWaves = 16;
 constexpr int kSepTcThreads = 128;
@@ -90,18 +91,18 @@ __device__ __forceinline__ void sep_tc_mma(uint32_t tmem_d, uint64_t adesc, uint
 }
 
 // Veltkamp split at 11 significant bits (TF32's 10 explicit + the implicit one):
-// with c = (2^13 + 1) v, c - (c - v) is v rounded to 11 bits, and v minus it is
-// exact. Applied twice, v = hi + lo + d with hi, lo exact TF32 values and |d| <=
-// 2^-22 |v|. All on the FP32 pipe, two lanes per packed instruction (a
-// conversion instruction per term would run at the conversion rate, a quarter
-// of MUFU's). a - b is written fma(b, -1, a): exact negation, one rounding.
-__device__ __forceinline__ float2 veltkamp11(float2 v) {
-  const float2 c = __fmul2_rn(v, f2(8193.0f));
-  return __ffma2_rn(__ffma2_rn(v, f2(-1.0f), c), f2(-1.0f), c);
-}
+// with c = (2^13 + 1) v, hi = c - (c - v) is v rounded to 11 bits, an exact TF32
+// value, and lo = v - hi is exact in FP32 (at most 13 significant bits, |lo| <=
+// 2^-11 |v|). The tensor core reads lo's leading 11 bits (a TF32 operand takes
+// an FP32 word's sign, exponent and top 10 mantissa bits), so v = hi + lo' + d
+// with |d| < 2^-10 |lo| <= 2^-21 |v|. All on the FP32 pipe, two lanes per packed
+// instruction (a conversion instruction per term would run at the conversion
+// rate, a quarter of MUFU's). a - b is written fma(b, -1, a): exact negation,
+// one rounding.
 __device__ __forceinline__ void tf32_split2(float2 v, float2 &hi, float2 &lo) {
-  hi = veltkamp11(v);
-  lo = veltkamp11(__ffma2_rn(hi, f2(-1.0f), v));
+  const float2 c = __fmul2_rn(v, f2(8193.0f));
+  hi = __ffma2_rn(__ffma2_rn(v, f2(-1.0f), c), f2(-1.0f), c);
+  lo = __ffma2_rn(hi, f2(-1.0f), v);
 }
 
 // 16 lanes x 64 columns of FP32 from tensor memory: r[4 j + e] = (lane t / 4,
@@ -205,9 +206,9 @@ __global__ void __launch_bounds__(kSepTcThreads, 4) k_pair_sum_culled_sep_tc(Cul
   // (point k = 2 j + e), with Kahan accumulators.
   const int prow = 8 * warp + (lane >> 2);
   auto pcol = [&](int k) { return 8 * (k >> 1) + 2 * (lane & 3) + (k & 1); };
-  float sum[8], comp[8];
+  float2 sum[4], comp[4];   // points (2 j, 2 j + 1) per pair
 #pragma unroll
-  for (int k = 0; k < 8; ++k) { sum[k] = 0.f; comp[k] = 0.f; }
+  for (int j = 0; j < 4; ++j) { sum[j] = f2(0.f); comp[j] = f2(0.f); }
   auto valid = [&](int k) { return i0 + pcol(k) < q.gnx && j0 + prow < q.gny; };
 
   // This thread's factors: references 4 kg .. 4 kg + 3 of a sub-chunk, of the
@@ -313,19 +314,21 @@ __global__ void __launch_bounds__(kSepTcThreads, 4) k_pair_sum_culled_sep_tc(Cul
   auto fold = [&](int b) {
     float v[32];
     sep_tc_ld(tmem + (uint32_t)(b * 64) + ((uint32_t)(warp * 32) << 16), v);
+    const float2 m1 = f2(-1.0f);
 #pragma unroll
-    for (int j = 0; j < 4; ++j)
-#pragma unroll
-      for (int e = 0; e < 2; ++e) {
-        const int k = 2 * j + e;
-        const float x = __fadd_rn(__fadd_rn(__fadd_rn(v[4 * j + 2 + e], v[4 * (j + 4) + e]),
-                                            v[4 * (j + 4) + 2 + e]),
-                                  v[4 * j + e]);
-        const float y = __fsub_rn(x, comp[k]);
-        const float s = __fadd_rn(sum[k], y);
-        comp[k] = __fsub_rn(__fsub_rn(s, sum[k]), y);
-        sum[k] = s;
-      }
+    for (int j = 0; j < 4; ++j) {
+      // quadrants of points (2 j, 2 j + 1): lo.hi, hi.lo, lo.lo first, then hi.hi
+      const float2 hh = make_float2(v[4 * j], v[4 * j + 1]);
+      const float2 lh = make_float2(v[4 * j + 2], v[4 * j + 3]);
+      const float2 hl = make_float2(v[4 * (j + 4)], v[4 * (j + 4) + 1]);
+      const float2 ll = make_float2(v[4 * (j + 4) + 2], v[4 * (j + 4) + 3]);
+      const float2 x = __fadd2_rn(__fadd2_rn(__fadd2_rn(lh, hl), ll), hh);
+      // Kahan, a - b as fma(b, -1, a): exact negation, one rounding
+      const float2 y = __ffma2_rn(comp[j], m1, x);
+      const float2 t2 = __fadd2_rn(sum[j], y);
+      comp[j] = __ffma2_rn(y, m1, __ffma2_rn(sum[j], m1, t2));
+      sum[j] = t2;
+    }
   };
 
   // Wait for group g and fold it.
@@ -409,7 +412,9 @@ __global__ void __launch_bounds__(kSepTcThreads, 4) k_pair_sum_culled_sep_tc(Cul
     drain();
   };
 
-  auto point_sum = [&](int k) { return sum[k] - comp[k]; };
+  auto point_sum = [&](int k) {
+    return (k & 1) ? sum[k >> 1].y - comp[k >> 1].y : sum[k >> 1].x - comp[k >> 1].x;
+  };
   double smin_all = 0.0, ratio = 0.0;
   if (kGauss) {
     pass(1);   // near field
@@ -466,7 +471,8 @@ __global__ void __launch_bounds__(kSepTcThreads, 4) k_pair_sum_culled_sep_tc(Cul
     for (int k = 0; k < 8; ++k) {
       if (!valid(k)) continue;
       q.out[(j0 + prow) * q.gnx + (i0 + pcol(k))] =
-          q.scale * ((double)sum[k] - (double)comp[k]);
+          q.scale * ((k & 1) ? (double)sum[k >> 1].y - (double)comp[k >> 1].y
+                             : (double)sum[k >> 1].x - (double)comp[k >> 1].x);
     }
   }
   // Every issued group has been waited for; after an expired wait, wait (bounded)

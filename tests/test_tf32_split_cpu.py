@@ -1,11 +1,13 @@
 """Host-side checks of the tensor-core factored grid sum (csrc/kde_culled_sep_tc.cuh).
 
-1. The two-term TF32 split of a kernel factor (veltkamp11 / tf32_split2): with
-   c = 8193 v, hi = c - (c - v) and lo the same split of v - hi. numpy float32
-   arithmetic rounds to nearest like the device's FP32 pipe (the kernel writes
-   a - b as fma(b, -1, a), which rounds once, as a subtraction). Checked: hi and lo
-   carry at most 11 significant bits (exact TF32 operands), and v - hi - lo is at
-   most 2^-22 |v| over factors from 1e-30 to 1e4.
+1. The two-term TF32 split of a kernel factor (tf32_split2): with c = 8193 v,
+   hi = c - (c - v) and lo = v - hi. numpy float32 arithmetic rounds to nearest
+   like the device's FP32 pipe (the kernel writes a - b as fma(b, -1, a), which
+   rounds once, as a subtraction). The tensor core reads a TF32 operand from an
+   FP32 word's sign, exponent and top 10 mantissa bits, modelled here by clearing
+   the low 13 bits of lo. Checked: hi carries at most 11 significant bits (an
+   exact TF32 operand), lo = v - hi exactly, and v - hi - tf32(lo) is below
+   2^-21 |v| over factors from 1e-30 to 1e4.
 2. The index mapping between the operand rows and the accumulator fragment: A's
    row 16 w + 8 p + i holds part p (hi, lo) of tile row 8 w + i, B's row c + 32 p
    part p of column c; an M = 64 accumulator row m sits in TMEM lane
@@ -29,9 +31,14 @@ def _veltkamp11(v):
     return (c - t).astype(f32)
 
 
+def _tf32_read(x):
+    """What the tensor core takes from an FP32 word: the low 13 bits dropped."""
+    return (x.astype(f32).view(np.uint32) & np.uint32(0xFFFFE000)).view(f32)
+
+
 def _split(v):
     hi = _veltkamp11(v)
-    lo = _veltkamp11((v - hi).astype(f32))
+    lo = (v - hi).astype(f32)
     return hi, lo
 
 
@@ -58,27 +65,30 @@ def test_tf32_split_terms_are_exact_and_remainder_bounded():
     v = v[np.isfinite(v) & (v > 0) & (v >= f32(1e-30))]
     hi, lo = _split(v)
     assert _significant_bits(hi).max() <= 11
-    assert _significant_bits(lo[lo != 0]).max() <= 11
-    rest = v.astype(np.float64) - hi.astype(np.float64) - lo.astype(np.float64)
-    assert np.all(np.abs(rest) <= 2.0 ** -22 * v.astype(np.float64))
-    # hi alone would leave up to 2^-12 of v
+    assert np.array_equal(hi.astype(np.float64) + lo.astype(np.float64), v.astype(np.float64))
+    assert np.all(np.abs(lo.astype(np.float64)) <= 2.0 ** -11 * v.astype(np.float64))
+    rest = v.astype(np.float64) - hi.astype(np.float64) - _tf32_read(lo).astype(np.float64)
+    assert np.all(np.abs(rest) < 2.0 ** -21 * v.astype(np.float64))
+    # hi alone leaves up to 2^-11 of v
     assert np.max(np.abs(v.astype(np.float64) - hi) / v) > 2.0 ** -14
 
 
 def test_quadrant_product_of_split_factors():
-    """Y X^T from the four quadrants of [Y_hi; Y_lo] [X_hi; X_lo]^T against FP64 of
-    the FP32 factors, with exact (FP64) products: what is left is the split."""
+    """Y X^T from the four quadrants of [Y_hi; Y_lo] [X_hi; X_lo]^T, as the tensor
+    core reads the operands, against FP64 of the FP32 factors, with exact (FP64)
+    products: what is left is the split, below 2^-20 of each product."""
     rng = np.random.default_rng(11)
     y = (2.0 ** rng.uniform(-20, 0, (32, 32))).astype(f32)
     x = (2.0 ** rng.uniform(-20, 0, (32, 32))).astype(f32)
     yh, yl = _split(y)
     xh, xl = _split(x)
-    a = np.concatenate([yh, yl]).astype(np.float64)
-    b = np.concatenate([xh, xl]).astype(np.float64)
+    a = _tf32_read(np.concatenate([yh, yl])).astype(np.float64)
+    b = _tf32_read(np.concatenate([xh, xl])).astype(np.float64)
+    assert np.array_equal(_tf32_read(yh), yh)
     d = a @ b.T
     got = d[32:, :32] + d[:32, 32:] + d[32:, 32:] + d[:32, :32]
     want = y.astype(np.float64) @ x.astype(np.float64).T
-    assert np.max(np.abs(got - want) / want) <= 2.0 ** -21
+    assert np.max(np.abs(got - want) / want) <= 2.0 ** -20
 
 
 def test_operand_rows_and_fragment_give_each_point_its_quadrants():
