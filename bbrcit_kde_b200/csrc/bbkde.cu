@@ -1536,22 +1536,31 @@ cudaError_t launch_cull_sep_split(unsigned nblk, cudaStream_t st, const CullArgs
 // Tensor-core form of the tile-32 factored sum: the dynamic shared memory it
 // requests (beyond its static arrays) keeps four blocks per SM, which together
 // hold all 512 tensor-memory columns. The attribute is set on every launch, for
-// the device that is current (function attributes are per device).
-template <int OP>
-cudaError_t launch_cull_sep_tc(unsigned nblk, cudaStream_t st, const CullArgs &a) {
+// the device that is current (function attributes are per device). Lists of at
+// least kSepTcMinWaves waves run 128-thread blocks, shorter ones 256-thread
+// blocks (the same values bitwise).
+template <int OP, int NT>
+cudaError_t launch_cull_sep_tc_nt(unsigned nblk, cudaStream_t st, const CullArgs &a) {
   const cudaError_t attr = cudaFuncSetAttribute(
-      k_pair_sum_culled_sep_tc<OP>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSepTcPadBytes);
+      k_pair_sum_culled_sep_tc<OP, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      kSepTcPadBytes);
   if (attr != cudaSuccess) return attr;
-  k_pair_sum_culled_sep_tc<OP><<<nblk, kSepTcThreads, kSepTcPadBytes, st>>>(a);
+  k_pair_sum_culled_sep_tc<OP, NT><<<nblk, NT, kSepTcPadBytes, st>>>(a);
   return cudaGetLastError();
+}
+template <int OP>
+cudaError_t launch_cull_sep_tc(unsigned nblk, cudaStream_t st, const CullArgs &a,
+                               bool long_list) {
+  return long_list ? launch_cull_sep_tc_nt<OP, kSepTcLongThreads>(nblk, st, a)
+                   : launch_cull_sep_tc_nt<OP, kSepTcShortThreads>(nblk, st, a);
 }
 
 // parts = 1: one block per tile; 2, 4, 8 (tile 16 only): clusters of that many.
 // tc: tile 32 on the tensor cores (k_pair_sum_culled_sep_tc).
 template <int OP>
 cudaError_t launch_cull_sep(int tile, int parts, unsigned nblk, cudaStream_t st,
-                            const CullArgs &a, bool tc = false) {
-  if (tile == 32 && tc) return launch_cull_sep_tc<OP>(nblk, st, a);
+                            const CullArgs &a, bool tc = false, bool long_list = false) {
+  if (tile == 32 && tc) return launch_cull_sep_tc<OP>(nblk, st, a, long_list);
   if (tile == 32) {
     k_pair_sum_culled_sep<OP, 32><<<nblk, 32 * 32 / 8, 0, st>>>(a);
     return cudaGetLastError();
@@ -1621,6 +1630,8 @@ int launch_culled(bbkde_ctx *c, const Resolved &r, int shape, unsigned nblk,
   TRY(ensure(c, c->cb_tiles, (size_t)nblk * sizeof(int)));
   TRY(ensure(c, c->cb_stats, 3 * sizeof(double)));   // [2]: status word of the launch
   const bool tc = sep_tc && sep_tile == 32;
+  const bool tc_long =
+      tc && (int64_t)nblk >= (int64_t)kSepTcMinWaves * kSepTcResident * c->sm_count;
   CullArgs a;
   a.refs = c->cull.rec.as<float4>();
   a.extra = c->cull.ext.as<float>();
@@ -1653,13 +1664,16 @@ int launch_culled(bbkde_ctx *c, const Resolved &r, int shape, unsigned nblk,
     }
     switch (r.op) {
       case OP_GAUSS_ISO:
-        CUDA_TRY(c, launch_cull_sep<OP_GAUSS_ISO>(sep_tile, parts, nblk, c->stream, a, tc));
+        CUDA_TRY(c, launch_cull_sep<OP_GAUSS_ISO>(sep_tile, parts, nblk, c->stream, a, tc,
+                                              tc_long));
         break;
       case OP_GAUSS_PROD:
-        CUDA_TRY(c, launch_cull_sep<OP_GAUSS_PROD>(sep_tile, parts, nblk, c->stream, a, tc));
+        CUDA_TRY(c, launch_cull_sep<OP_GAUSS_PROD>(sep_tile, parts, nblk, c->stream, a, tc,
+                                              tc_long));
         break;
       case OP_EPAN_PROD:
-        CUDA_TRY(c, launch_cull_sep<OP_EPAN_PROD>(sep_tile, parts, nblk, c->stream, a, tc));
+        CUDA_TRY(c, launch_cull_sep<OP_EPAN_PROD>(sep_tile, parts, nblk, c->stream, a, tc,
+                                              tc_long));
         break;
       default: return fail(c, BBKDE_UNSUPPORTED, "culled sum: kernel does not factor");
     }
@@ -2027,8 +2041,7 @@ GridDesc make_grid(int64_t nx, int64_t ny, double x0, double dx, double y0, doub
 // Exact sums at the points of every listed tile of g (results row-major into out),
 // in the factored form where the kernel factors over the axes unless pair_form.
 // tensor_cores (bbkde_grid_config.tensor_cores): 0 = tile-32 factored sums on the
-// tensor cores when rel >= kSepTcMinRel (culled) and the list is long (at least
-// kSepTcMinWaves waves of resident blocks), 1 = never, 2 = always.
+// tensor cores when rel >= kSepTcMinRel (culled), 1 = never, 2 = always.
 int grid_exact(bbkde_ctx *c, const Resolved &r, const GridDesc &g, const int *list, int64_t n,
                double rel, bool full, double *out, double *pairs, double *ratio,
                bool pair_form = false, int tensor_cores = 1) {
@@ -2047,10 +2060,8 @@ int grid_exact(bbkde_ctx *c, const Resolved &r, const GridDesc &g, const int *li
   q.scale = r.norm;
   const int shape = g.tile == 32 ? 0 : 1;
   const int sep = (!pair_form && r.dim == 2 && op_separable(r.op)) ? g.tile : 0;
-  const bool tc =
-      sep == 32 && (tensor_cores == 2 ||
-                    (tensor_cores == 0 && !full && rel >= kSepTcMinRel &&
-                     n >= (int64_t)kSepTcMinWaves * kSepTcResident * c->sm_count));
+  const bool tc = sep == 32 && (tensor_cores == 2 ||
+                                (tensor_cores == 0 && !full && rel >= kSepTcMinRel));
   return launch_culled(c, r, shape, (unsigned)n, q, rel, full, pairs, ratio, sep, 0.0, tc);
 }
 

@@ -25,11 +25,17 @@
 //     16 + (k % 4) * 4), double-buffered in shared memory; two 64-column
 //     accumulators in tensor memory alternate, so that the MMAs of sub-chunk s run
 //     while the block computes the factors of s + 1 and folds s - 1.
-// Row order of A: rows 16 w .. 16 w + 15 land in the TMEM lanes of warp w (the
-// M = 64 data path uses lanes 0-15 of each warp's quarter), and row 16 w + 8 p +
-// i holds part p (hi, lo) of tile row 8 w + i, so that the 16x256b read hands one
-// thread both parts of its row: thread t of warp w owns tile row 8 w + t / 4 and
-// columns 8 j + 2 (t % 4) + e (j < 4, e < 2).
+// Row order of A: rows 16 q .. 16 q + 15 land in TMEM lane quarter q (the M = 64
+// data path uses lanes 0-15 of each quarter), and row 16 q + 8 p + i holds part p
+// (hi, lo) of tile row 8 q + i, so that a 16x256b read hands one thread both parts
+// of its row. Two block shapes, four blocks per SM either way: NT = 128 threads
+// (115 registers), each owning 8 points and making the factors of 4 tile rows or
+// columns per group, or NT = 256 (64 registers), each owning 4 points and making 2.
+// With 256, warps w and w + 4 share lane quarter w % 4 and split the columns.
+// Thread t of warp w owns tile row 8 (w % 4) + t / 4 and columns 8 j + 2 (t % 4) +
+// e, j = PP (w / 4) + j', j' < PP = 512 / NT, e < 2. The shapes compute the same
+// values bitwise; 256 threads hide more latency, which is what a short list of
+// tiles (under ~2 waves) needs, while 128 threads run long lists faster.
 //
 // Accuracy: the split leaves less than 2^-21 of each factor; the MMA chain's FP32
 // accumulation over 32 references was measured at up to 6e-7 relative (mean 2e-7)
@@ -50,13 +56,15 @@ namespace bbkde {
 
 constexpr double kSepTcMinRel = 1e-5;   // smallest tolerance the tensor-core form serves
 // Resident blocks per SM (all 512 tensor-memory columns), and the list length in
-// waves of them from which the automatic setting takes the tensor cores
-// (measured on the 8192^2 grid of 4M references at 1e-5: 65,536 tiles 19.2 vs 16.1
-// Tpair/s; on the 1025^2 lattice of that grid's pipeline, 1,089 tiles in 1.8
-// waves, the two forms are level: pipeline 8.25 vs 8.33 ms).
+// waves of them from which 128-thread blocks are used instead of 256-thread ones
+// (measured on the 8192^2 grid of 4M references at 1e-5: 65,536 tiles 236 ms with
+// 128 threads, 258 ms with 256, 282 ms on the FP32 pipe; on the 1025^2 lattice of
+// that grid's pipeline, 1,089 tiles in 1.8 waves, the pipeline step 8.25 ms with
+// 128 threads, 8.06 ms with 256, 8.27 ms on the FP32 pipe).
 constexpr int kSepTcResident = 4;
 constexpr int kSepTcMinWaves = 16;
-constexpr int kSepTcThreads = 128;
+constexpr int kSepTcLongThreads = 128;   // block shape for long tile lists
+constexpr int kSepTcShortThreads = 256;  // block shape for short ones
 constexpr int kSepTcSub = 32;            // references per accumulator (MMA K)
 constexpr int kSepTcOpBytes = 64 * kSepTcSub * 4;   // one 64-row TF32 operand
 constexpr uint32_t kSepTcTmemCols = 128;            // two 64-column accumulators
@@ -64,9 +72,10 @@ constexpr uint32_t kSepTcTmemCols = 128;            // two 64-column accumulator
 // 24..28: M / 16); c_format F32 = 1 at bit 4, a/b_format TF32 = 2 at bits 7, 10.
 constexpr uint32_t kSepTcIdesc =
     (1u << 4) | (2u << 7) | (2u << 10) | ((64u >> 3) << 17) | ((64u >> 4) << 24);
-// Dynamic shared memory each block requests beyond its static arrays, so that at
-// most four blocks (4 x 128 TMEM columns = all 512) are resident per SM.
-constexpr int kSepTcPadBytes = 12 * 1024;
+// Dynamic shared memory each block requests beyond its static arrays (about 44
+// KB): four blocks (4 x 128 TMEM columns = all 512) fit in an SM's shared memory,
+// a fifth does not.
+constexpr int kSepTcPadBytes = 4 * 1024;
 
 __device__ __forceinline__ uint32_t sep_tc_off(int m, int k) {
   return (uint32_t)((k >> 2) * 1024 + (m >> 3) * 128 + (m & 7) * 16 + (k & 3) * 4);
@@ -105,30 +114,37 @@ __device__ __forceinline__ void tf32_split2(float2 v, float2 &hi, float2 &lo) {
   lo = __ffma2_rn(hi, f2(-1.0f), v);
 }
 
-// 16 lanes x 64 columns of FP32 from tensor memory: r[4 j + e] = (lane t / 4,
-// column 8 j + 2 (t % 4) + e), r[4 j + 2 + e] = (lane 8 + t / 4, the same column).
-__device__ __forceinline__ void sep_tc_ld(uint32_t taddr, float (&v)[32]) {
-  uint32_t r[32];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.16x256b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
-      "%11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, "
-      "%28, %29, %30, %31}, [%32];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
-        "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]),
-        "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
-        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),
-        "=r"(r[31])
-      : "r"(taddr));
+// 16 lanes x 8 X columns: r[4 j + e] = (lane t / 4, column 8 j + 2 (t % 4) + e),
+// r[4 j + 2 + e] = (lane 8 + t / 4, the same column), j < X.
+template <int X>
+__device__ __forceinline__ void sep_tc_ld(uint32_t taddr, float (&v)[4 * X]) {
+  static_assert(X == 2 || X == 4, "16x256b.x2 or .x4");
+  uint32_t r[4 * X];
+  if constexpr (X == 2) {
+    asm volatile("tcgen05.ld.sync.aligned.16x256b.x2.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+                   "=r"(r[6]), "=r"(r[7])
+                 : "r"(taddr));
+  } else {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.16x256b.x4.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+        "%11, %12, %13, %14, %15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+          "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+  }
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+  for (int i = 0; i < 4 * X; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-template <int OP>
-__global__ void __launch_bounds__(kSepTcThreads, 4) k_pair_sum_culled_sep_tc(CullArgs a) {
+template <int OP, int NT>
+__global__ void __launch_bounds__(NT, 4) k_pair_sum_culled_sep_tc(CullArgs a) {
+  static_assert(NT == 128 || NT == 256, "block shape");
   constexpr int T = 32;
-  constexpr int BLOCK = kSepTcThreads;
+  constexpr int BLOCK = NT;
+  constexpr int PP = 512 / NT;                 // point pairs per thread (and factor rows)
   constexpr int NW = BLOCK / 32;
   constexpr int NS = 8;                        // slots: strips of T / 8 rows
   constexpr int SPR = T / NS;                  // rows per slot
@@ -204,25 +220,31 @@ __global__ void __launch_bounds__(kSepTcThreads, 4) k_pair_sum_culled_sep_tc(Cul
 
   // This thread's points: row 8 warp + lane / 4, columns 8 j + 2 (lane % 4) + e
   // (point k = 2 j + e), with Kahan accumulators.
-  const int prow = 8 * warp + (lane >> 2);
-  auto pcol = [&](int k) { return 8 * (k >> 1) + 2 * (lane & 3) + (k & 1); };
-  float2 sum[4], comp[4];   // points (2 j, 2 j + 1) per pair
+  // Warp w reads the TMEM lanes of quarter w % 4 and the column half w / 4: its
+  // thread t owns tile row 8 (w % 4) + t / 4 and the 4 columns 8 j + 2 (t % 4) + e
+  // with j = PP (w / 4) + (k / 2), e = k % 2 (point k < 2 PP).
+  const int lq = warp & 3, ch = warp >> 2;
+  const int prow = 8 * lq + (lane >> 2);
+  auto pcol = [&](int k) { return 8 * (PP * ch + (k >> 1)) + 2 * (lane & 3) + (k & 1); };
+  float2 sum[PP], comp[PP];   // points (2 j', 2 j' + 1) per pair
 #pragma unroll
-  for (int j = 0; j < 4; ++j) { sum[j] = f2(0.f); comp[j] = f2(0.f); }
+  for (int j = 0; j < PP; ++j) { sum[j] = f2(0.f); comp[j] = f2(0.f); }
   auto valid = [&](int k) { return i0 + pcol(k) < q.gnx && j0 + prow < q.gny; };
 
   // This thread's factors: references 4 kg .. 4 kg + 3 of a sub-chunk, of the
-  // tile rows (half 0: A, with the mass) or columns (half 1: B) r8 + 8 i, i < 4.
-  const int kg = tid >> 4, half = (tid >> 3) & 1, r8 = tid & 7;
-  float fq[4];
-  uint32_t o_hi[4], o_lo[4];   // byte offsets in a buffer of the hi and lo rows
+  // tile rows (half 0: A, with the mass) or columns (half 1: B) r8 + 8 i, i = PP rs
+  // + i', i' < PP.
+  const int kg = (tid >> 4) & 7, half = (tid >> 3) & 1, r8 = tid & 7, rs = tid >> 7;
+  float fq[PP];
+  uint32_t o_hi[PP], o_lo[PP];   // byte offsets in a buffer of the hi and lo rows
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    fq[i] = half ? s_qx[r8 + 8 * i] : s_qy[r8 + 8 * i];
+  for (int ii = 0; ii < PP; ++ii) {
+    const int i = PP * rs + ii;
+    fq[ii] = half ? s_qx[r8 + 8 * i] : s_qy[r8 + 8 * i];
     const int mh = half ? r8 + 8 * i : 16 * i + r8;
     const int ml = half ? 32 + r8 + 8 * i : 16 * i + 8 + r8;
-    o_hi[i] = (uint32_t)(half * kSepTcOpBytes) + sep_tc_off(mh, 4 * kg);
-    o_lo[i] = (uint32_t)(half * kSepTcOpBytes) + sep_tc_off(ml, 4 * kg);
+    o_hi[ii] = (uint32_t)(half * kSepTcOpBytes) + sep_tc_off(mh, 4 * kg);
+    o_lo[ii] = (uint32_t)(half * kSepTcOpBytes) + sep_tc_off(ml, 4 * kg);
   }
   const int foff = half ? 0 : STG;
 
@@ -287,7 +309,7 @@ __global__ void __launch_bounds__(kSepTcThreads, 4) k_pair_sum_culled_sep_tc(Cul
     const float2 ma = make_float2(m4.x, m4.y), mb = make_float2(m4.z, m4.w);
     unsigned char *base = &s_op[b][0];
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
+    for (int i = 0; i < PP; ++i) {
       const float2 da = __fadd2_rn(f2(fq[i]), ca), db = __fadd2_rn(f2(fq[i]), cb);
       const float2 dda = __fmul2_rn(da, da), ddb = __fmul2_rn(db, db);
       float2 ua, ub;
@@ -312,16 +334,20 @@ __global__ void __launch_bounds__(kSepTcThreads, 4) k_pair_sum_culled_sep_tc(Cul
 
   // Fold accumulator b (every thread, after its group's wait) into the points.
   auto fold = [&](int b) {
-    float v[32];
-    sep_tc_ld(tmem + (uint32_t)(b * 64) + ((uint32_t)(warp * 32) << 16), v);
+    // columns of X_hi (8 PP ch ..) and of X_lo (32 + 8 PP ch ..) of this warp
+    float v[4 * PP], w[4 * PP];
+    const uint32_t ta =
+        tmem + (uint32_t)(b * 64 + 8 * PP * ch) + ((uint32_t)(lq * 32) << 16);
+    sep_tc_ld<PP>(ta, v);
+    sep_tc_ld<PP>(ta + 32u, w);
     const float2 m1 = f2(-1.0f);
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
+    for (int j = 0; j < PP; ++j) {
       // quadrants of points (2 j, 2 j + 1): lo.hi, hi.lo, lo.lo first, then hi.hi
       const float2 hh = make_float2(v[4 * j], v[4 * j + 1]);
       const float2 lh = make_float2(v[4 * j + 2], v[4 * j + 3]);
-      const float2 hl = make_float2(v[4 * (j + 4)], v[4 * (j + 4) + 1]);
-      const float2 ll = make_float2(v[4 * (j + 4) + 2], v[4 * (j + 4) + 3]);
+      const float2 hl = make_float2(w[4 * j], w[4 * j + 1]);
+      const float2 ll = make_float2(w[4 * j + 2], w[4 * j + 3]);
       const float2 x = __fadd2_rn(__fadd2_rn(__fadd2_rn(lh, hl), ll), hh);
       // Kahan, a - b as fma(b, -1, a): exact negation, one rounding
       const float2 y = __ffma2_rn(comp[j], m1, x);
@@ -421,7 +447,7 @@ __global__ void __launch_bounds__(kSepTcThreads, 4) k_pair_sum_culled_sep_tc(Cul
     if (!failed) {
       float mn = INFINITY;
 #pragma unroll
-      for (int k = 0; k < 8; ++k)
+      for (int k = 0; k < 2 * PP; ++k)
         if (valid(k)) mn = fminf(mn, fmaxf(point_sum(k), 0.f));
       if (mn < INFINITY) atomicMin(&s_min[prow / SPR], __float_as_uint(mn));
     }
@@ -468,7 +494,7 @@ __global__ void __launch_bounds__(kSepTcThreads, 4) k_pair_sum_culled_sep_tc(Cul
   }
   if (!failed) {
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
+    for (int k = 0; k < 2 * PP; ++k) {
       if (!valid(k)) continue;
       q.out[(j0 + prow) * q.gnx + (i0 + pcol(k))] =
           q.scale * ((k & 1) ? (double)sum[k >> 1].y - (double)comp[k >> 1].y

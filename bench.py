@@ -711,19 +711,36 @@ def run_surrogate_grid(a, world, rank, local):
     # T = 16, 256 at T = 32): the FMA pipe is the bound. Pairs at tile granularity
     # of the culled-exact comparator at that tile edge over its device time.
     lt = int(stats[-1]["lattice_tile_used"])
-    ce = results["culled_exact" if lt == 16 else "culled_exact_tile32"]
     peaks = measured_peaks()
     sm_max = float(peaks.get("sm_max_mhz") or clocks.get("sm_max_mhz") or 1965.0)
-    peak = sm_count * FP32_FMA_PER_CLK_PER_SM * sm_max * 1e6
-    ach = ce["pairs"] / (ce["ms_total"] / 1e3)
-    roofline = {"bound": "fp32", "kernel": f"k_pair_sum_culled_sep<GAUSS_ISO,{lt}> "
-                                           "(factored culled exact grid; the pipeline's "
-                                           "lattice launch)",
-                "achieved": ach / 1e9, "peak": peak / 1e9, "unit": "Gpair/s",
-                "frac": ach / peak, "traffic": None,
-                "peak_basis": f"{sm_count} SMs x 128 FP32 FMA/clk x {sm_max:.0f} MHz "
-                              f"(MUFU allows {8 * lt} pairs/clk/SM at tile {lt}); "
-                              "compute-bound, DRAM traffic negligible"}
+    if lt == 32:
+        # At tile 32 the lattice (culled to 1e-5) runs on the tensor cores: the
+        # whole-grid tensor-core comparator measures that kernel; its ceiling is the
+        # factored method's MUFU bound, 2T ex2 per reference and tile = 8T pairs/clk/SM.
+        ce = results["culled_exact_tile32_1e-5_tensor_cores"]
+        peak = sm_count * MUFU_EX2_PER_CLK_PER_SM * (lt / 2) * sm_max * 1e6
+        ach = ce["pairs"] / (ce["ms_total"] / 1e3)
+        roofline = {"bound": "mufu", "kernel": "k_pair_sum_culled_sep_tc<GAUSS_ISO> (factored "
+                                               "culled grid on the tcgen05 tensor cores; the "
+                                               "pipeline's lattice launch)",
+                    "achieved": ach / 1e9, "peak": peak / 1e9, "unit": "Gpair/s",
+                    "frac": ach / peak, "traffic": None,
+                    "peak_basis": f"{sm_count} SMs x 16 MUFU ex2/clk x {lt // 2} pairs per ex2 "
+                                  f"(2T factors per reference on a T x T tile, T = {lt}) x "
+                                  f"{sm_max:.0f} MHz; measured by the whole-grid comparator "
+                                  "at 1e-5; compute-bound, DRAM traffic negligible"}
+    else:
+        ce = results["culled_exact"]
+        peak = sm_count * FP32_FMA_PER_CLK_PER_SM * sm_max * 1e6
+        ach = ce["pairs"] / (ce["ms_total"] / 1e3)
+        roofline = {"bound": "fp32", "kernel": f"k_pair_sum_culled_sep<GAUSS_ISO,{lt}> "
+                                               "(factored culled exact grid; the pipeline's "
+                                               "lattice launch)",
+                    "achieved": ach / 1e9, "peak": peak / 1e9, "unit": "Gpair/s",
+                    "frac": ach / peak, "traffic": None,
+                    "peak_basis": f"{sm_count} SMs x 128 FP32 FMA/clk x {sm_max:.0f} MHz "
+                                  f"(MUFU allows {8 * lt} pairs/clk/SM at tile {lt}); "
+                                  "compute-bound, DRAM traffic negligible"}
     cpu = None
     if rank == 0 and not a.no_cpu_baseline:
         wl = W.Workload("cfg5", W.GAUSS, 2, (0.05, 0.05), refs, w,
@@ -759,7 +776,8 @@ def run_surrogate_grid(a, world, rank, local):
                                f"automatic probe set ({stats[-1]['probes_used']} at this "
                                "spacing) and lattice tile "
                                f"({stats[-1]['lattice_tile_used']}), probe tolerance 5e-4, "
-                               "no low-density cut, exact parts culled to 1e-5; network in "
+                               "no low-density cut, exact parts culled to 1e-5 (tile-32 "
+                               "factored sums on the tcgen05 tensor cores); network in "
                                "rescue mode (two-term BF16 inference on tcgen05 on the tiles "
                                "the interpolated exact anchors miss)",
                    "l2": "flushed between timed steps (256 MB write)"},

@@ -422,9 +422,9 @@ typedef struct {
   int tensor_cores;  /* factored sums on 32 x 32 tiles (lattices, exact tiles): 0 =
                         automatic: on the tcgen05 tensor cores (each factor split into
                         two TF32 terms, up to ~1e-6 relative error against FP64) when
-                        cull_rel >= 1e-5 and the tile list is long (16 waves of four
-                        blocks per SM), else on the FP32 pipe (FP32-compensated);
-                        1 = always the FP32 pipe; 2 = always the tensor cores */
+                        the sums are culled with cull_rel >= 1e-5, else on the FP32
+                        pipe (FP32-compensated); 1 = always the FP32 pipe; 2 = always
+                        the tensor cores */
 } bbkde_grid_config;
 
 enum { BBKDE_NET_RESCUE = 0, BBKDE_NET_EVERYWHERE = 1 };

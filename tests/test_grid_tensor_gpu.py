@@ -79,36 +79,34 @@ def test_tensor_core_tiles_match_direct_and_fp32_pipe(ctx, kind, h):
 
 
 def test_tensor_core_tiles_long_list_and_automatic_choice(ctx):
-    """The automatic setting takes the tensor cores for tile-32 lists of at least
-    16 waves of resident blocks (4 per SM) at tolerances of 1e-5 and above: a
-    ragged 3200 x 3100 grid (9,700 tiles, the most-expensive-first launch order)
-    at 1e-5 runs on them (bitwise the forced result) and matches the direct sum;
-    a 1,024-tile list at 1e-5, and any list at 1e-7, stay on the FP32 pipe
-    (bitwise the forced FP32-pipe result)."""
+    """The automatic setting takes the tensor cores for every culled tile-32 sum at
+    tolerances of 1e-5 and above: 128-thread blocks for lists of at least 16
+    waves (a ragged 3200 x 3100 grid, 9,700 tiles, in the most-expensive-first
+    launch order), 256-thread blocks for shorter ones (a 1,024-tile list). Both
+    are bitwise the forced result and match the direct sum and the FP32-pipe
+    form; at 1e-7 every list stays on the FP32 pipe (bitwise the forced
+    FP32-pipe result)."""
     desc = _adaptive_refs(ctx)
     sms = torch.cuda.get_device_properties(0).multi_processor_count
-    grid = (3200, 3100, -4.0, 4.0, -4.0, 4.0)
-    assert 100 * 97 >= 16 * 4 * sms
-    want = _direct_on_grid(ctx, desc, grid)
-    auto5, st = _grid_eval(ctx, desc, grid, mode=bk.GRID_EXACT, tile=32, cull_rel=1e-5)
-    forced5, _ = _grid_eval(ctx, desc, grid, mode=bk.GRID_EXACT, tile=32, cull_rel=1e-5,
-                            tensor_cores=2)
-    assert np.array_equal(auto5, forced5)
-    assert_parity(auto5, want, 1e-5 + TC_REL, 1e-8, what="9,700 tiles, 1e-5, tensor cores")
-    assert st.max_bound_ratio <= 1e-5
-    fp5, _ = _grid_eval(ctx, desc, grid, mode=bk.GRID_EXACT, tile=32, cull_rel=1e-5,
-                        tensor_cores=1)
-    assert_parity(auto5, fp5, TC_REL, 1e-8, what="9,700 tiles, tensor cores vs FP32 pipe")
-    auto7, _ = _grid_eval(ctx, desc, grid, mode=bk.GRID_EXACT, tile=32, cull_rel=1e-7)
-    fp7, _ = _grid_eval(ctx, desc, grid, mode=bk.GRID_EXACT, tile=32, cull_rel=1e-7,
-                        tensor_cores=1)
-    assert np.array_equal(auto7, fp7)
-    assert_parity(auto7, want, 1e-6 + 1e-7, 1e-8, what="9,700 tiles, 1e-7, FP32 pipe")
-    short = (1000, 990, -4.0, 4.0, -4.0, 4.0)
-    a_short, _ = _grid_eval(ctx, desc, short, mode=bk.GRID_EXACT, tile=32, cull_rel=1e-5)
-    f_short, _ = _grid_eval(ctx, desc, short, mode=bk.GRID_EXACT, tile=32, cull_rel=1e-5,
+    for grid, what in (((3200, 3100, -4.0, 4.0, -4.0, 4.0), "9,700 tiles"),
+                       ((1000, 990, -4.0, 4.0, -4.0, 4.0), "1,024 tiles")):
+        tiles = ((grid[0] + 31) // 32) * ((grid[1] + 31) // 32)
+        assert (tiles >= 16 * 4 * sms) == (tiles == 9700)
+        want = _direct_on_grid(ctx, desc, grid)
+        auto5, st = _grid_eval(ctx, desc, grid, mode=bk.GRID_EXACT, tile=32, cull_rel=1e-5)
+        forced5, _ = _grid_eval(ctx, desc, grid, mode=bk.GRID_EXACT, tile=32, cull_rel=1e-5,
+                                tensor_cores=2)
+        assert np.array_equal(auto5, forced5)
+        assert_parity(auto5, want, 1e-5 + TC_REL, 1e-8, what=f"{what}, 1e-5, tensor cores")
+        assert st.max_bound_ratio <= 1e-5
+        fp5, _ = _grid_eval(ctx, desc, grid, mode=bk.GRID_EXACT, tile=32, cull_rel=1e-5,
                             tensor_cores=1)
-    assert np.array_equal(a_short, f_short)
+        assert_parity(auto5, fp5, TC_REL, 1e-8, what=f"{what}, tensor cores vs FP32 pipe")
+        auto7, _ = _grid_eval(ctx, desc, grid, mode=bk.GRID_EXACT, tile=32, cull_rel=1e-7)
+        fp7, _ = _grid_eval(ctx, desc, grid, mode=bk.GRID_EXACT, tile=32, cull_rel=1e-7,
+                            tensor_cores=1)
+        assert np.array_equal(auto7, fp7)
+        assert_parity(auto7, want, 1e-6 + 1e-7, 1e-8, what=f"{what}, 1e-7, FP32 pipe")
 
 
 def test_tensor_cores_setting_is_checked(ctx):
