@@ -8,15 +8,15 @@
    the low 13 bits of lo. Checked: hi carries at most 11 significant bits (an
    exact TF32 operand), lo = v - hi exactly, and v - hi - tf32(lo) is below
    2^-21 |v| over factors from 1e-30 to 1e4.
-2. The index mappings of the 256-thread block. A's row 16 q + 8 p + i holds part
+2. The index mappings of both block shapes (128 and 256 threads). A's row 16 q + 8 p + i holds part
    p (hi, lo) of tile row 8 q + i, and B's row c + 32 p holds part p of column c.
    An M = 64 accumulator row m sits in TMEM lane (m / 16) * 32 + m % 16. A
    tcgen05.ld 16x256b.x2 at column c0 gives thread t register 4 j + e = (lane
    t / 4, column c0 + 8 j + 2 (t % 4) + e) and register 4 j + 2 + e = (lane 8 +
    t / 4, the same column) of its warp's lane quarter. Warps w and w + 4 share
    quarter w % 4 and read column halves w / 4.
-   Checked: the four registers the fold adds for each of a thread's 4 points are
-   the four quadrant products of that point's own row and column, and the 256
+   Checked: the four registers the fold adds for each of a thread's points are
+   the four quadrant products of that point's own row and column, and the
    threads cover the 32 x 32 tile once. The factor-making threads write every
    (operand row, reference quad) of both operands once, and 128 contiguous bytes
    per 8 lanes.
@@ -24,6 +24,7 @@
 from __future__ import annotations
 
 import numpy as np
+import pytest
 
 f32 = np.float32
 
@@ -94,7 +95,8 @@ def test_quadrant_product_of_split_factors():
     assert np.max(np.abs(got - want) / want) <= 2.0 ** -20
 
 
-def test_operand_rows_and_fragment_give_each_point_its_quadrants():
+@pytest.mark.parametrize("nt", [128, 256])
+def test_operand_rows_and_fragment_give_each_point_its_quadrants(nt):
     # accumulator entry (m, n) tagged by the product it holds
     def a_row(tile_row, part):
         return 16 * (tile_row // 8) + 8 * part + tile_row % 8
@@ -109,10 +111,12 @@ def test_operand_rows_and_fragment_give_each_point_its_quadrants():
     lane_of_row = {m: (m // 16) * 32 + m % 16 for m in range(64)}
     row_of_lane = {ln: m for m, ln in lane_of_row.items()}
 
-    def ld16(lane_base, col_base, t):
-        """16x256b.x2: register -> (TMEM lane, column) for thread t."""
+    pp = 512 // nt     # point pairs per thread: 4 at 128 threads, 2 at 256
+
+    def ld(lane_base, col_base, t):
+        """16x256b.x{pp}: register -> (TMEM lane, column) for thread t."""
         regs = {}
-        for j in range(2):
+        for j in range(pp):
             for e in range(2):
                 col = col_base + 8 * j + 2 * (t % 4) + e
                 regs[4 * j + e] = (lane_base + t // 4, col)
@@ -120,15 +124,15 @@ def test_operand_rows_and_fragment_give_each_point_its_quadrants():
         return regs
 
     covered = np.zeros((32, 32), dtype=int)
-    for warp in range(8):
+    for warp in range(nt // 32):
         lq, ch = warp % 4, warp // 4
         for t in range(32):
-            v = ld16(32 * lq, 16 * ch, t)          # X_hi columns of this half
-            w = ld16(32 * lq, 32 + 16 * ch, t)     # X_lo columns
+            v = ld(32 * lq, 8 * pp * ch, t)          # X_hi columns of this warp
+            w = ld(32 * lq, 32 + 8 * pp * ch, t)     # X_lo columns
             prow = 8 * lq + t // 4
-            for k in range(4):
+            for k in range(2 * pp):
                 j, e = k // 2, k % 2
-                pcol = 8 * (2 * ch + j) + 2 * (t % 4) + e
+                pcol = 8 * (pp * ch + j) + 2 * (t % 4) + e
                 # the fold adds lo.hi, hi.lo, lo.lo, hi.hi
                 got = set()
                 for lane, col in (v[4 * j + 2 + e], w[4 * j + e], w[4 * j + 2 + e], v[4 * j + e]):
@@ -140,17 +144,20 @@ def test_operand_rows_and_fragment_give_each_point_its_quadrants():
     assert np.all(covered == 1)
 
 
-def test_factor_threads_cover_both_operands_once():
-    """256 threads: kg = (t / 16) % 8, half = (t / 8) % 2, r8 = t % 8, rs = t / 128,
-    rows i = 2 rs, 2 rs + 1; every (operand row, reference quad) is written once,
-    and each 8-lane group writes one 8-row core matrix (128 contiguous bytes)."""
+@pytest.mark.parametrize("nt", [128, 256])
+def test_factor_threads_cover_both_operands_once(nt):
+    """kg = (t / 16) % 8, half = (t / 8) % 2, r8 = t % 8, rs = t / 128, rows i =
+    PP rs + i', i' < PP = 512 / NT: every (operand row, reference quad) is written
+    once, and each 8-lane group writes one 8-row core matrix (128 contiguous
+    bytes)."""
+    pp = 512 // nt
     def off(m, k):
         return (k // 4) * 1024 + (m // 8) * 128 + (m % 8) * 16 + (k % 4) * 4
 
     seen = {}
-    for t in range(256):
+    for t in range(nt):
         kg, half, r8, rs = (t // 16) % 8, (t // 8) % 2, t % 8, t // 128
-        for i in (2 * rs, 2 * rs + 1):
+        for i in range(pp * rs, pp * rs + pp):
             mh = r8 + 8 * i if half else 16 * i + r8
             ml = 32 + r8 + 8 * i if half else 16 * i + 8 + r8
             for m in (mh, ml):
@@ -159,12 +166,12 @@ def test_factor_threads_cover_both_operands_once():
                 seen[key] = t
                 assert off(m, 4 * kg) + 16 <= 8192
     assert len(seen) == 2 * 64 * 8
-    for t0 in range(0, 256, 8):
-        for i_sel in (0, 1):
+    for t0 in range(0, nt, 8):
+        for i_sel in range(pp):
             offs = []
             for t in range(t0, t0 + 8):
                 kg, half, r8, rs = (t // 16) % 8, (t // 8) % 2, t % 8, t // 128
-                i = 2 * rs + i_sel
+                i = pp * rs + i_sel
                 m = r8 + 8 * i if half else 16 * i + r8
                 offs.append(off(m, 4 * kg))
             assert sorted(offs) == list(range(min(offs), min(offs) + 128, 16))
