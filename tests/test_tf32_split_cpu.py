@@ -11,10 +11,10 @@
 2. The index mappings of both block shapes (128 and 256 threads). A's row 16 q + 8 p + i holds part
    p (hi, lo) of tile row 8 q + i, and B's row c + 32 p holds part p of column c.
    An M = 64 accumulator row m sits in TMEM lane (m / 16) * 32 + m % 16. A
-   tcgen05.ld 16x256b.x2 at column c0 gives thread t register 4 j + e = (lane
-   t / 4, column c0 + 8 j + 2 (t % 4) + e) and register 4 j + 2 + e = (lane 8 +
-   t / 4, the same column) of its warp's lane quarter. Warps w and w + 4 share
-   quarter w % 4 and read column halves w / 4.
+   tcgen05.ld 16x256b.x(512 / NT) at column c0 gives thread t register 4 j + e =
+   (lane t / 4, column c0 + 8 j + 2 (t % 4) + e) and register 4 j + 2 + e = (lane
+   8 + t / 4, the same column) of its warp's lane quarter. With 256 threads, warps
+   w and w + 4 share quarter w % 4 and read column halves w / 4.
    Checked: the four registers the fold adds for each of a thread's points are
    the four quadrant products of that point's own row and column, and the
    threads cover the 32 x 32 tile once. The factor-making threads write every
