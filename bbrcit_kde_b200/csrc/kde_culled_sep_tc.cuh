@@ -10,8 +10,8 @@
 // bytes of loads per multiply-add. Here it is a tcgen05.mma chain instead:
 //   * each FP32 factor v is split into two TF32 terms, hi = v rounded to TF32
 //     and lo = v - hi, of which the tensor core reads the leading 11 bits (hi +
-//     lo carries 21 or more of v's 24 bits), and one
-//     kind::tf32 MMA of M = 64, N = 64, K = 8 multiplies A = [Y_hi; Y_lo] (rows)
+//     lo carries 21 or more of v's 24 bits), and one kind::tf32 MMA of M = 64,
+//     N = 64, K = 8 multiplies A = [Y_hi; Y_lo] (rows)
 //     by B = [X_hi; X_lo] (columns), so its four 32 x 32 quadrants are the four
 //     cross products; a point's value is the sum of its four quadrant entries,
 //     the small three first;
@@ -29,7 +29,7 @@
 // data path uses lanes 0-15 of each quarter), and row 16 q + 8 p + i holds part p
 // (hi, lo) of tile row 8 q + i, so that a 16x256b read hands one thread both parts
 // of its row. Two block shapes, four blocks per SM either way: NT = 128 threads
-// (115 registers), each owning 8 points and making the factors of 4 tile rows or
+// (118 registers), each owning 8 points and making the factors of 4 tile rows or
 // columns per group, or NT = 256 (64 registers), each owning 4 points and making 2.
 // With 256, warps w and w + 4 share lane quarter w % 4 and split the columns.
 // Thread t of warp w owns tile row 8 (w % 4) + t / 4 and columns 8 j + 2 (t % 4) +
@@ -39,8 +39,8 @@
 //
 // Accuracy: the split leaves less than 2^-21 of each factor; the MMA chain's FP32
 // accumulation over 32 references was measured at up to 6e-7 relative (mean 2e-7)
-// against FP64 of the same FP32 factors. The host uses this kernel only for sums
-// whose tolerance is at least kSepTcMinRel.
+// against FP64 of the same FP32 factors. The automatic setting uses this kernel
+// only for culled sums whose tolerance is at least kSepTcMinRel.
 //
 // Every wait on an mbarrier is bounded; on expiry the kernel stops issuing work,
 // sets *status and writes no results.
@@ -74,7 +74,8 @@ constexpr uint32_t kSepTcIdesc =
     (1u << 4) | (2u << 7) | (2u << 10) | ((64u >> 3) << 17) | ((64u >> 4) << 24);
 // Dynamic shared memory each block requests beyond its static arrays (about 44
 // KB): four blocks (4 x 128 TMEM columns = all 512) fit in an SM's shared memory,
-// a fifth does not.
+// a fifth does not (nor in its registers), so no block ever waits for tensor
+// memory.
 constexpr int kSepTcPadBytes = 4 * 1024;
 
 __device__ __forceinline__ uint32_t sep_tc_off(int m, int k) {
